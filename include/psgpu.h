@@ -1,0 +1,73 @@
+/*
+ * psgpu.h -- re-entrant C API of psgpu_b200 (libpsgpu.so).
+ *
+ * The reference (psgpu) exposes one non-re-entrant Fortran-ABI entry point
+ * per flavour, timestep_cuda_, that allocates, plans, copies, integrates and
+ * frees on every call (declared in psgpu_ref_abi.h, exported by the drop-in
+ * libraries).  This API is the persistent form of the same step: a handle
+ * owns device buffers and an explicit stream; the state stays resident in HBM
+ * between calls; every function returns a status (PSG_OK = 0) and
+ * psg_last_error() describes the last failure of the calling thread.
+ *
+ * Host state arrays use the reference's layout: complex128 interleaved boxes,
+ * kx fastest, ik = (ikz*IKTY + iky)*IKTX + ikx (3D) or iky*IKTX + ikx (2D),
+ * IKTX = N/3+1, IKTY = IKTZ = 2*(N/3)+1.
+ */
+#ifndef PSGPU_H
+#define PSGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSG_VERSION 100
+
+#define PSG_OK 0
+#define PSG_ERR_ARG 1
+#define PSG_ERR_CUDA 2
+#define PSG_ERR_UNSUPPORTED 3
+#define PSG_ERR_STATE 4
+
+/* time schemes of the 3D engine */
+#define PSG_SCHEME_NS_HEUN 0   /* 3D_NavierStokes/src/kernels.h:309-464 (Heun + CN)      */
+#define PSG_SCHEME_EULER_HEUN 1 /* 3D_Euler/src/kernels.h:296-439 (Heun, inviscid)      */
+#define PSG_SCHEME_NS_RK4 2    /* 3D_Boussinesq/src/kernels.h:331-621 with Ri = 0, no rho */
+#define PSG_SCHEME_BOUS_RK4 3  /* 3D_Boussinesq/src/kernels.h:331-621 (RK4 + CN stages)  */
+
+const char* psg_last_error(void);
+void psg_clear_error(void);
+int psg_version(void);
+
+/* ---------------------------------------------------------------- 3D */
+typedef struct psg_ns3d psg_ns3d;
+
+/* n: grid points per direction (16..512, power of two); alpha must be 1;
+ * precision: 32 (FP32 storage and transforms) or 64. */
+int psg_ns3d_create(psg_ns3d** h, int n, double alpha, int scheme, int precision);
+void psg_ns3d_destroy(psg_ns3d* h);
+/* nu = 1/Re; ampfor/kf: forcing as the reference's d_AMPFOR/d_KFY; ri, sc,
+ * theta (radians): Boussinesq parameters (ignored by the other schemes). */
+int psg_ns3d_set_params(psg_ns3d* h, double nu, double ampfor, double kf, double ri,
+                        double sc, double theta);
+int psg_ns3d_set_stream(psg_ns3d* h, void* cuda_stream);
+/* comps[0..2] = xii, eta, zet (+ comps[3] = rho for the Boussinesq scheme) */
+int psg_ns3d_upload(psg_ns3d* h, const double* const* comps);
+int psg_ns3d_download(psg_ns3d* h, double* const* comps);
+/* RK4 schemes: the stage state x0 (vorticity before the divergence clean-up) */
+int psg_ns3d_download_stage(psg_ns3d* h, double* const* comps);
+/* nsteps steps of length dt, enqueued on the handle's stream.  dump_last:
+ * keep the physical vorticity of the last predictor (Heun schemes) */
+int psg_ns3d_step(psg_ns3d* h, double dt, int nsteps, int dump_last);
+/* dz/dt at the uploaded state (RK4 schemes), written to out[0..nc-1] */
+int psg_ns3d_timederiv(psg_ns3d* h, double* const* out);
+/* physical fields kept by dump_last: out[0..2], n^3 doubles each, x fastest */
+int psg_ns3d_download_phys(psg_ns3d* h, double* const* out);
+int psg_ns3d_sync(psg_ns3d* h);
+long psg_ns3d_launches(psg_ns3d* h);
+/* device state pointers and padded row length (complex words) */
+int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

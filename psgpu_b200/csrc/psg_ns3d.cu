@@ -1,0 +1,921 @@
+// psg_ns3d.cu -- sm_100a kernels and host engine of the 3D pseudospectral step
+// (Navier-Stokes Heun/CN, Euler Heun, Navier-Stokes RK4/CN, Boussinesq RK4/CN).
+//
+// See psg_ns3d.cuh for the data layout and the pass structure.  Each scheme
+// update restates the reference kernel cited beside it; the transforms replace
+// the reference's conj -> setFFN -> cufftExecZ2D -> multReal -> cufftExecD2Z ->
+// normFF1 sequence (3D_NavierStokes/src/functions.h:26-108).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <type_traits>
+#include <vector>
+
+#include "psg_ns3d.cuh"
+#include "psgpu_internal.h"
+
+namespace psg {
+
+// FFT row (0..n-1) -> box index (0..2K) or -1 when the row is truncated
+__device__ __forceinline__ int row_to_box(int r, int K, int n) {
+  if (r <= K) return r + K;
+  if (r >= n - K) return r - n + K;
+  return -1;
+}
+
+// 2/3-rule mask of the reference (3D_NavierStokes/src/init.F90:43-46) for
+// integer box indices; alpha scales kx.
+template <typename T>
+__device__ __forceinline__ bool keep_mode(int ix, int ky, int kz, int K, T alpha) {
+  if (ix == 0 && ky < 0) return false;
+  if (ix == 0 && ky == 0 && kz <= 0) return false;
+  const T kx = (T)ix * alpha;
+  const T wk = kx * kx + (T)(ky * ky + kz * kz);
+  const T lim = (T)K - (T)0.5;
+  return !(wk > lim * lim);
+}
+
+template <typename T>
+__device__ __forceinline__ T wkinv(T wk) {
+  return (T)1 / (wk > (T)0.001 ? wk : (T)0.001);
+}
+
+// ---------------------------------------------------------------------------
+// pass A: z-inverse of the stage state with the velocity (and density
+// gradient) formed in registers; Hermitian completion of the kx = 0 plane.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int W, int NC, int NF>
+__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
+pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
+       int mask_vel) {
+  using F = LineFFT<N, +1, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* s_in = s_tw + N;                       // [NC][Y][W]
+  cpx<T>* s_ex = s_in + NC * g.Y * W;            // [W][SMEM]
+  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + W * F::SMEM);  // [Y][W]
+
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int c = tid % W, gi = tid / W;
+  const int x0 = blockIdx.x * W, iky = blockIdx.y;
+  const int K = g.K, Y = g.Y, XP = g.XP;
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  for (int idx = tid; idx < Y * W; idx += nth) {
+    const int ikz = idx / W, cc = idx % W, ikx = x0 + cc;
+    int sz = ikz, sy = iky;
+    bool cj = false, zero = (ikx >= g.X);
+    if (ikx == 0) {
+      if (iky < K || (iky == K && ikz < K)) { sz = 2 * K - ikz; sy = 2 * K - iky; cj = true; }
+      else if (iky == K && ikz == K) zero = true;
+    }
+    const long src = ((long)sz * Y + sy) * XP + ikx;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      cpx<T> v = zero ? czero<T>() : in.c[q][src];
+      if (cj) v.y = -v.y;
+      s_in[(q * Y + ikz) * W + cc] = v;
+    }
+    s_ll[idx] = zero ? 0 : (unsigned char)keep_mode<T>(ikx, sy - K, sz - K, K, g.alpha);
+  }
+  __syncthreads();
+
+  const T kx = (T)(x0 + c) * g.alpha;
+  const T ky = (T)(iky - K);
+#pragma unroll 1
+  for (int f = 0; f < NF; ++f) {
+    cpx<T> v[F::E];
+#pragma unroll
+    for (int e = 0; e < F::E; ++e) {
+      const int ikz = row_to_box(F::in_index(gi, e), K, N);
+      cpx<T> r = czero<T>();
+      if (ikz >= 0) {
+        const int o = ikz * W + c;
+        if (f < 3) {
+          r = s_in[f * Y * W + o];
+        } else if (f < 6) {
+          const cpx<T> xi = s_in[o], et = s_in[Y * W + o], zt = s_in[2 * Y * W + o];
+          const T kz = (T)(ikz - K);
+          const T wk = kx * kx + ky * ky + kz * kz;
+          T wki = wkinv(wk);
+          if (mask_vel && !s_ll[o]) wki = (T)0;
+          // u = i k x w / k^2 (3D_NavierStokes/src/kernels.h:194-201)
+          if (f == 3) r = cpx<T>{-(ky * zt.y - kz * et.y) * wki, -(kz * et.x - ky * zt.x) * wki};
+          else if (f == 4) r = cpx<T>{-(kz * xi.y - kx * zt.y) * wki, -(kx * zt.x - kz * xi.x) * wki};
+          else r = cpx<T>{-(kx * et.y - ky * xi.y) * wki, -(ky * xi.x - kx * et.x) * wki};
+        } else {
+          // i k_j rho (setFFK, 3D_Boussinesq/src/kernels.h:75-93)
+          const cpx<T> rho = s_in[3 * Y * W + o];
+          const T kk = (f == 6) ? kx : (f == 7) ? ky : (T)(ikz - K);
+          r = cpx<T>{-kk * rho.y, kk * rho.x};
+        }
+      }
+      v[e] = r;
+    }
+    F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
+    cpx<T>* o = out + ((long)f * N * Y + iky) * XP + x0 + c;
+#pragma unroll
+    for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * XP] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// passes B and D: transform a tile of W columns along the middle (y) axis.
+//   INV: rows iky (Y of them) -> rows y (N);  !INV: rows y (N) -> rows iky (Y)
+// in/out planes: [f][z][rows][XP]
+// ---------------------------------------------------------------------------
+template <typename T, int N, int W, bool INV>
+__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
+pass_y(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
+       const cpx<T>* __restrict__ tw) {
+  using F = LineFFT<N, INV ? +1 : -1, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* s_ex = s_tw + N;
+  const int tid = threadIdx.x, c = tid % W, gi = tid / W;
+  const int x0 = blockIdx.x * W, z = blockIdx.y, f = blockIdx.z;
+  const int K = g.K, Y = g.Y, XP = g.XP;
+  const int rin = INV ? Y : N, rout = INV ? N : Y;
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
+  const cpx<T>* src = in + (((long)f * N + z) * rin) * XP + x0 + c;
+  cpx<T> v[F::E];
+#pragma unroll
+  for (int e = 0; e < F::E; ++e) {
+    const int r = F::in_index(gi, e);
+    if (INV) {
+      const int iky = row_to_box(r, K, N);
+      v[e] = iky >= 0 ? src[(long)iky * XP] : czero<T>();
+    } else {
+      v[e] = src[(long)r * XP];
+    }
+  }
+  __syncthreads();
+  F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
+  cpx<T>* dst = out + (((long)f * N + z) * rout) * XP + x0 + c;
+#pragma unroll
+  for (int e = 0; e < F::E; ++e) {
+    const int k = F::out_index(gi, e);
+    if (INV) {
+      dst[(long)k * XP] = v[e];
+    } else {
+      const int iky = row_to_box(k, K, N);
+      if (iky >= 0) dst[(long)iky * XP] = v[e];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pass C: x rows.  C2R of the fields (packed two real signals per complex
+// transform), the products -(u x w) (multReal, 3D_NavierStokes/src/kernels.h:
+// 281-306) and u.grad rho (3D_Boussinesq/src/kernels.h:298-328) in registers,
+// scaled by 1/N^3 (normFF1), and R2C back, keeping kx <= K.
+// in: [NF][z][y][XP], out: [NO][z][y][XP].  One row per group of G threads.
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+struct RowOps {
+  using FI = LineFFT<N, +1, T>;
+  using FO = LineFFT<N, -1, T>;
+  static constexpr int G = FI::G, E = FI::E;
+
+  // inverse transform of two real fields a, b given by their half spectra
+  static __device__ __forceinline__ void c2r_pair(const cpx<T>* __restrict__ A,
+                                                  const cpx<T>* __restrict__ B, int K, int gi,
+                                                  const cpx<T>* tw, cpx<T>* ex, T (&ra)[E],
+                                                  T (&rb)[E]) {
+    cpx<T> v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int r = FI::in_index(gi, e);
+      cpx<T> z = czero<T>();
+      if (r == 0) {
+        const T a = A[0].x, b = B ? B[0].x : (T)0;
+        z = cpx<T>{a, b};
+      } else if (r <= K) {
+        const cpx<T> a = A[r], b = B ? B[r] : czero<T>();
+        z = cpx<T>{a.x - b.y, a.y + b.x};  // a + i b
+      } else if (r >= N - K) {
+        const cpx<T> a = A[N - r], b = B ? B[N - r] : czero<T>();
+        z = cpx<T>{a.x + b.y, -a.y + b.x};  // conj(a) + i conj(b)
+      }
+      v[e] = z;
+    }
+    FI::run(v, gi, tw, ex, WarpSync());
+#pragma unroll
+    for (int e = 0; e < E; ++e) { ra[e] = v[e].x; rb[e] = v[e].y; }
+  }
+
+  // forward transform of two real signals p, q; writes P_k, Q_k for k < XP
+  // (zero beyond K).  q == nullptr: single signal p.
+  static __device__ __forceinline__ void r2c_pair(const T (&p)[E], const T* q, int K, int XP,
+                                                  int gi, const cpx<T>* tw, cpx<T>* ex,
+                                                  cpx<T>* __restrict__ P,
+                                                  cpx<T>* __restrict__ Q) {
+    cpx<T> v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cpx<T>{p[e], q ? q[e] : (T)0};
+    FO::run(v, gi, tw, ex, WarpSync());
+    if (q) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) ex[FO::out_index(gi, e)] = v[e];
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = FO::out_index(gi, e);
+        if (k < XP) {
+          cpx<T> pk = czero<T>(), qk = czero<T>();
+          if (k <= K) {
+            const cpx<T> a = v[e], b = ex[(N - k) & (N - 1)];
+            // P = (Z_k + conj Z_{N-k}) / 2,  Q = -i (Z_k - conj Z_{N-k}) / 2
+            pk = cpx<T>{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+            qk = cpx<T>{(T)0.5 * (a.y + b.y), (T)(-0.5) * (a.x - b.x)};
+          }
+          P[k] = pk;
+          Q[k] = qk;
+        }
+      }
+      __syncwarp();
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = FO::out_index(gi, e);
+        if (k < XP) P[k] = (k <= K) ? v[e] : czero<T>();
+      }
+    }
+  }
+};
+
+template <typename T, int N, bool BOUS>
+__global__ void __launch_bounds__(128)
+pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
+       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump) {
+  using R = RowOps<T, N>;
+  constexpr int G = R::G, E = R::E;
+  constexpr int L = 128 / G;  // rows per block
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* s_ex = s_tw + N;
+  const int tid = threadIdx.x, lr = tid / G, gi = tid % G;
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
+  __syncthreads();
+  const long row = (long)blockIdx.x * L + lr;  // z * N + y
+  const int K = g.K, XP = g.XP;
+  const long plane = (long)N * N * XP;
+  const cpx<T>* src = in + row * XP;
+  cpx<T>* ex = s_ex + lr * R::FI::SMEM;
+
+  T xi[E], et[E], zt[E], u[E], v[E], w[E];
+  R::c2r_pair(src, src + plane, K, gi, s_tw, ex, xi, et);
+  R::c2r_pair(src + 2 * plane, src + 3 * plane, K, gi, s_tw, ex, zt, u);
+  R::c2r_pair(src + 4 * plane, src + 5 * plane, K, gi, s_tw, ex, v, w);
+  if (dump) {
+    const long base = row * N;
+    const long nr = (long)N * N * N;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int x = R::FI::out_index(gi, e);
+      dump[base + x] = xi[e];
+      dump[nr + base + x] = et[e];
+      dump[2 * nr + base + x] = zt[e];
+    }
+  }
+  T n1[E], n2[E], n3[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    // U,V,W <- -(u x w)  (multReal)
+    n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * scale;
+    n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
+    n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
+  }
+  cpx<T>* dst = out + row * XP;
+  if (!BOUS) {
+    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + plane);
+    R::r2c_pair(n3, nullptr, K, XP, gi, s_tw, ex, dst + 2 * plane, nullptr);
+  } else {
+    T rx[E], ry[E], n4[E];
+    R::c2r_pair(src + 6 * plane, src + 7 * plane, K, gi, s_tw, ex, rx, ry);
+#pragma unroll
+    for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
+    R::c2r_pair(src + 8 * plane, nullptr, K, gi, s_tw, ex, rx, ry);
+#pragma unroll
+    for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
+    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + plane);
+    R::r2c_pair(n3, n4, K, XP, gi, s_tw, ex, dst + 2 * plane, dst + 3 * plane);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pass E: z-forward of the NO fields of one ky plane tile, then the spectral
+// finish and the scheme update for every mode of the tile.
+// in: [NO][z][ky][XP]
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Regs {
+  Fields4<T> S, X0, K1, K2, K3;
+};
+
+template <typename T, int N, int W, int NO, int SCHEME>
+__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
+pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw, Regs<T> R,
+       StepParams<T> p, int stage) {
+  using F = LineFFT<N, -1, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* s_res = s_tw + N;            // [NO][Y][W]
+  cpx<T>* s_ex = s_res + NO * g.Y * W;  // [W][SMEM]
+  const int tid = threadIdx.x, nth = blockDim.x, c = tid % W, gi = tid / W;
+  const int x0 = blockIdx.x * W, iky = blockIdx.y;
+  const int K = g.K, Y = g.Y, XP = g.XP;
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  __syncthreads();
+#pragma unroll 1
+  for (int f = 0; f < NO; ++f) {
+    const cpx<T>* src = in + ((long)f * N * Y + iky) * XP + x0 + c;
+    cpx<T> v[F::E];
+#pragma unroll
+    for (int e = 0; e < F::E; ++e) v[e] = src[(long)F::in_index(gi, e) * Y * XP];
+    F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
+#pragma unroll
+    for (int e = 0; e < F::E; ++e) {
+      const int ikz = row_to_box(F::out_index(gi, e), K, N);
+      if (ikz >= 0) s_res[(f * Y + ikz) * W + c] = v[e];
+    }
+  }
+  __syncthreads();
+
+  for (int idx = tid; idx < Y * W; idx += nth) {
+    const int ikz = idx / W, cc = idx % W, ikx = x0 + cc;
+    if (ikx >= g.X) continue;
+    const long ik = ((long)ikz * Y + iky) * XP + ikx;
+    const int iy = iky - K, iz = ikz - K;
+    const T kx = (T)ikx * g.alpha, ky = (T)iy, kz = (T)iz;
+    const T wk = kx * kx + ky * ky + kz * kz;
+    const T wki = wkinv(wk);
+    const T LL = keep_mode<T>(ikx, iy, iz, K, g.alpha) ? (T)1 : (T)0;
+    const cpx<T> U = s_res[(0 * Y + ikz) * W + cc];
+    const cpx<T> V = s_res[(1 * Y + ikz) * W + cc];
+    const cpx<T> Wv = s_res[(2 * Y + ikz) * W + cc];
+    // curl of F(-(u x w)) as preStep/corStep form it (3D_NavierStokes/src/kernels.h:327-334)
+    T xiX = ky * Wv.y - kz * V.y, xiY = kz * V.x - ky * Wv.x;
+    T etX = kz * U.y - kx * Wv.y, etY = kx * Wv.x - kz * U.x;
+    T ztX = kx * V.y - ky * U.y, ztY = ky * U.x - kx * V.x;
+
+    if (SCHEME == SCHEME_NS_HEUN || SCHEME == SCHEME_EULER_HEUN) {
+      cpx<T>* S0 = R.S.c[0]; cpx<T>* S1 = R.S.c[1]; cpx<T>* S2 = R.S.c[2];
+      cpx<T>* H0 = R.K1.c[0]; cpx<T>* H1 = R.K1.c[1]; cpx<T>* H2 = R.K1.c[2];
+      const cpx<T> s0 = S0[ik], s1 = S1[ik], s2 = S2[ik];
+      if (SCHEME == SCHEME_NS_HEUN) {
+        if (kx == (T)0 && kz == p.kf && ky == p.kf) xiX += p.ampfor;
+        if (kx == (T)0 && kz == -p.kf && ky == p.kf) xiX -= p.ampfor;
+        // nuzn = (1 - nu k^2 dt/2)/dt, nu1 = dt/(1 + nu k^2 dt/2) (3D_NavierStokes/src/init.F90:194-198)
+        const T NU = p.nu * wk;
+        const T nuzn = LL * (((T)1 - (T)0.5 * NU * p.dt) / p.dt);
+        const T nu1 = LL * (p.dt / ((T)1 + (T)0.5 * NU * p.dt));
+        if (stage == STAGE_HEUN_PRED) {
+          H0[ik] = cpx<T>{xiX, xiY}; H1[ik] = cpx<T>{etX, etY}; H2[ik] = cpx<T>{ztX, ztY};
+          const T NU1 = LL * nu1;
+          S0[ik] = cpx<T>{NU1 * (nuzn * s0.x + xiX), NU1 * (nuzn * s0.y + xiY)};
+          S1[ik] = cpx<T>{NU1 * (nuzn * s1.x + etX), NU1 * (nuzn * s1.y + etY)};
+          S2[ik] = cpx<T>{NU1 * (nuzn * s2.x + ztX), NU1 * (nuzn * s2.y + ztY)};
+        } else {
+          const T NU2 = (T)0.5 * nu1;
+          const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
+          S0[ik] = cpx<T>{LL * (s0.x + NU2 * (xiX - h0.x)), LL * (s0.y + NU2 * (xiY - h0.y))};
+          S1[ik] = cpx<T>{LL * (s1.x + NU2 * (etX - h1.x)), LL * (s1.y + NU2 * (etY - h1.y))};
+          S2[ik] = cpx<T>{LL * (s2.x + NU2 * (ztX - h2.x)), LL * (s2.y + NU2 * (ztY - h2.y))};
+        }
+      } else {  // Euler (3D_Euler/src/kernels.h:324-341, 396-406)
+        if (stage == STAGE_HEUN_PRED) {
+          H0[ik] = cpx<T>{LL * xiX, LL * xiY}; H1[ik] = cpx<T>{LL * etX, LL * etY};
+          H2[ik] = cpx<T>{LL * ztX, LL * ztY};
+          S0[ik] = cpx<T>{s0.x + p.dt * xiX, s0.y + p.dt * xiY};
+          S1[ik] = cpx<T>{s1.x + p.dt * etX, s1.y + p.dt * etY};
+          S2[ik] = cpx<T>{s2.x + p.dt * ztX, s2.y + p.dt * ztY};
+        } else {
+          const T hd = (T)0.5 * p.dt;
+          const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
+          S0[ik] = cpx<T>{LL * (s0.x + hd * (xiX - h0.x)), LL * (s0.y + hd * (xiY - h0.y))};
+          S1[ik] = cpx<T>{LL * (s1.x + hd * (etX - h1.x)), LL * (s1.y + hd * (etY - h1.y))};
+          S2[ik] = cpx<T>{LL * (s2.x + hd * (ztX - h2.x)), LL * (s2.y + hd * (ztY - h2.y))};
+        }
+      }
+    } else {
+      // RK4 with per-stage CN factors (3D_Boussinesq/src/kernels.h:331-621)
+      constexpr bool BOUS = (SCHEME == SCHEME_BOUS_RK4);
+      T rXR = 0, rXC = 0;  // density right-hand side
+      const bool final_stage = (stage == STAGE_RK4);
+      const T LC = final_stage ? (T)1 : LL;
+      const cpx<T> x0 = R.X0.c[0][ik], e0 = R.X0.c[1][ik], z0 = R.X0.c[2][ik];
+      if (BOUS) {
+        const cpx<T> r0 = R.X0.c[3][ik];
+        const cpx<T> RK = s_res[(3 * Y + ikz) * W + cc];
+        const T gXR = -kx * r0.y, gXC = kx * r0.x, gYR = -ky * r0.y, gYC = ky * r0.x;
+        const T gZR = -kz * r0.y, gZC = kz * r0.x;
+        xiX = LC * (xiX - p.ri * (gYR * p.sinth - gZR * p.costh));
+        xiY = LC * (xiY - p.ri * (gYC * p.sinth - gZC * p.costh));
+        etX = LC * (etX + p.ri * gXR * p.sinth);
+        etY = LC * (etY + p.ri * gXC * p.sinth);
+        ztX = LC * (ztX - p.ri * gXR * p.costh);
+        ztY = LC * (ztY - p.ri * gXC * p.costh);
+        rXR = -LC * (RK.x + (kz * x0.y - kx * z0.y) * wki * p.costh +
+                     (kx * e0.y - ky * x0.y) * wki * p.sinth);
+        rXC = -LC * (RK.y + (kx * z0.x - kz * x0.x) * wki * p.costh +
+                     (ky * x0.x - kx * e0.x) * wki * p.sinth);
+      } else {
+        xiX *= LC; xiY *= LC; etX *= LC; etY *= LC; ztX *= LC; ztY *= LC;
+      }
+      if (kx == (T)0 && kz == (T)0 && ky == p.kf) ztX += p.ampfor;
+      const T dt = p.dt;
+      const T nk = dt * p.nu * wk;
+      const T nks = BOUS ? nk / p.sc : (T)0;
+      if (stage == STAGE_DERIV) {  // RHS kernel: dz/dt = -nu k^2 z + N
+        const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
+        const T d1 = -p.nu * wk;
+        R.K1.c[0][ik] = cpx<T>{d1 * s0.x + xiX, d1 * s0.y + xiY};
+        R.K1.c[1][ik] = cpx<T>{d1 * s1.x + etX, d1 * s1.y + etY};
+        R.K1.c[2][ik] = cpx<T>{d1 * s2.x + ztX, d1 * s2.y + ztY};
+        if (BOUS) {
+          const cpx<T> s3 = R.S.c[3][ik];
+          const T d2 = -p.nu * wk / p.sc;
+          R.K1.c[3][ik] = cpx<T>{d2 * s3.x + rXR, d2 * s3.y + rXC};
+        }
+      } else if (!final_stage) {
+        const T q = (stage == STAGE_RK3) ? (T)0.5 : (T)0.25;
+        const T fr = (stage == STAGE_RK3) ? (T)1 : (T)0.5;
+        const T d1 = ((T)1 - q * nk) / ((T)1 + q * nk);
+        const Fields4<T>& KR = (stage == STAGE_RK1) ? R.K1 : (stage == STAGE_RK2) ? R.K2 : R.K3;
+        KR.c[0][ik] = cpx<T>{dt * xiX, dt * xiY};
+        KR.c[1][ik] = cpx<T>{dt * etX, dt * etY};
+        KR.c[2][ik] = cpx<T>{dt * ztX, dt * ztY};
+        const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
+        R.X0.c[0][ik] = cpx<T>{d1 * (s0.x + fr * dt * xiX), d1 * (s0.y + fr * dt * xiY)};
+        R.X0.c[1][ik] = cpx<T>{d1 * (s1.x + fr * dt * etX), d1 * (s1.y + fr * dt * etY)};
+        R.X0.c[2][ik] = cpx<T>{d1 * (s2.x + fr * dt * ztX), d1 * (s2.y + fr * dt * ztY)};
+        if (BOUS) {
+          const T d2 = ((T)1 - q * nks) / ((T)1 + q * nks);
+          KR.c[3][ik] = cpx<T>{dt * rXR, dt * rXC};
+          const cpx<T> s3 = R.S.c[3][ik];
+          R.X0.c[3][ik] = cpx<T>{d2 * (s3.x + fr * dt * rXR), d2 * (s3.y + fr * dt * rXC)};
+        }
+      } else {
+        const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
+        const T d1 = (T)1 - (T)0.5 * nk;
+        const T den = (T)1 + (T)0.5 * nk;
+        T o[4][2];
+        const T nr[3][2] = {{xiX, xiY}, {etX, etY}, {ztX, ztY}};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const cpx<T> s = R.S.c[q][ik], a = R.K1.c[q][ik], b = R.K2.c[q][ik], cc3 = R.K3.c[q][ik];
+          o[q][0] = LL * (d1 * s.x + sixth * (a.x + dt * nr[q][0]) + third * (b.x + cc3.x)) / den;
+          o[q][1] = LL * (d1 * s.y + sixth * (a.y + dt * nr[q][1]) + third * (b.y + cc3.y)) / den;
+        }
+        if (BOUS) {
+          const T d2 = (T)1 - (T)0.5 * nks;
+          const T den2 = (T)1 + (T)0.5 * nks;
+          const cpx<T> s = R.S.c[3][ik], a = R.K1.c[3][ik], b = R.K2.c[3][ik], cc3 = R.K3.c[3][ik];
+          o[3][0] = LL * (d2 * s.x + sixth * (a.x + dt * rXR) + third * (b.x + cc3.x)) / den2;
+          o[3][1] = LL * (d2 * s.y + sixth * (a.y + dt * rXC) + third * (b.y + cc3.y)) / den2;
+          R.X0.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
+          R.S.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) R.X0.c[q][ik] = cpx<T>{o[q][0], o[q][1]};
+        // remove the divergence of the vorticity (3D_Boussinesq/src/kernels.h:597-606)
+        const T phiR = (kx * o[0][1] + ky * o[1][1] + kz * o[2][1]) * wki;
+        const T phiC = -(kx * o[0][0] + ky * o[1][0] + kz * o[2][0]) * wki;
+        R.S.c[0][ik] = cpx<T>{o[0][0] - (-kx * phiC), o[0][1] - kx * phiR};
+        R.S.c[1][ik] = cpx<T>{o[1][0] - (-ky * phiC), o[1][1] - ky * phiR};
+        R.S.c[2][ik] = cpx<T>{o[2][0] - (-kz * phiC), o[2][1] - kz * phiR};
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion between the reference's FP64 boxes and the device layout
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>* __restrict__ dst) {
+  const long total = (long)g.Y * g.Y * g.XP;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.XP);
+    const long r = i / g.XP;
+    cpx<T> v = czero<T>();
+    if (ix < g.X) {
+      const double2 s = src[r * g.X + ix];
+      v = cpx<T>{(T)s.x, (T)s.y};
+    }
+    dst[i] = v;
+  }
+}
+
+template <typename T>
+__global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* __restrict__ dst) {
+  const long total = (long)g.Y * g.Y * g.X;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.X);
+    const long r = i / g.X;
+    const cpx<T> s = src[r * g.XP + ix];
+    dst[i] = make_double2((double)s.x, (double)s.y);
+  }
+}
+
+template <typename T>
+__global__ void real_to_double(const T* __restrict__ src, double* __restrict__ dst, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+template <typename T>
+__global__ void copy_fields(Fields4<T> src, Fields4<T> dst, int nc, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x)
+    for (int q = 0; q < nc; ++q) dst.c[q][i] = src.c[q][i];
+}
+
+// ---------------------------------------------------------------------------
+// host engine
+// ---------------------------------------------------------------------------
+constexpr int kTileW = 8;
+
+template <typename T>
+struct Engine3D {
+  Geom3<T> g{};
+  int scheme = 0;
+  int nc = 3;    // state components
+  int nfi = 6;   // fields transformed to physical space
+  int nfo = 3;   // fields transformed back
+  long box = 0;  // complex words per component
+  StepParams<T> prm{};
+  cudaStream_t stream = 0;
+  int first_rhs = 1;     // mask velocity on the first evaluation after an upload
+  cpx<T>* pool = nullptr;
+  cpx<T>* tw = nullptr;
+  T* dump = nullptr;     // physical vorticity of the last predictor (Heun schemes)
+  Regs<T> R{};
+  cpx<T>* B1 = nullptr;
+  cpx<T>* B2 = nullptr;
+  double2* stage_h = nullptr;  // device FP64 staging box
+  long launches = 0;
+
+  size_t smem_a() const {
+    return sizeof(cpx<T>) * (g.n + (size_t)nc * g.Y * kTileW + kTileW * fft_smem()) + g.Y * kTileW;
+  }
+  size_t smem_y() const { return sizeof(cpx<T>) * (g.n + kTileW * fft_smem()); }
+  size_t smem_c() const { return sizeof(cpx<T>) * (g.n + (size_t)(128 / fft_g()) * fft_smem()); }
+  size_t smem_e() const {
+    return sizeof(cpx<T>) * (g.n + (size_t)nfo * g.Y * kTileW + kTileW * fft_smem());
+  }
+  int fft_g() const {
+    switch (g.n) {
+      case 16: return LineFFT<16, 1, T>::G;
+      case 32: return LineFFT<32, 1, T>::G;
+      case 64: return LineFFT<64, 1, T>::G;
+      case 128: return LineFFT<128, 1, T>::G;
+      case 256: return LineFFT<256, 1, T>::G;
+      default: return LineFFT<512, 1, T>::G;
+    }
+  }
+  int fft_smem() const {
+    switch (g.n) {
+      case 16: return LineFFT<16, 1, T>::SMEM;
+      case 32: return LineFFT<32, 1, T>::SMEM;
+      case 64: return LineFFT<64, 1, T>::SMEM;
+      case 128: return LineFFT<128, 1, T>::SMEM;
+      case 256: return LineFFT<256, 1, T>::SMEM;
+      default: return LineFFT<512, 1, T>::SMEM;
+    }
+  }
+
+  int init(int n, double alpha, int scheme_) {
+    if (!(n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512)) {
+      psg_set_error("3D grid size %d unsupported (powers of two 16..512)", n);
+      return PSG_ERR_UNSUPPORTED;
+    }
+    g.n = n; g.K = n / 3; g.X = g.K + 1; g.Y = 2 * g.K + 1;
+    g.XP = (g.X + kTileW - 1) / kTileW * kTileW;
+    g.alpha = (T)alpha;
+    scheme = scheme_;
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    nc = bous ? 4 : 3;
+    nfi = bous ? 9 : 6;
+    nfo = bous ? 4 : 3;
+    box = (long)g.Y * g.Y * g.XP;
+    const int nregs = (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) ? 2 : 5;
+    const long b1 = (long)nfi * n * g.Y * g.XP;
+    const long b3 = (long)nfo * n * n * g.XP;
+    const long b2 = (long)nfi * n * n * g.XP;
+    const long nb1 = b1 > b3 ? b1 : b3;
+    const long total = (long)nregs * nc * box + nb1 + b2 + n;
+    PSG_CUDA_TRY(cudaMalloc(&pool, sizeof(cpx<T>) * total));
+    PSG_CUDA_TRY(cudaMemset(pool, 0, sizeof(cpx<T>) * total));
+    cpx<T>* p = pool;
+    Fields4<T>* regs[5] = {&R.S, &R.K1, &R.X0, &R.K2, &R.K3};
+    for (int r = 0; r < 5; ++r)
+      for (int q = 0; q < 4; ++q) regs[r]->c[q] = nullptr;
+    for (int r = 0; r < nregs; ++r)
+      for (int q = 0; q < nc; ++q) { regs[r]->c[q] = p; p += box; }
+    B1 = p; p += nb1;
+    B2 = p; p += b2;
+    tw = p; p += n;
+    std::vector<cpx<T>> h(n);
+    for (int j = 0; j < n; ++j) {
+      const double a = -2.0 * M_PI * (double)j / (double)n;
+      h[j] = cpx<T>{(T)cos(a), (T)sin(a)};
+    }
+    PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
+    PSG_CUDA_TRY(cudaMalloc(&stage_h, sizeof(double2) * (long)g.Y * g.Y * g.X));
+    if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN)
+      PSG_CUDA_TRY(cudaMalloc(&dump, sizeof(T) * 3L * n * n * n));
+    return set_smem_limits();
+  }
+
+  void release() {
+    if (pool) cudaFree(pool);
+    if (stage_h) cudaFree(stage_h);
+    if (dump) cudaFree(dump);
+    pool = nullptr; stage_h = nullptr; dump = nullptr;
+  }
+
+  template <int N>
+  int set_smem_limits_n() {
+    const int big = 200 * 1024;
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, kTileW, 3, 6>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, kTileW, 4, 9>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_NS_HEUN>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_EULER_HEUN>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_NS_RK4>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 4, SCHEME_BOUS_RK4>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    return PSG_OK;
+  }
+  int set_smem_limits() {
+    switch (g.n) {
+      case 16: return set_smem_limits_n<16>();
+      case 32: return set_smem_limits_n<32>();
+      case 64: return set_smem_limits_n<64>();
+      case 128: return set_smem_limits_n<128>();
+      case 256: return set_smem_limits_n<256>();
+      default: return set_smem_limits_n<512>();
+    }
+  }
+
+  Fields4<T> stage_input() const {
+    if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) return R.S;
+    return R.X0;
+  }
+
+  // one right-hand-side evaluation followed by the stage update
+  template <int N>
+  int rhs_n(int stage, bool want_dump) {
+    using FG = LineFFT<N, 1, T>;
+    const int G = FG::G;
+    const dim3 blk(kTileW * G);
+    const int tiles = g.XP / kTileW;
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    Fields4<T> in = stage_input();
+    const int mv = first_rhs;
+    first_rhs = 0;
+    if (bous)
+      pass_a<T, N, kTileW, 4, 9><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
+    else
+      pass_a<T, N, kTileW, 3, 6><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
+    pass_y<T, N, kTileW, true><<<dim3(tiles, N, nfi), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    const T scale = (T)1 / ((T)N * (T)N * (T)N);
+    const int rows_per_block = 128 / G;
+    const int cblocks = (N * N) / rows_per_block;
+    T* dp = want_dump ? dump : nullptr;
+    if (bous)
+      pass_c<T, N, true><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
+    else
+      pass_c<T, N, false><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
+    pass_y<T, N, kTileW, false><<<dim3(tiles, N, nfo), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    const dim3 ge(tiles, g.Y);
+    switch (scheme) {
+      case SCHEME_NS_HEUN:
+        pass_e<T, N, kTileW, 3, SCHEME_NS_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        break;
+      case SCHEME_EULER_HEUN:
+        pass_e<T, N, kTileW, 3, SCHEME_EULER_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        break;
+      case SCHEME_NS_RK4:
+        pass_e<T, N, kTileW, 3, SCHEME_NS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        break;
+      default:
+        pass_e<T, N, kTileW, 4, SCHEME_BOUS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+    }
+    launches += 5;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  int rhs(int stage, bool want_dump = false) {
+    switch (g.n) {
+      case 16: return rhs_n<16>(stage, want_dump);
+      case 32: return rhs_n<32>(stage, want_dump);
+      case 64: return rhs_n<64>(stage, want_dump);
+      case 128: return rhs_n<128>(stage, want_dump);
+      case 256: return rhs_n<256>(stage, want_dump);
+      default: return rhs_n<512>(stage, want_dump);
+    }
+  }
+
+  // one full time step of length dt; dump: keep the physical vorticity of the
+  // predictor (Heun schemes)
+  int step(T dt, bool want_dump = false) {
+    prm.dt = dt;
+    int rc;
+    if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) {
+      if ((rc = rhs(STAGE_HEUN_PRED))) return rc;
+      return rhs(STAGE_HEUN_CORR, want_dump);
+    }
+    if ((rc = rhs(STAGE_RK1))) return rc;
+    if ((rc = rhs(STAGE_RK2))) return rc;
+    if ((rc = rhs(STAGE_RK3))) return rc;
+    return rhs(STAGE_RK4);
+  }
+
+  // host FP64 boxes (reference layout) -> device state; RK4 schemes also set
+  // the stage state X0 = S as the reference's setVelocity does.
+  int upload(const double* const* comps) {
+    const long nref = (long)g.Y * g.Y * g.X;
+    for (int q = 0; q < nc; ++q) {
+      PSG_CUDA_TRY(cudaMemcpyAsync(stage_h, comps[q], sizeof(double2) * nref,
+                                   cudaMemcpyHostToDevice, stream));
+      box_from_ref<T><<<592, 256, 0, stream>>>(g, stage_h, R.S.c[q]);
+      ++launches;
+    }
+    if (R.X0.c[0]) {
+      copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
+      ++launches;
+    }
+    first_rhs = 1;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  int download(double* const* comps, const Fields4<T>* src = nullptr) {
+    const long nref = (long)g.Y * g.Y * g.X;
+    const Fields4<T>& F = src ? *src : R.S;
+    for (int q = 0; q < nc; ++q) {
+      box_to_ref<T><<<592, 256, 0, stream>>>(g, F.c[q], stage_h);
+      ++launches;
+      PSG_CUDA_TRY(cudaMemcpyAsync(comps[q], stage_h, sizeof(double2) * nref,
+                                   cudaMemcpyDeviceToHost, stream));
+    }
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return PSG_OK;
+  }
+
+  int download_phys(double* const* out) {
+    const long nr = (long)g.n * g.n * g.n;
+    double* tmp = nullptr;
+    PSG_CUDA_TRY(cudaMalloc(&tmp, sizeof(double) * nr));
+    for (int q = 0; q < 3; ++q) {
+      real_to_double<T><<<592, 256, 0, stream>>>(dump + q * nr, tmp, nr);
+      ++launches;
+      cudaError_t e = cudaMemcpyAsync(out[q], tmp, sizeof(double) * nr, cudaMemcpyDeviceToHost, stream);
+      if (e != cudaSuccess) { cudaFree(tmp); PSG_CUDA_TRY(e); }
+    }
+    cudaError_t e = cudaStreamSynchronize(stream);
+    cudaFree(tmp);
+    PSG_CUDA_TRY(e);
+    return PSG_OK;
+  }
+};
+
+}  // namespace psg
+
+// ---------------------------------------------------------------------------
+// C API (include/psgpu.h)
+// ---------------------------------------------------------------------------
+using namespace psg;
+
+struct psg_ns3d {
+  int precision;  // 32 or 64
+  Engine3D<float> f;
+  Engine3D<double> d;
+};
+
+template <typename Fn>
+static int with_engine(psg_ns3d* h, Fn fn) {
+  if (!h) { psg_set_error("null handle"); return PSG_ERR_ARG; }
+  if (h->precision == 64) return fn(h->d);
+  return fn(h->f);
+}
+
+extern "C" int psg_ns3d_create(psg_ns3d** out, int n, double alpha, int scheme, int precision) {
+  if (!out) { psg_set_error("null output handle"); return PSG_ERR_ARG; }
+  *out = nullptr;
+  if (scheme < 0 || scheme > 3) { psg_set_error("unknown scheme %d", scheme); return PSG_ERR_ARG; }
+  if (precision != 32 && precision != 64) { psg_set_error("precision must be 32 or 64"); return PSG_ERR_ARG; }
+  if (alpha != 1.0) {
+    psg_set_error("aspect ratio alpha=%g unsupported: the box must be cubic", alpha);
+    return PSG_ERR_UNSUPPORTED;
+  }
+  psg_ns3d* h = new psg_ns3d();
+  h->precision = precision;
+  int rc = (precision == 64) ? h->d.init(n, alpha, scheme) : h->f.init(n, alpha, scheme);
+  if (rc) { h->f.release(); h->d.release(); delete h; return rc; }
+  *out = h;
+  return PSG_OK;
+}
+
+extern "C" void psg_ns3d_destroy(psg_ns3d* h) {
+  if (!h) return;
+  h->f.release();
+  h->d.release();
+  delete h;
+}
+
+extern "C" int psg_ns3d_set_params(psg_ns3d* h, double nu, double ampfor, double kf, double ri,
+                                   double sc, double theta) {
+  return with_engine(h, [&](auto& e) {
+    using T = typename std::remove_reference<decltype(e.prm.dt)>::type;
+    e.prm.nu = (T)nu; e.prm.ampfor = (T)ampfor; e.prm.kf = (T)kf; e.prm.ri = (T)ri;
+    e.prm.sc = (T)sc; e.prm.sinth = (T)sin(theta); e.prm.costh = (T)cos(theta);
+    return PSG_OK;
+  });
+}
+
+extern "C" int psg_ns3d_set_stream(psg_ns3d* h, void* stream) {
+  return with_engine(h, [&](auto& e) { e.stream = (cudaStream_t)stream; return PSG_OK; });
+}
+
+extern "C" int psg_ns3d_upload(psg_ns3d* h, const double* const* comps) {
+  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
+  return with_engine(h, [&](auto& e) { return e.upload(comps); });
+}
+
+extern "C" int psg_ns3d_download(psg_ns3d* h, double* const* comps) {
+  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
+  return with_engine(h, [&](auto& e) { return e.download(comps); });
+}
+
+extern "C" int psg_ns3d_download_stage(psg_ns3d* h, double* const* comps) {
+  return with_engine(h, [&](auto& e) {
+    if (!e.R.X0.c[0]) { psg_set_error("scheme keeps no stage state"); return PSG_ERR_STATE; }
+    return e.download(comps, &e.R.X0);
+  });
+}
+
+extern "C" int psg_ns3d_step(psg_ns3d* h, double dt, int nsteps, int dump_last) {
+  if (nsteps < 0) { psg_set_error("negative step count"); return PSG_ERR_ARG; }
+  return with_engine(h, [&](auto& e) {
+    using T = typename std::remove_reference<decltype(e.prm.dt)>::type;
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = e.step((T)dt, dump_last && s == nsteps - 1);
+      if (rc) return rc;
+    }
+    return PSG_OK;
+  });
+}
+
+extern "C" int psg_ns3d_timederiv(psg_ns3d* h, double* const* out) {
+  return with_engine(h, [&](auto& e) {
+    if (e.scheme != SCHEME_BOUS_RK4 && e.scheme != SCHEME_NS_RK4) {
+      psg_set_error("time derivative is defined for the RK4 schemes");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    int rc = e.rhs(STAGE_DERIV);
+    if (rc) return rc;
+    return e.download(out, &e.R.K1);
+  });
+}
+
+extern "C" int psg_ns3d_download_phys(psg_ns3d* h, double* const* out) {
+  return with_engine(h, [&](auto& e) {
+    if (!e.dump) { psg_set_error("scheme keeps no physical fields"); return PSG_ERR_STATE; }
+    return e.download_phys(out);
+  });
+}
+
+extern "C" int psg_ns3d_sync(psg_ns3d* h) {
+  return with_engine(h, [&](auto& e) {
+    PSG_CUDA_TRY(cudaStreamSynchronize(e.stream));
+    return PSG_OK;
+  });
+}
+
+extern "C" long psg_ns3d_launches(psg_ns3d* h) {
+  if (!h) return -1;
+  return h->precision == 64 ? h->d.launches : h->f.launches;
+}
+
+// device pointers of the state components, for callers that keep the state
+// resident (layout: [2K+1][2K+1][XP] complex of the engine's precision)
+extern "C" int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps) {
+  return with_engine(h, [&](auto& e) {
+    if (xp) *xp = e.g.XP;
+    if (comps)
+      for (int q = 0; q < 4; ++q) comps[q] = (void*)e.R.S.c[q];
+    return PSG_OK;
+  });
+}

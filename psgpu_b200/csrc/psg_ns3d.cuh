@@ -1,0 +1,64 @@
+// psg_ns3d.cuh -- the 3D pseudospectral right-hand side as five fused passes.
+//
+// State layout in HBM (per component, complex T):
+//   S[ikz][iky][ikx], ikz,iky in [0, 2K], ikx in [0, XP) with XP = IKTX rounded
+//   up to the tile width (padding columns hold zeros).  This is the
+//   reference's truncated box (kx fastest, 3D_NavierStokes/src/init.F90:25-36)
+//   with padded rows so that every tile row is an aligned 64-byte segment.
+//
+// One evaluation of N(w) = curl(u x w) (plus buoyancy / density advection for
+// the Boussinesq system) is
+//   A  z-inverse  : stage state -> {w, u = i k x w / k^2 (, i k rho)}   [f][z][ky][kx]
+//   B  y-inverse  :                                                      [f][z][y][kx]
+//   C  x-pass     : C2R -> -(u x w) (, u.grad rho) -> R2C, scaled 1/N^3   [g][z][y][kx]
+//   D  y-forward  :                                                      [g][z][ky][kx]
+//   E  z-forward  : + curl, forcing, buoyancy and the time-scheme update  -> state
+// Passes A, B, D and E transform tiles of W adjacent kx columns along a
+// strided axis; pass C transforms whole x rows, one row per thread group.
+// Truncated modes are never loaded in the inverse direction and never
+// produced in the forward direction.
+#pragma once
+#include "psg_common.cuh"
+#include "psg_fft.cuh"
+
+namespace psg {
+
+enum Scheme3D : int {
+  SCHEME_NS_HEUN = 0,     // 3D_NavierStokes/src/kernels.h:309-464
+  SCHEME_EULER_HEUN = 1,  // 3D_Euler/src/kernels.h:296-439
+  SCHEME_NS_RK4 = 2,      // 3D_Boussinesq/src/kernels.h:331-621 without density
+  SCHEME_BOUS_RK4 = 3,    // 3D_Boussinesq/src/kernels.h:331-621
+};
+
+// stage codes of pass E
+enum StageCode : int {
+  STAGE_HEUN_PRED = 0,
+  STAGE_HEUN_CORR = 1,
+  STAGE_RK1 = 2,
+  STAGE_RK2 = 3,
+  STAGE_RK3 = 4,
+  STAGE_RK4 = 5,
+  STAGE_DERIV = 6,  // dz/dt into K1 (3D_Boussinesq/src/kernels.h:624-692)
+};
+
+template <typename T>
+struct Geom3 {
+  int n, K, X, Y, XP;
+  T alpha;
+};
+
+template <typename T>
+struct StepParams {
+  T dt;      // step length
+  T nu;      // viscosity (1/Re)
+  T ampfor;  // forcing amplitude (the reference's d_AMPFOR)
+  T kf;      // forcing wavenumber
+  T ri, sc, sinth, costh;  // Boussinesq parameters
+};
+
+template <typename T>
+struct Fields4 {
+  cpx<T>* c[4];
+};
+
+}  // namespace psg
