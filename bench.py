@@ -1,0 +1,393 @@
+"""Benchmark: 3D Navier-Stokes 256^3 RK4/CN steps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (per GPU): the Taylor-Green vortex u = (sin x cos y cos z,
+-cos x sin y cos z, 0) on [0, 2pi]^3 plus a seeded divergence-free
+perturbation of amplitude 1e-3 on |k| <= 4, nu = 1/1600, dt = 1e-3, 256^3 grid,
+2/3 dealiasing, RK4 with per-stage Crank-Nicolson factors (the reference's RK4
+scheme, 3D_Boussinesq/src/kernels.h:331-621, at Ri = 0).  Data are synthetic
+(seeded initial field).  A step is one full RK4 step (four right-hand sides).
+
+* ``value``: steps/s with the state resident in HBM (FP32 storage and
+  transforms, vorticity only), all ranks' steps / max-over-ranks device time.
+* ``e2e``: the same metric through the reference-facing C ABI
+  (libpsg_bous3d.so ``timestep_cuda_``, Ri = 0, FP64 host arrays in pinned
+  memory) with the host<->device copies of every call inside the timed region,
+  10 steps per call.
+* ``--impl reference``: the reference's own CUDA step built from its sources
+  (oracle/_ref/libref_bous3d.so, FP64 cuFFT), driven by the same calls.
+* ``cpu_baseline``: the FP64 CPU oracle (C + OpenMP on all host threads) on a
+  bounded sample of the same workload (one RK4 step of the same scheme).
+* ``roofline``: the dominant pass (largest share of the step's device time),
+  its algorithmic HBM bytes per launch over its average CUDA-event duration,
+  against the measured copy bandwidth in MEASURED_PEAKS.json.
+
+The device working set (state, stage registers, transform buffers: ~0.8 GB)
+is far larger than the 126 MB L2, so every pass streams from HBM; no L2 flush
+is needed between steps.  Multi-GPU runs are independent replicas (a single
+256^3 field is not split across GPUs), scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+NU = 1.0 / 1600.0
+DT = 1e-3
+STEPS_PER_CALL = 10
+METRIC = "3D NS 256^3 RK4/CN steps/s (Taylor-Green, FP32, 1 B200 per replica)"
+
+
+# ---------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(n, word=8):
+    """HBM bytes of one right-hand side per pass, complex words of `word` bytes,
+    counting only kept modes (IKTX = n/3+1 columns, IKTY = IKTZ = 2(n/3)+1 rows)
+    and one read plus one write per pass; pass A also reads the 3 stage-state
+    components, pass E writes/reads the scheme registers (counted per stage in
+    stage_bytes)."""
+    K = n // 3
+    X, Y = K + 1, 2 * K + 1
+    a = (3 * X * Y * Y + 6 * X * Y * n) * word
+    b = (6 * X * Y * n + 6 * X * n * n) * word
+    c = (6 * X * n * n + 3 * X * n * n) * word
+    d = (3 * X * n * n + 3 * X * Y * n) * word
+    e = (3 * X * Y * n) * word
+    return [a, b, c, d, e]
+
+
+def stage_bytes(n, stage, word=8):
+    """state/register traffic of pass E for RK4 stage 0..3 (3 components each):
+    stages 0-2 read S and write K_s and X0; the final stage reads S, K1, K2, K3
+    and writes S and X0."""
+    K = n // 3
+    nkt = (K + 1) * (2 * K + 1) ** 2
+    arrays = 3 if stage < 3 else 6
+    return arrays * 3 * nkt * word
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, dist):
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import taylor_green3d
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    xi, et, zt = taylor_green3d(N, 1234 + rank, amp=1e-3)
+    eng = P.NS3D(N, P.SCHEME_NS_RK4, precision=32, nu=NU)
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    eng.upload(xi, et, zt)
+    for _ in range(args.warmup):
+        eng.step(DT, 1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(dev.index)
+    clk.start()
+    l0 = eng.launches
+    eng.profile(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.step(DT, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = eng.launches - l0
+    prof = eng.profile_read()
+    eng.profile(False)
+    clocks = clk.stop()
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1e3)
+
+    # roofline of the dominant pass
+    peak, peak_kind = measured_peaks()
+    alg = algorithmic_bytes(N, 8)
+    per_step_stage = sum(stage_bytes(N, s) for s in range(4)) / 4.0
+    shares = {}
+    tot = sum(v[0] for v in prof.values())
+    roof = None
+    for i, (name, (pms, cnt)) in enumerate(prof.items()):
+        shares[name] = round(pms / tot, 4) if tot else None
+    dom_i = max(range(5), key=lambda i: list(prof.values())[i][0])
+    dom_name = list(prof.keys())[dom_i]
+    dom_ms, dom_cnt = list(prof.values())[dom_i]
+    dom_bytes = alg[dom_i] + (per_step_stage if dom_i == 4 else 0)
+    achieved = dom_bytes / (dom_ms / dom_cnt / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get(dom_name)
+    roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
+            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes": int(dom_bytes), "avg_launch_ms": round(dom_ms / dom_cnt, 5),
+            "pass_share": shares}
+    step_bytes = 4 * sum(alg) + sum(stage_bytes(N, s) for s in range(4))
+    whole = {"algorithmic_bytes_per_step": int(step_bytes),
+             "achieved_GBps": round(step_bytes / (ms / args.steps / 1e3) / 1e9, 1)}
+    whole["frac"] = round(whole["achieved_GBps"] / peak, 4)
+
+    # e2e through the reference-facing C ABI with host buffers
+    e2e = run_e2e(args, dev, dist, world, rank)
+    eng.close()
+
+    out = None
+    if rank == 0:
+        cpu = cpu_baseline() if world == 1 and not args.no_cpu else None
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3D NS 256^3 Taylor-Green, RK4/CN (Boussinesq scheme, Ri=0), "
+                                   "nu=1/1600, dt=1e-3, 2/3 dealias",
+                       "grid": N, "replicas": world, "parallelism": f"replicas{world}",
+                       "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
+            "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu,
+            "clocks": clocks, "gpu_launches": int(launches),
+        }
+    return out
+
+
+def run_e2e(args, dev, dist, world, rank):
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import taylor_green3d
+
+    os.environ["PSG_PRECISION"] = "32"
+    lib = TimestepLibrary(P.dropin_path("bous3d"), "bous3d")
+    return time_abi_calls(lib, args, dev, dist, world, rank, ours=True)
+
+
+def time_abi_calls(lib, args, dev, dist, world, rank, ours):
+    """K steps in calls of STEPS_PER_CALL through timestep_cuda_ with pinned host
+    arrays; the copies in and out of every call are inside the timed region."""
+    import torch
+    from psgpu_b200.fields import Grid3D, taylor_green3d
+
+    g = Grid3D(N)
+    xi, et, zt = taylor_green3d(N, 1234 + rank, amp=1e-3)
+    comps = []
+    for a in (xi, et, zt, np.zeros_like(xi)):
+        t = torch.empty(g.nkt * 2, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = a.view(np.float64).ravel()
+        comps.append(t.numpy().view(np.complex128).reshape(g.shape))
+    calls = max(1, args.steps // STEPS_PER_CALL)
+    wcalls = max(1, args.warmup // STEPS_PER_CALL)
+    tend = STEPS_PER_CALL * DT
+    per_call = rk4_evaluations(0.0, tend, DT)
+
+    def call():
+        lib.bous3d_inplace(comps, N, NU, DT, tend)
+
+    for _ in range(wcalls):
+        call()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        call()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    steps = calls * per_call
+    nbytes = 4 * g.nkt * 16
+    return {"value": round(world * steps / sec, 3), "unit": "steps/s",
+            "h2d_bytes_per_step": int(nbytes / per_call) if ours else 0,
+            "d2h_bytes_per_step": int(nbytes / per_call) if ours else 0,
+            "steps_per_call": per_call, "calls": calls,
+            "api": "timestep_cuda_ (3D Boussinesq ABI, Ri=0, FP64 host arrays)"}
+
+
+def rk4_evaluations(tstart, tend, dt):
+    """RK4 steps one Boussinesq call takes: full steps while tend - t > dt, then
+    one adjusted step if t != tend (3D_Boussinesq/src/src_gmres/cuda.cu:187-250)."""
+    t, n = tstart, 0
+    while tend - t > dt:
+        n += 1
+        t += dt
+    return n + (1 if t != tend else 0)
+
+
+def cpu_baseline():
+    """One RK4/CN step of the same workload on the host cores, FP64 oracle."""
+    from oracle import pyoracle as O
+    from psgpu_b200.fields import taylor_green3d
+
+    xi, et, zt = taylor_green3d(N, 1234, amp=1e-3)
+    t0 = time.perf_counter()
+    O.bous3d_timestep(xi, et, zt, np.zeros_like(xi), N, NU, DT, 2 * DT)
+    sec = time.perf_counter() - t0
+    nsteps = rk4_evaluations(0.0, 2 * DT, DT)
+    return {"value": round(nsteps / sec, 5), "unit": "steps/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"{nsteps} RK4/CN steps of the 256^3 Taylor-Green workload, FP64, "
+                      "Boussinesq scheme at Ri=0 (density carried), oracle C code"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank, world, dist):
+    import torch
+    from psgpu_b200.abi import TimestepLibrary
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_bous3d.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_bous3d.so not built"}
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = TimestepLibrary(path, "bous3d")
+    clk = ClockSampler(dev.index)
+    clk.start()
+    e2e = time_abi_calls(lib, args, dev, dist, world, rank, ours=False)
+    clocks = clk.stop()
+    if rank != 0:
+        return None
+    v = e2e["value"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * world / v, 4) if v else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3D NS 256^3 Taylor-Green, RK4/CN (Boussinesq scheme, Ri=0), "
+                               "nu=1/1600, dt=1e-3, 2/3 dealias",
+                   "grid": N, "replicas": world, "parallelism": f"replicas{world}",
+                   "implementation": "reference timestep_cuda_ (3D_Boussinesq/src/src_gmres/"
+                                     "cuda.cu) built unmodified for sm_100a, FP64 cuFFT"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
+                         "sample": "the reference has no host implementation of this step; "
+                                   "this arm runs its CUDA step on the GPU, "
+                                   f"{e2e['steps_per_call']} steps per call"},
+        "clocks": clocks,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        # rank 0 alone times the reference; the other ranks exit without work
+        if rank != 0:
+            return
+        out = run_reference(args, 0, 1, None)
+        if out is not None:
+            out["n_gpus"] = world
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        out = run_ours(args, rank, world, dist)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -37,6 +37,10 @@ extern "C" {
 const char* psg_last_error(void);
 void psg_clear_error(void);
 int psg_version(void);
+/* building-block check: the library's line FFT on nlines contiguous lines of n
+ * complex doubles (in -> out), unnormalised, sign -1 forward / +1 inverse;
+ * swap selects the transposed factorisation used after another transform */
+int psg_debug_linefft(int n, int sign, int swap, const double* in, double* out, int nlines);
 
 /* ---------------------------------------------------------------- 3D */
 typedef struct psg_ns3d psg_ns3d;
@@ -66,6 +70,34 @@ int psg_ns3d_sync(psg_ns3d* h);
 long psg_ns3d_launches(psg_ns3d* h);
 /* device state pointers and padded row length (complex words) */
 int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps);
+/* per-pass timing: enable(1) resets and records CUDA events between the five
+ * passes of every right-hand side; read returns total ms and launch counts of
+ * passes A..E (z-inverse, y-inverse, x, y-forward, z-forward + update) */
+int psg_ns3d_profile(psg_ns3d* h, int enable);
+int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts);
+
+/* ---------------------------------------------------------------- 2D */
+/* A batch of independent 2D Kolmogorov-flow instances (sizes 16..256, any
+ * mix) integrated by one persistent launch: one thread block per instance,
+ * largest first.  The scheme is the reference's 2D RK4 step with the final
+ * Crank-Nicolson viscous factor and the forcing -2 at (kx,ky) = (0,+-4)
+ * (2D_NavierStokes/src_RK4/kernels.h:112-435).  The single-instance drop-in
+ * libpsg_ns2d.so is a batch of one. */
+typedef struct psg_batch2d psg_batch2d;
+
+int psg_batch2d_create(psg_batch2d** h, int ninst, const int* sizes, int precision);
+void psg_batch2d_destroy(psg_batch2d* h);
+int psg_batch2d_set_stream(psg_batch2d* h, void* cuda_stream);
+/* Z: complex128 box [2K+1][K+1] of instance i (reference layout) */
+int psg_batch2d_upload(psg_batch2d* h, int i, const double* Z);
+int psg_batch2d_download(psg_batch2d* h, int i, double* Z);
+/* enqueue nsteps[i] steps of length dt[i] with viscosity nu[i] for every
+ * instance, in one kernel launch on the handle's stream */
+int psg_batch2d_run(psg_batch2d* h, const double* nu, const double* dt, const int* nsteps);
+int psg_batch2d_sync(psg_batch2d* h);
+long psg_batch2d_launches(psg_batch2d* h);
+/* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]) */
+int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,255 @@
+"""psgpu_b200 -- B200-native pseudospectral time step for periodic-box flows.
+
+Python host side of the CUDA layer (``psgpu_b200/lib/libpsgpu.so``).  The
+library is required: there is no CPU fallback, and every entry point raises
+if the shared object is missing or a CUDA call fails.
+
+The reference-compatible ``timestep_cuda_`` entry points live in the drop-in
+libraries ``lib/libpsg_<flavour>.so`` and are driven through
+:class:`psgpu_b200.abi.TimestepLibrary`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .fields import Grid2D, Grid3D  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+CORE = os.path.join(LIBDIR, "libpsgpu.so")
+
+SCHEME_NS_HEUN = 0
+SCHEME_EULER_HEUN = 1
+SCHEME_NS_RK4 = 2
+SCHEME_BOUS_RK4 = 3
+
+_lib = None
+
+
+class PsgError(RuntimeError):
+    pass
+
+
+def dropin_path(flavour: str) -> str:
+    p = os.path.join(LIBDIR, f"libpsg_{flavour}.so")
+    if not os.path.exists(p):
+        raise PsgError(f"drop-in library {p} is not built (run python -m psgpu_b200.build)")
+    return p
+
+
+def lib():
+    """Load libpsgpu.so (raises PsgError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(CORE):
+        raise PsgError(f"{CORE} is not built; run `python -m psgpu_b200.build`")
+    L = C.CDLL(CORE, mode=C.RTLD_GLOBAL)
+    vp, ip, d, i = C.c_void_p, C.c_int, C.c_double, C.c_int
+    pp = C.POINTER(C.c_void_p)
+    L.psg_last_error.restype = C.c_char_p
+    L.psg_version.restype = i
+    L.psg_debug_linefft.argtypes = [i, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double), i]
+    L.psg_ns3d_create.argtypes = [C.POINTER(vp), i, d, i, i]
+    L.psg_ns3d_destroy.argtypes = [vp]
+    L.psg_ns3d_destroy.restype = None
+    L.psg_ns3d_set_params.argtypes = [vp, d, d, d, d, d, d]
+    L.psg_ns3d_set_stream.argtypes = [vp, vp]
+    L.psg_ns3d_upload.argtypes = [vp, pp]
+    L.psg_ns3d_download.argtypes = [vp, pp]
+    L.psg_ns3d_download_stage.argtypes = [vp, pp]
+    L.psg_ns3d_step.argtypes = [vp, d, i, i]
+    L.psg_ns3d_timederiv.argtypes = [vp, pp]
+    L.psg_ns3d_download_phys.argtypes = [vp, pp]
+    L.psg_ns3d_sync.argtypes = [vp]
+    L.psg_ns3d_launches.argtypes = [vp]
+    L.psg_ns3d_launches.restype = C.c_long
+    L.psg_ns3d_layout.argtypes = [vp, C.POINTER(ip), pp]
+    L.psg_ns3d_profile.argtypes = [vp, i]
+    L.psg_ns3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    _declare_2d(L)
+    _lib = L
+    return L
+
+
+def _declare_2d(L):
+    vp, i = C.c_void_p, C.c_int
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    L.psg_batch2d_create.argtypes = [C.POINTER(vp), i, ip, i]
+    L.psg_batch2d_destroy.argtypes = [vp]
+    L.psg_batch2d_destroy.restype = None
+    L.psg_batch2d_set_stream.argtypes = [vp, vp]
+    L.psg_batch2d_upload.argtypes = [vp, i, dp]
+    L.psg_batch2d_download.argtypes = [vp, i, dp]
+    L.psg_batch2d_run.argtypes = [vp, dp, dp, ip]
+    L.psg_batch2d_sync.argtypes = [vp]
+    L.psg_batch2d_launches.argtypes = [vp]
+    L.psg_batch2d_launches.restype = C.c_long
+    L.psg_batch2d_device_state.argtypes = [vp, i, C.POINTER(vp)]
+
+
+def _check(rc):
+    if rc != 0:
+        raise PsgError(lib().psg_last_error().decode(errors="replace"))
+
+
+def _ptrs(arrays):
+    arr = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    return C.cast(arr, C.POINTER(C.c_void_p))
+
+
+class NS3D:
+    """Persistent 3D instance: device buffers and state stay in HBM across calls.
+
+    scheme: SCHEME_NS_HEUN (3D NS DNS build), SCHEME_EULER_HEUN, SCHEME_NS_RK4
+    (the Boussinesq RK4/CN scheme without density), SCHEME_BOUS_RK4.
+    precision: 32 or 64.
+    """
+
+    def __init__(self, n: int, scheme: int = SCHEME_NS_RK4, precision: int = 32,
+                 nu: float = 0.0, ampfor: float = 0.0, kf: float = 4.0, ri: float = 0.0,
+                 sc: float = 1.0, theta: float = 0.0):
+        L = lib()
+        h = C.c_void_p()
+        _check(L.psg_ns3d_create(C.byref(h), n, 1.0, scheme, precision))
+        self._h = h
+        self.n = n
+        self.grid = Grid3D(n)
+        self.scheme = scheme
+        self.precision = precision
+        self.ncomp = 4 if scheme == SCHEME_BOUS_RK4 else 3
+        self.set_params(nu, ampfor, kf, ri, sc, theta)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().psg_ns3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, nu, ampfor=0.0, kf=4.0, ri=0.0, sc=1.0, theta=0.0):
+        _check(lib().psg_ns3d_set_params(self._h, nu, ampfor, kf, ri, sc, theta))
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().psg_ns3d_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def upload(self, *comps):
+        if len(comps) != self.ncomp:
+            raise ValueError(f"expected {self.ncomp} components")
+        arrs = [np.ascontiguousarray(c, dtype=np.complex128).reshape(-1) for c in comps]
+        for a in arrs:
+            if a.size != self.grid.nkt:
+                raise ValueError("component size does not match the grid")
+        _check(lib().psg_ns3d_upload(self._h, _ptrs(arrs)))
+
+    def download(self, stage: bool = False):
+        out = [np.zeros(self.grid.shape, np.complex128) for _ in range(self.ncomp)]
+        fn = lib().psg_ns3d_download_stage if stage else lib().psg_ns3d_download
+        _check(fn(self._h, _ptrs(out)))
+        return tuple(out)
+
+    def step(self, dt: float, nsteps: int = 1, dump_last: bool = False):
+        _check(lib().psg_ns3d_step(self._h, dt, nsteps, int(dump_last)))
+
+    def timederiv(self):
+        out = [np.zeros(self.grid.shape, np.complex128) for _ in range(self.ncomp)]
+        _check(lib().psg_ns3d_timederiv(self._h, _ptrs(out)))
+        return tuple(out)
+
+    def physical(self):
+        n = self.n
+        out = [np.zeros(n * n * n) for _ in range(3)]
+        _check(lib().psg_ns3d_download_phys(self._h, _ptrs(out)))
+        return np.stack([o.reshape(n, n, n) for o in out])
+
+    def sync(self):
+        _check(lib().psg_ns3d_sync(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().psg_ns3d_launches(self._h))
+
+    PASSES = ("z-inverse", "y-inverse", "x-pass", "y-forward", "z-forward+update")
+
+    def profile(self, enable: bool = True):
+        _check(lib().psg_ns3d_profile(self._h, int(enable)))
+
+    def profile_read(self):
+        ms = (C.c_double * 5)()
+        cnt = (C.c_long * 5)()
+        _check(lib().psg_ns3d_profile_read(self._h, ms, cnt))
+        return {p: (ms[i], cnt[i]) for i, p in enumerate(self.PASSES)}
+
+    def device_state(self):
+        xp = C.c_int()
+        ptrs = (C.c_void_p * 4)()
+        _check(lib().psg_ns3d_layout(self._h, C.byref(xp), C.cast(ptrs, C.POINTER(C.c_void_p))))
+        return xp.value, [ptrs[i] for i in range(self.ncomp)]
+
+
+class Batch2D:
+    """Independent 2D Kolmogorov-flow instances of mixed sizes, integrated by one
+    persistent kernel launch (one thread block per instance)."""
+
+    def __init__(self, sizes, precision: int = 32):
+        L = lib()
+        self.sizes = [int(s) for s in sizes]
+        arr = (C.c_int * len(self.sizes))(*self.sizes)
+        h = C.c_void_p()
+        _check(L.psg_batch2d_create(C.byref(h), len(self.sizes), arr, precision))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().psg_batch2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().psg_batch2d_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def upload(self, i: int, Z):
+        g = Grid2D(self.sizes[i])
+        a = np.ascontiguousarray(Z, dtype=np.complex128).reshape(-1)
+        if a.size != g.nkt:
+            raise ValueError("state size does not match the instance grid")
+        _check(lib().psg_batch2d_upload(self._h, i, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def download(self, i: int):
+        g = Grid2D(self.sizes[i])
+        a = np.zeros(g.shape, np.complex128)
+        _check(lib().psg_batch2d_download(self._h, i, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def run(self, nu, dt, nsteps):
+        m = len(self.sizes)
+        nu = np.broadcast_to(np.asarray(nu, np.float64), (m,)).copy()
+        dt = np.broadcast_to(np.asarray(dt, np.float64), (m,)).copy()
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (m,)).copy()
+        _check(lib().psg_batch2d_run(self._h, nu.ctypes.data_as(C.POINTER(C.c_double)),
+                                     dt.ctypes.data_as(C.POINTER(C.c_double)),
+                                     ns.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def sync(self):
+        _check(lib().psg_batch2d_sync(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().psg_batch2d_launches(self._h))

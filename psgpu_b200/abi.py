@@ -151,6 +151,29 @@ class TimestepLibrary:
                 _i(0), _i(0), _i(0), _i(0))
         return xii, eta, zet, rho, float(t[0])
 
+    def bous3d_inplace(self, comps, n, nu, dt, tend, ri=0.0, sc=1.0, theta=0.0, ampfor=0.0,
+                       kf=4, tstart=0.0, alpha=1.0):
+        """The Boussinesq call on caller-owned arrays (complex128 boxes, e.g. in
+        pinned memory), overwritten in place; the driver-side argument arrays are
+        built once per grid and cached.  Returns the advanced time."""
+        key = (n, alpha)
+        cache = getattr(self, "_args3", {})
+        if key not in cache:
+            cache[key] = self._grid3(n, alpha)
+            self._args3 = cache
+        g, kx, ky, kz, LC, ikF, ikN = cache[key]
+        for a in comps:
+            if a.dtype != np.complex128 or a.size != g.nkt or not a.flags.c_contiguous:
+                raise ValueError("state arrays must be contiguous complex128 boxes")
+        t = np.zeros(1)
+        self.fn(*[_pd(a.view(np.float64)) for a in comps],
+                _pd(kx), _pd(ky), _pd(kz), _pd(t), _d(tstart), _d(tend), _d(ampfor),
+                _d(dt), _d(1.0), _d(float(kf)), _d(nu), _d(ri), _d(sc), _d(theta),
+                _d(alpha), _d(0.0), _pi(ikF), _pi(ikN), _pi(LC), _i(g.iktx), _i(g.ikty),
+                _i(g.iktz), _i(g.kt), _i(g.nkt), _i(n), _i(n), _i(n), _i(1), _i(1),
+                _i(0), _i(0), _i(0), _i(0))
+        return float(t[0])
+
     def bous3d_timederiv(self, xii, eta, zet, rho, n, nu, ri=0.0, sc=1.0, theta=0.0,
                          ampfor=0.0, kf=4, alpha=1.0):
         """dz/dt of the Boussinesq system.  Signature as timestep_cuda_ of the same

@@ -1,0 +1,101 @@
+"""In-tree build of the CUDA layer for sm_100a.
+
+    python -m psgpu_b200.build          # or psgpu_b200.build.build()
+
+Produces (git-ignored, shipped with the tree):
+  psgpu_b200/lib/libpsgpu.so          engines + re-entrant C API (include/psgpu.h)
+  psgpu_b200/lib/libpsg_<flavour>.so  reference-compatible timestep_cuda_ drop-ins
+                                      (include/psgpu_ref_abi.h), linked to libpsgpu.so
+Objects are rebuilt only when a source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "lib")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+         "--ptxas-options=-O3", f"-I{INCLUDE}", f"-I{CSRC}"]
+
+# translation units of libpsgpu.so
+CORE = ["psg_api.cu", "psg_ns3d_api.cu", "psg_ns3d_f32.cu", "psg_ns3d_f64.cu",
+        "psg_ns2d.cu"]
+# drop-in libraries: name -> (source, macro)
+DROPINS = {
+    "ns3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D"),
+    "euler3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_EULER3D"),
+    "bous3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_BOUS3D"),
+    "ns2d": ("psg_dropin2d.cu", "PSG_FLAVOUR_NS2D"),
+}
+
+
+def _headers():
+    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    hs += glob.glob(os.path.join(INCLUDE, "*.h"))
+    return max((os.path.getmtime(h) for h in hs), default=0.0)
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources) or _headers() > t
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r
+
+
+def _compile(src, obj, defines=()):
+    srcp = os.path.join(CSRC, src)
+    if not _stale(obj, [srcp]):
+        return obj
+    cmd = [NVCC, *ARCH, *FLAGS, *[f"-D{d}" for d in defines], "-c", srcp, "-o", obj]
+    _run(cmd)
+    return obj
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(LIB, exist_ok=True)
+    jobs = []
+    core = [s for s in CORE if os.path.exists(os.path.join(CSRC, s))]
+    dropins = {k: v for k, v in DROPINS.items() if os.path.exists(os.path.join(CSRC, v[0]))}
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        for s in core:
+            jobs.append(ex.submit(_compile, s, os.path.join(OBJ, s.replace(".cu", ".o"))))
+        for name, (s, macro) in dropins.items():
+            jobs.append(ex.submit(_compile, s, os.path.join(OBJ, f"dropin_{name}.o"), (macro,)))
+        for j in jobs:
+            j.result()
+    core_objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in core]
+    libcore = os.path.join(LIB, "libpsgpu.so")
+    if _stale(libcore, core_objs):
+        _run([NVCC, *ARCH, "-shared", "-o", libcore, *core_objs, "-lcudart"])
+    for name in dropins:
+        obj = os.path.join(OBJ, f"dropin_{name}.o")
+        out = os.path.join(LIB, f"libpsg_{name}.so")
+        if _stale(out, [obj, libcore]):
+            _run([NVCC, *ARCH, "-shared", "-o", out, obj, f"-L{LIB}", "-lpsgpu", "-lcudart",
+                  "-Xlinker", "-rpath,$ORIGIN"])
+    if verbose:
+        print("built", libcore)
+    return libcore
+
+
+if __name__ == "__main__":
+    build(verbose=True)
+    sys.exit(0)

@@ -1,0 +1,81 @@
+// psg_dropin2d.cu -- reference-compatible timestep_cuda_ of the 2D flavour
+// (libpsg_ns2d.so).  Same argument list as
+// 2D_NavierStokes/src_RK4/src_gmres/cuda.cu:16-34; Z is overwritten with the
+// state after NSTOP RK4/CN steps and *Time = NSTOP*DELT (accumulated as the
+// reference does).  The Kolmogorov forcing (-2 at kx = 0, |ky| = 4) is part of
+// the scheme, as in the reference.  Device buffers persist between calls.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime.h>
+
+#include "../../include/psgpu.h"
+#include "../../include/psgpu_ref_abi.h"
+
+extern "C" {
+typedef struct psg_batch2d psg_batch2d;
+int psg_batch2d_create(psg_batch2d** out, int ninst, const int* sizes, int precision);
+void psg_batch2d_destroy(psg_batch2d* h);
+int psg_batch2d_upload(psg_batch2d* h, int i, const double* Z);
+int psg_batch2d_download(psg_batch2d* h, int i, double* Z);
+int psg_batch2d_run(psg_batch2d* h, const double* nu, const double* dt, const int* nsteps);
+}
+
+namespace {
+psg_batch2d* g_h = nullptr;
+int g_n = 0, g_prec = 0;
+
+int env_precision() {
+  const char* s = getenv("PSG_PRECISION");
+  if (s && (!strcmp(s, "64") || !strcmp(s, "fp64"))) return 64;
+  return 32;
+}
+}  // namespace
+
+extern "C" void timestep_cuda_(double2* Z, double* ZR, double* kx, double* ky, double* Time,
+                               double* TSTART, double* TNEWT, double* DELT, double* alpha,
+                               double* V2, int* ikF, int* ikN, int* IKTX, int* IKTY, int* KTY,
+                               int* NX, int* NY, int* NSTOP, int* LC) {
+  (void)ZR; (void)kx; (void)ky; (void)TSTART; (void)TNEWT; (void)ikF; (void)ikN; (void)LC;
+  const int n = *NY, K = n / 3;
+  if (*NX != *NY || *alpha != 1.0 || *KTY != K || *IKTX != K + 1 || *IKTY != 2 * K + 1) {
+    fprintf(stderr, "psgpu_b200 timestep_cuda_: unsupported sizes NX=%d NY=%d IKTX=%d IKTY=%d KTY=%d alpha=%g\n",
+            *NX, *NY, *IKTX, *IKTY, *KTY, *alpha);
+    return;
+  }
+  const int prec = env_precision();
+  if (!g_h || g_n != n || g_prec != prec) {
+    if (g_h) psg_batch2d_destroy(g_h);
+    g_h = nullptr;
+    if (psg_batch2d_create(&g_h, 1, &n, prec)) {
+      fprintf(stderr, "psgpu_b200 timestep_cuda_: %s\n", psg_last_error());
+      g_h = nullptr;
+      return;
+    }
+    g_n = n; g_prec = prec;
+  }
+  const double nu = *V2, dt = *DELT;
+  const int ns = *NSTOP;
+  if (psg_batch2d_upload(g_h, 0, (const double*)Z) || psg_batch2d_run(g_h, &nu, &dt, &ns) ||
+      psg_batch2d_download(g_h, 0, (double*)Z)) {
+    fprintf(stderr, "psgpu_b200 timestep_cuda_: %s\n", psg_last_error());
+    return;
+  }
+  *Time = 0.0;
+  for (int i = 0; i < ns; ++i) *Time += dt;
+}
+
+// set_gpu_ of the 2D build reports the current device (2D_NavierStokes/src_RK4/functions.h:13-29)
+extern "C" void set_gpu_(int* go) {
+  (void)go;
+  int count = 0, dev = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    printf("cutil error: no devices supporting CUDA\n");
+    exit(-1);
+  }
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  printf("\n Using CUDA device %d: %s\n\n", dev, prop.name);
+}

@@ -1,0 +1,205 @@
+// psg_dropin3d.cu -- reference-compatible timestep_cuda_ entry points (3D).
+//
+// Compiled once per flavour (-DPSG_FLAVOUR_NS3D / _EULER3D / _BOUS3D) into
+// libpsg_<flavour>.so, because every flavour exports the same Fortran-mangled
+// symbol.  The argument lists are the reference's, all by pointer; the state
+// arrays are overwritten in place exactly as the reference does.  Unlike the
+// reference, device buffers persist between calls (one cached engine per grid
+// size), so a call costs one upload, the steps and one download.
+//
+// Precision: FP32 storage and transforms by default; PSG_PRECISION=64 in the
+// environment selects the FP64 engine.  Failures print one line to stderr and
+// leave the state arrays as they were (the reference has no error channel).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime.h>
+
+#include "../../include/psgpu.h"
+#include "../../include/psgpu_ref_abi.h"
+
+namespace {
+
+struct Cached {
+  psg_ns3d* h = nullptr;
+  int n = 0, scheme = -1, precision = 0;
+};
+Cached g_cache;
+
+int env_precision() {
+  const char* s = getenv("PSG_PRECISION");
+  if (s && (!strcmp(s, "64") || !strcmp(s, "fp64"))) return 64;
+  return 32;
+}
+
+void report(const char* where) {
+  fprintf(stderr, "psgpu_b200 %s: %s\n", where, psg_last_error());
+}
+
+psg_ns3d* engine(int n, int scheme) {
+  const int prec = env_precision();
+  if (g_cache.h && g_cache.n == n && g_cache.scheme == scheme && g_cache.precision == prec)
+    return g_cache.h;
+  if (g_cache.h) psg_ns3d_destroy(g_cache.h);
+  g_cache = Cached();
+  psg_ns3d* h = nullptr;
+  if (psg_ns3d_create(&h, n, 1.0, scheme, prec) != PSG_OK) return nullptr;
+  g_cache.h = h; g_cache.n = n; g_cache.scheme = scheme; g_cache.precision = prec;
+  return h;
+}
+
+// the sizes the drivers pass must describe a cubic 2/3-truncated box
+bool check_sizes(const char* who, int IKTX, int IKTY, int IKTZ, int KTZ, int NKT, int NX,
+                 int NY, int NZ, double alpha) {
+  const int K = NY / 3;
+  if (NX != NY || NY != NZ || alpha != 1.0 || IKTX != K + 1 || IKTY != 2 * K + 1 ||
+      IKTZ != 2 * K + 1 || KTZ != K || NKT != IKTX * IKTY * IKTZ) {
+    fprintf(stderr,
+            "psgpu_b200 %s: unsupported sizes NX=%d NY=%d NZ=%d IKTX=%d IKTY=%d IKTZ=%d KTZ=%d "
+            "NKT=%d alpha=%g (cubic 2/3-truncated boxes only)\n",
+            who, NX, NY, NZ, IKTX, IKTY, IKTZ, KTZ, NKT, alpha);
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+#if defined(PSG_FLAVOUR_NS3D)
+
+extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* xir, double* etr,
+                               double* ztr, double* nuzn, double* nu1, double* kx, double* ky,
+                               double* kz, double* Time, double* TSTART, double* AMPFOR,
+                               double* DELT, double* ResThresh, double* KFY, double* V2,
+                               double* alpha, int* ikF, int* ikN, int* LC, int* IKTX, int* IKTY,
+                               int* IKTZ, int* KTZ, int* NKT, int* NX, int* NY, int* NZ,
+                               int* NSTOP, int* NOUT, int* NOUTV, int* statsFLAG, int* RecFLAG,
+                               int* RANK) {
+  (void)nuzn; (void)nu1; (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)ikF; (void)ikN;
+  (void)LC; (void)NOUT; (void)NOUTV; (void)statsFLAG; (void)RecFLAG; (void)RANK;
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_NS_HEUN);
+  if (!h) { report("timestep_cuda_"); return; }
+  const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
+  double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
+  double* phys[3] = {xir, etr, ztr};
+  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, 0.0, 1.0, 0.0) ||
+      psg_ns3d_upload(h, in) || psg_ns3d_step(h, *DELT, *NSTOP, 1) || psg_ns3d_download(h, out) ||
+      (*NSTOP > 0 && psg_ns3d_download_phys(h, phys))) {
+    report("timestep_cuda_");
+    return;
+  }
+  if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
+}
+
+#elif defined(PSG_FLAVOUR_EULER3D)
+
+extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* xir, double* etr,
+                               double* ztr, double* kx, double* ky, double* kz, double* Time,
+                               double* TSTART, double* DELT, double* alpha, int* ikF, int* ikN,
+                               int* LC, int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT,
+                               int* NX, int* NY, int* NZ, int* NSTOP, int* NOUT, int* NOUTV,
+                               int* statsFLAG) {
+  (void)kx; (void)ky; (void)kz; (void)ikF; (void)ikN; (void)LC; (void)NOUT; (void)NOUTV;
+  (void)statsFLAG;
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_EULER_HEUN);
+  if (!h) { report("timestep_cuda_"); return; }
+  const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
+  double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
+  double* phys[3] = {xir, etr, ztr};
+  if (psg_ns3d_set_params(h, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0) || psg_ns3d_upload(h, in) ||
+      psg_ns3d_step(h, *DELT, *NSTOP, 1) || psg_ns3d_download(h, out) ||
+      (*NSTOP > 0 && psg_ns3d_download_phys(h, phys))) {
+    report("timestep_cuda_");
+    return;
+  }
+  if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
+}
+
+#elif defined(PSG_FLAVOUR_BOUS3D)
+
+// Integration from TSTART to Tstep with the reference's loop: full steps while
+// Tstep - t > dt, then one step of the remaining length
+// (3D_Boussinesq/src/src_gmres/cuda.cu:187-250).  *Time advances by dt per full step.
+extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
+                               double* ky, double* kz, double* Time, double* TSTART,
+                               double* Tstep, double* AMPFOR, double* DELT, double* ResThresh,
+                               double* KFY, double* V2, double* Ri, double* Sc, double* Theta,
+                               double* alpha, double* Dtarget, int* ikF, int* ikN, int* LC,
+                               int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT, int* NX,
+                               int* NY, int* NZ, int* NOUT, int* NOUTV, int* statsFLAG,
+                               int* RecFLAG, int* adaptFLAG, int* RANK) {
+  (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)Dtarget; (void)ikF; (void)ikN; (void)LC;
+  (void)NOUT; (void)NOUTV; (void)statsFLAG; (void)RecFLAG; (void)adaptFLAG; (void)RANK;
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
+  if (!h) { report("timestep_cuda_"); return; }
+  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
+  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
+  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) || psg_ns3d_upload(h, in)) {
+    report("timestep_cuda_");
+    return;
+  }
+  const double delt = *DELT;
+  double tme = *TSTART;
+  int nfull = 0;
+  while (*Tstep - tme > delt) {
+    ++nfull;
+    tme += delt;
+  }
+  if (psg_ns3d_step(h, delt, nfull, 0)) { report("timestep_cuda_"); return; }
+  if (tme != *Tstep && psg_ns3d_step(h, *Tstep - tme, 1, 0)) { report("timestep_cuda_"); return; }
+  if (psg_ns3d_download(h, out)) { report("timestep_cuda_"); return; }
+  for (int i = 0; i < nfull; ++i) *Time = *Time + delt;
+}
+
+// dz/dt at the given state; the state arrays receive the derivative
+// (3D_Boussinesq/src/src_gmres/cuda.cu:319-533).
+extern "C" void timederiv_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
+                                double* ky, double* kz, double* Time, double* TSTART,
+                                double* Tstep, double* AMPFOR, double* DELT, double* ResThresh,
+                                double* KFY, double* V2, double* Ri, double* Sc, double* Theta,
+                                double* alpha, double* Dtarget, int* ikF, int* ikN, int* LC,
+                                int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT, int* NX,
+                                int* NY, int* NZ, int* NOUT, int* NOUTV, int* statsFLAG,
+                                int* RecFLAG, int* adaptFLAG, int* RANK) {
+  (void)kx; (void)ky; (void)kz; (void)Time; (void)TSTART; (void)Tstep; (void)DELT;
+  (void)ResThresh; (void)Dtarget; (void)ikF; (void)ikN; (void)LC; (void)NOUT; (void)NOUTV;
+  (void)statsFLAG; (void)RecFLAG; (void)adaptFLAG; (void)RANK;
+  if (!check_sizes("timederiv_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
+  if (!h) { report("timederiv_cuda_"); return; }
+  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
+  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
+  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) || psg_ns3d_upload(h, in) ||
+      psg_ns3d_timederiv(h, out))
+    report("timederiv_cuda_");
+}
+
+#else
+#error "define PSG_FLAVOUR_NS3D, PSG_FLAVOUR_EULER3D or PSG_FLAVOUR_BOUS3D"
+#endif
+
+// set_gpu_: the Navier-Stokes and Euler builds only report the current device
+// (3D_NavierStokes/src/functions.h:3-20); the Boussinesq build selects device
+// *go (3D_Boussinesq/src/functions.h:9-28).
+extern "C" void set_gpu_(int* go) {
+  int count = 0, dev = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    printf("cutil error: no devices supporting CUDA\n");
+    exit(-1);
+  }
+#if defined(PSG_FLAVOUR_BOUS3D)
+  dev = *go;
+  cudaSetDevice(dev);
+#else
+  (void)go;
+  cudaGetDevice(&dev);
+#endif
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  printf("\n Using CUDA device %d: %s\n\n", dev, prop.name);
+}

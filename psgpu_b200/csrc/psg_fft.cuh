@@ -94,15 +94,20 @@ template <> struct Plan<128> { static constexpr int R1 = 16, R2 = 8;  };
 template <> struct Plan<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Plan<512> { static constexpr int R1 = 32, R2 = 16; };
 
-template <int N, int SIGN, typename T>
+// SWAP exchanges the two radices.  The output distribution of a plan is the
+// input distribution of its swapped plan, so a transform that consumes the
+// registers another transform produced (the x-pass: C2R -> product -> R2C)
+// must use the swapped factorisation.
+template <int N, int SIGN, typename T, bool SWAP = false>
 struct LineFFT {
-  static constexpr int R1 = Plan<N>::R1;
-  static constexpr int R2 = Plan<N>::R2;
+  static constexpr int R1 = SWAP ? Plan<N>::R2 : Plan<N>::R1;
+  static constexpr int R2 = SWAP ? Plan<N>::R1 : Plan<N>::R2;
   static constexpr int G = R1 < R2 ? R1 : R2;   // threads per line
   static constexpr int E = N / G;               // elements per thread
   static constexpr int A = R1 / G;              // step-1 DFTs per thread
   static constexpr int B = R2 / G;              // step-2 DFTs per thread
-  static constexpr int SMEM = R2 * (R1 + 1);    // complex words of exchange space per line
+  // complex words of exchange space per line, enough for either orientation
+  static constexpr int SMEM = (R2 * (R1 + 1) > R1 * (R2 + 1)) ? R2 * (R1 + 1) : R1 * (R2 + 1);
 
   // input position of register e (e = a*R2 + n2) for thread g
   static __device__ __forceinline__ int in_index(int g, int e) {

@@ -61,4 +61,27 @@ struct Fields4 {
   cpx<T>* c[4];
 };
 
+// precision-independent interface of the 3D engine (psg_ns3d_impl.cuh)
+struct Engine3DBase {
+  virtual ~Engine3DBase() {}
+  virtual int init(int n, double alpha, int scheme) = 0;
+  virtual int set_params(double nu, double ampfor, double kf, double ri, double sc, double theta) = 0;
+  virtual void set_stream(cudaStream_t s) = 0;
+  virtual cudaStream_t get_stream() const = 0;
+  virtual int upload(const double* const* comps) = 0;
+  virtual int download(double* const* comps) = 0;
+  virtual int download_stage(double* const* comps) = 0;
+  virtual int steps(double dt, int nsteps, int dump_last) = 0;
+  virtual int timederiv(double* const* out) = 0;
+  virtual int phys(double* const* out) = 0;
+  virtual int layout(int* xp, void** comps) = 0;
+  virtual long launch_count() const = 0;
+  // per-pass timing (A, B, C, D, E) with CUDA events between the launches
+  virtual int profile(int enable) = 0;
+  virtual int profile_read(double* ms, long* counts) = 0;
+};
+
+Engine3DBase* make_engine3d_f32();
+Engine3DBase* make_engine3d_f64();
+
 }  // namespace psg

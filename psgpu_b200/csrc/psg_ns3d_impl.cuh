@@ -1,10 +1,11 @@
-// psg_ns3d.cu -- sm_100a kernels and host engine of the 3D pseudospectral step
+// psg_ns3d_impl.cuh -- sm_100a kernels and host engine of the 3D pseudospectral step
 // (Navier-Stokes Heun/CN, Euler Heun, Navier-Stokes RK4/CN, Boussinesq RK4/CN).
 //
 // See psg_ns3d.cuh for the data layout and the pass structure.  Each scheme
 // update restates the reference kernel cited beside it; the transforms replace
 // the reference's conj -> setFFN -> cufftExecZ2D -> multReal -> cufftExecD2Z ->
 // normFF1 sequence (3D_NavierStokes/src/functions.h:26-108).
+#pragma once
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -174,7 +175,7 @@ pass_y(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
 template <typename T, int N>
 struct RowOps {
   using FI = LineFFT<N, +1, T>;
-  using FO = LineFFT<N, -1, T>;
+  using FO = LineFFT<N, -1, T, true>;  // consumes FI's output distribution
   static constexpr int G = FI::G, E = FI::E;
 
   // inverse transform of two real fields a, b given by their half spectra
@@ -541,7 +542,7 @@ __global__ void copy_fields(Fields4<T> src, Fields4<T> dst, int nc, long len) {
 constexpr int kTileW = 8;
 
 template <typename T>
-struct Engine3D {
+struct Engine3D final : Engine3DBase {
   Geom3<T> g{};
   int scheme = 0;
   int nc = 3;    // state components
@@ -559,6 +560,42 @@ struct Engine3D {
   cpx<T>* B2 = nullptr;
   double2* stage_h = nullptr;  // device FP64 staging box
   long launches = 0;
+  // optional per-pass timing with CUDA events recorded between the passes
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_tag;
+  size_t ev_used = 0;
+
+  void mark(int tag) {
+    if (!profiling) return;
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    cudaEventRecord(ev_pool[ev_used], stream);
+    ev_tag.push_back(tag);
+    ++ev_used;
+  }
+  int profile(int enable) override {
+    profiling = enable != 0;
+    ev_used = 0;
+    ev_tag.clear();
+    return PSG_OK;
+  }
+  int profile_read(double* ms, long* counts) override {
+    for (int k = 0; k < 5; ++k) { ms[k] = 0.0; counts[k] = 0; }
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    for (size_t i = 1; i < ev_used; ++i) {
+      const int t = ev_tag[i];
+      if (t < 0) continue;
+      float v = 0.f;
+      PSG_CUDA_TRY(cudaEventElapsedTime(&v, ev_pool[i - 1], ev_pool[i]));
+      ms[t] += v;
+      counts[t] += 1;
+    }
+    return PSG_OK;
+  }
 
   size_t smem_a() const {
     return sizeof(cpx<T>) * (g.n + (size_t)nc * g.Y * kTileW + kTileW * fft_smem()) + g.Y * kTileW;
@@ -589,7 +626,7 @@ struct Engine3D {
     }
   }
 
-  int init(int n, double alpha, int scheme_) {
+  int init(int n, double alpha, int scheme_) override {
     if (!(n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512)) {
       psg_set_error("3D grid size %d unsupported (powers of two 16..512)", n);
       return PSG_ERR_UNSUPPORTED;
@@ -632,6 +669,10 @@ struct Engine3D {
     return set_smem_limits();
   }
 
+  ~Engine3D() override {
+    release();
+    for (auto e : ev_pool) cudaEventDestroy(e);
+  }
   void release() {
     if (pool) cudaFree(pool);
     if (stage_h) cudaFree(stage_h);
@@ -683,11 +724,14 @@ struct Engine3D {
     Fields4<T> in = stage_input();
     const int mv = first_rhs;
     first_rhs = 0;
+    mark(-1);
     if (bous)
       pass_a<T, N, kTileW, 4, 9><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
     else
       pass_a<T, N, kTileW, 3, 6><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
+    mark(0);
     pass_y<T, N, kTileW, true><<<dim3(tiles, N, nfi), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    mark(1);
     const T scale = (T)1 / ((T)N * (T)N * (T)N);
     const int rows_per_block = 128 / G;
     const int cblocks = (N * N) / rows_per_block;
@@ -696,7 +740,9 @@ struct Engine3D {
       pass_c<T, N, true><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
     else
       pass_c<T, N, false><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
+    mark(2);
     pass_y<T, N, kTileW, false><<<dim3(tiles, N, nfo), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    mark(3);
     const dim3 ge(tiles, g.Y);
     switch (scheme) {
       case SCHEME_NS_HEUN:
@@ -711,6 +757,7 @@ struct Engine3D {
       default:
         pass_e<T, N, kTileW, 4, SCHEME_BOUS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
     }
+    mark(4);
     launches += 5;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
@@ -744,7 +791,7 @@ struct Engine3D {
 
   // host FP64 boxes (reference layout) -> device state; RK4 schemes also set
   // the stage state X0 = S as the reference's setVelocity does.
-  int upload(const double* const* comps) {
+  int upload(const double* const* comps) override {
     const long nref = (long)g.Y * g.Y * g.X;
     for (int q = 0; q < nc; ++q) {
       PSG_CUDA_TRY(cudaMemcpyAsync(stage_h, comps[q], sizeof(double2) * nref,
@@ -761,7 +808,46 @@ struct Engine3D {
     return PSG_OK;
   }
 
-  int download(double* const* comps, const Fields4<T>* src = nullptr) {
+  int download(double* const* comps) override { return download_from(comps, nullptr); }
+  int download_stage(double* const* comps) override {
+    if (!R.X0.c[0]) { psg_set_error("scheme keeps no stage state"); return PSG_ERR_STATE; }
+    return download_from(comps, &R.X0);
+  }
+  int timederiv(double* const* out) override {
+    if (scheme != SCHEME_BOUS_RK4 && scheme != SCHEME_NS_RK4) {
+      psg_set_error("time derivative is defined for the RK4 schemes");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    int rc = rhs(STAGE_DERIV);
+    if (rc) return rc;
+    return download_from(out, &R.K1);
+  }
+  int set_params(double nu, double ampfor, double kf, double ri, double sc, double theta) override {
+    prm.nu = (T)nu; prm.ampfor = (T)ampfor; prm.kf = (T)kf; prm.ri = (T)ri; prm.sc = (T)sc;
+    prm.sinth = (T)sin(theta); prm.costh = (T)cos(theta);
+    return PSG_OK;
+  }
+  void set_stream(cudaStream_t s) override { stream = s; }
+  cudaStream_t get_stream() const override { return stream; }
+  long launch_count() const override { return launches; }
+  int steps(double dt, int nsteps, int dump_last) override {
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = step((T)dt, dump_last && s == nsteps - 1);
+      if (rc) return rc;
+    }
+    return PSG_OK;
+  }
+  int layout(int* xp, void** comps) override {
+    if (xp) *xp = g.XP;
+    if (comps)
+      for (int q = 0; q < 4; ++q) comps[q] = (void*)R.S.c[q];
+    return PSG_OK;
+  }
+  int phys(double* const* out) override {
+    if (!dump) { psg_set_error("scheme keeps no physical fields"); return PSG_ERR_STATE; }
+    return download_phys(out);
+  }
+  int download_from(double* const* comps, const Fields4<T>* src) {
     const long nref = (long)g.Y * g.Y * g.X;
     const Fields4<T>& F = src ? *src : R.S;
     for (int q = 0; q < nc; ++q) {
@@ -793,129 +879,3 @@ struct Engine3D {
 
 }  // namespace psg
 
-// ---------------------------------------------------------------------------
-// C API (include/psgpu.h)
-// ---------------------------------------------------------------------------
-using namespace psg;
-
-struct psg_ns3d {
-  int precision;  // 32 or 64
-  Engine3D<float> f;
-  Engine3D<double> d;
-};
-
-template <typename Fn>
-static int with_engine(psg_ns3d* h, Fn fn) {
-  if (!h) { psg_set_error("null handle"); return PSG_ERR_ARG; }
-  if (h->precision == 64) return fn(h->d);
-  return fn(h->f);
-}
-
-extern "C" int psg_ns3d_create(psg_ns3d** out, int n, double alpha, int scheme, int precision) {
-  if (!out) { psg_set_error("null output handle"); return PSG_ERR_ARG; }
-  *out = nullptr;
-  if (scheme < 0 || scheme > 3) { psg_set_error("unknown scheme %d", scheme); return PSG_ERR_ARG; }
-  if (precision != 32 && precision != 64) { psg_set_error("precision must be 32 or 64"); return PSG_ERR_ARG; }
-  if (alpha != 1.0) {
-    psg_set_error("aspect ratio alpha=%g unsupported: the box must be cubic", alpha);
-    return PSG_ERR_UNSUPPORTED;
-  }
-  psg_ns3d* h = new psg_ns3d();
-  h->precision = precision;
-  int rc = (precision == 64) ? h->d.init(n, alpha, scheme) : h->f.init(n, alpha, scheme);
-  if (rc) { h->f.release(); h->d.release(); delete h; return rc; }
-  *out = h;
-  return PSG_OK;
-}
-
-extern "C" void psg_ns3d_destroy(psg_ns3d* h) {
-  if (!h) return;
-  h->f.release();
-  h->d.release();
-  delete h;
-}
-
-extern "C" int psg_ns3d_set_params(psg_ns3d* h, double nu, double ampfor, double kf, double ri,
-                                   double sc, double theta) {
-  return with_engine(h, [&](auto& e) {
-    using T = typename std::remove_reference<decltype(e.prm.dt)>::type;
-    e.prm.nu = (T)nu; e.prm.ampfor = (T)ampfor; e.prm.kf = (T)kf; e.prm.ri = (T)ri;
-    e.prm.sc = (T)sc; e.prm.sinth = (T)sin(theta); e.prm.costh = (T)cos(theta);
-    return PSG_OK;
-  });
-}
-
-extern "C" int psg_ns3d_set_stream(psg_ns3d* h, void* stream) {
-  return with_engine(h, [&](auto& e) { e.stream = (cudaStream_t)stream; return PSG_OK; });
-}
-
-extern "C" int psg_ns3d_upload(psg_ns3d* h, const double* const* comps) {
-  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
-  return with_engine(h, [&](auto& e) { return e.upload(comps); });
-}
-
-extern "C" int psg_ns3d_download(psg_ns3d* h, double* const* comps) {
-  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
-  return with_engine(h, [&](auto& e) { return e.download(comps); });
-}
-
-extern "C" int psg_ns3d_download_stage(psg_ns3d* h, double* const* comps) {
-  return with_engine(h, [&](auto& e) {
-    if (!e.R.X0.c[0]) { psg_set_error("scheme keeps no stage state"); return PSG_ERR_STATE; }
-    return e.download(comps, &e.R.X0);
-  });
-}
-
-extern "C" int psg_ns3d_step(psg_ns3d* h, double dt, int nsteps, int dump_last) {
-  if (nsteps < 0) { psg_set_error("negative step count"); return PSG_ERR_ARG; }
-  return with_engine(h, [&](auto& e) {
-    using T = typename std::remove_reference<decltype(e.prm.dt)>::type;
-    for (int s = 0; s < nsteps; ++s) {
-      int rc = e.step((T)dt, dump_last && s == nsteps - 1);
-      if (rc) return rc;
-    }
-    return PSG_OK;
-  });
-}
-
-extern "C" int psg_ns3d_timederiv(psg_ns3d* h, double* const* out) {
-  return with_engine(h, [&](auto& e) {
-    if (e.scheme != SCHEME_BOUS_RK4 && e.scheme != SCHEME_NS_RK4) {
-      psg_set_error("time derivative is defined for the RK4 schemes");
-      return PSG_ERR_UNSUPPORTED;
-    }
-    int rc = e.rhs(STAGE_DERIV);
-    if (rc) return rc;
-    return e.download(out, &e.R.K1);
-  });
-}
-
-extern "C" int psg_ns3d_download_phys(psg_ns3d* h, double* const* out) {
-  return with_engine(h, [&](auto& e) {
-    if (!e.dump) { psg_set_error("scheme keeps no physical fields"); return PSG_ERR_STATE; }
-    return e.download_phys(out);
-  });
-}
-
-extern "C" int psg_ns3d_sync(psg_ns3d* h) {
-  return with_engine(h, [&](auto& e) {
-    PSG_CUDA_TRY(cudaStreamSynchronize(e.stream));
-    return PSG_OK;
-  });
-}
-
-extern "C" long psg_ns3d_launches(psg_ns3d* h) {
-  if (!h) return -1;
-  return h->precision == 64 ? h->d.launches : h->f.launches;
-}
-
-// device pointers of the state components, for callers that keep the state
-// resident (layout: [2K+1][2K+1][XP] complex of the engine's precision)
-extern "C" int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps) {
-  return with_engine(h, [&](auto& e) {
-    if (xp) *xp = e.g.XP;
-    if (comps)
-      for (int q = 0; q < 4; ++q) comps[q] = (void*)e.R.S.c[q];
-    return PSG_OK;
-  });
-}
