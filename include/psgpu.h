@@ -99,6 +99,29 @@ long psg_batch2d_launches(psg_batch2d* h);
 /* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]) */
 int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z);
 
+/* Allocation-free 2D step.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory when they step: a plugin
+ * inside a host runtime that owns all GPU memory, code running while a CUDA
+ * graph is being captured, or an embedded driver with a fixed memory budget.
+ * It integrates nsteps RK4/CN steps of one 2D instance (the same kernel body
+ * as psg_batch2d_run) with all scratch -- stage registers, row buffers and
+ * twiddles -- in a 512 KiB array compiled into the library, which every GPU
+ * that loads the library holds until the process exits.  Limits: n in
+ * {16, 32, 64, 128}; larger grids are rejected with PSG_ERR_UNSUPPORTED.
+ *
+ * z_in, z_out: device pointers owned by the caller to the complex state in the
+ * reference layout [2K+1][K+1] (float2 for precision 32, double2 for 64);
+ * z_in == z_out is allowed.  The work is enqueued on `stream` (NULL: the
+ * default stream).  The first call on a device looks up the array's address
+ * and writes the twiddle tables (a synchronous copy), so make that first call
+ * before any stream capture.  Every call uses the same array and leaves its
+ * last contents there (no call relies on them: each scratch word is written
+ * before it is read), so calls that overlap on the GPU -- e.g. on two streams
+ * at once -- race; serialise them on one stream. */
+int psg_ns2d_step_noalloc(int n, int precision, double nu, double dt, int nsteps,
+                          const void* z_in, void* z_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

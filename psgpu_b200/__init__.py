@@ -90,6 +90,7 @@ def _declare_2d(L):
     L.psg_batch2d_launches.argtypes = [vp]
     L.psg_batch2d_launches.restype = C.c_long
     L.psg_batch2d_device_state.argtypes = [vp, i, C.POINTER(vp)]
+    L.psg_ns2d_step_noalloc.argtypes = [i, i, C.c_double, C.c_double, i, vp, vp, vp]
 
 
 def _check(rc):

@@ -531,3 +531,149 @@ extern "C" int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z) {
   if (!Z) { psg_set_error("null output"); return PSG_ERR_ARG; }
   return h->b->device_state(i, Z);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the 2D step.
+//
+// Some hosts cannot call cudaMalloc from the code that drives the step: a
+// plugin running inside another runtime that owns all device memory, a
+// callback invoked while a CUDA graph is being captured, or an embedded
+// driver whose memory budget is fixed at start-up.  psg_ns2d_step_noalloc
+// serves them: it runs the same per-instance kernel body as the batched engine
+// (Rhs2D::run), but its stage registers, row scratch and twiddle tables live
+// in the file-scope array below instead of buffers allocated at run time.  The
+// caller passes only the state, in device memory it already owns.
+//
+// Size limit: grids up to 128 x 128 (FP32 or FP64).  The array is part of the
+// library image, so every GPU that loads the library holds these 512 KiB until
+// the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr int kNoallocMaxN = 128;
+constexpr size_t kNoallocBytes = 512 * 1024;
+constexpr size_t kTw64Off = 0;          // 240 complex doubles (n = 16..128)
+constexpr size_t kTw32Off = 4096;       // 240 complex floats
+constexpr size_t kWorkOff = 8192;       // Z0..Z3 and row scratch
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+// device address of g_noalloc_scratch, looked up once per device
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[kMaxDevices] = {nullptr};
+
+template <typename T>
+__global__ void __launch_bounds__(256) ns2d_single(Inst2D<T> I, const cpx<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* smem = reinterpret_cast<cpx<T>*>(smem_raw);
+  switch (I.n) {
+    case 16: Rhs2D<T, 16>::run(I, tw, smem); break;
+    case 32: Rhs2D<T, 32>::run(I, tw, smem); break;
+    case 64: Rhs2D<T, 64>::run(I, tw, smem); break;
+    default: Rhs2D<T, 128>::run(I, tw, smem); break;
+  }
+}
+
+template <typename T>
+size_t noalloc_smem() {
+  // the densest exchange layout among the supported sizes
+  size_t worst = 0;
+  worst = std::max(worst, (size_t)(16 + (256 / LineFFT<16, 1, T>::G) * LineFFT<16, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(32 + (256 / LineFFT<32, 1, T>::G) * LineFFT<32, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(64 + (256 / LineFFT<64, 1, T>::G) * LineFFT<64, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(128 + (256 / LineFFT<128, 1, T>::G) * LineFFT<128, 1, T>::SMEM));
+  return worst * sizeof(cpx<T>);
+}
+
+// One-time set-up on the current device: find the array's device address,
+// write the twiddle tables into it, raise the kernels' shared-memory limit.
+// Nothing here allocates device memory.
+int noalloc_setup(unsigned char** out) {
+  int dev = 0;
+  PSG_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    psg_set_error("device ordinal %d beyond %d", dev, kMaxDevices);
+    return PSG_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[dev]) { *out = g_noalloc_addr[dev]; return PSG_OK; }
+  void* addr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    psg_set_error("cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+    return PSG_ERR_CUDA;
+  }
+  cpx<double> t64[240];
+  cpx<float> t32[240];
+  int o = 0;
+  for (int n = 16; n <= kNoallocMaxN; n *= 2) {
+    for (int j = 0; j < n; ++j) {
+      const double a = -2.0 * M_PI * (double)j / (double)n;
+      t64[o + j] = cpx<double>{cos(a), sin(a)};
+      t32[o + j] = cpx<float>{(float)cos(a), (float)sin(a)};
+    }
+    o += n;
+  }
+  PSG_CUDA_TRY(cudaMemcpy((unsigned char*)addr + kTw64Off, t64, sizeof t64, cudaMemcpyHostToDevice));
+  PSG_CUDA_TRY(cudaMemcpy((unsigned char*)addr + kTw32Off, t32, sizeof t32, cudaMemcpyHostToDevice));
+  PSG_CUDA_TRY(cudaFuncSetAttribute(ns2d_single<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)noalloc_smem<double>()));
+  PSG_CUDA_TRY(cudaFuncSetAttribute(ns2d_single<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)noalloc_smem<float>()));
+  g_noalloc_addr[dev] = (unsigned char*)addr;
+  *out = (unsigned char*)addr;
+  return PSG_OK;
+}
+
+template <typename T>
+int noalloc_run(unsigned char* base, int n, double nu, double dt, int nsteps, const void* z_in,
+                void* z_out, cudaStream_t stream) {
+  const long nk = nkt2(n);
+  if (z_in != z_out)
+    PSG_CUDA_TRY(cudaMemcpyAsync(z_out, z_in, sizeof(cpx<T>) * nk, cudaMemcpyDeviceToDevice, stream));
+  cpx<T>* work = reinterpret_cast<cpx<T>*>(base + kWorkOff);
+  Inst2D<T> I;
+  I.n = n; I.nsteps = nsteps; I.nu = (T)nu; I.dt = (T)dt;
+  I.Z = reinterpret_cast<cpx<T>*>(z_out);
+  I.Z0 = work; I.Z1 = work + nk; I.Z2 = work + 2 * nk; I.Z3 = work + 3 * nk;
+  I.work = work + 4 * nk;
+  const cpx<T>* tw = reinterpret_cast<const cpx<T>*>(base + (sizeof(T) == 8 ? kTw64Off : kTw32Off));
+  int off = 0;
+  for (int m = 16; m < n; m *= 2) off += m;
+  ns2d_single<T><<<1, 256, noalloc_smem<T>(), stream>>>(I, tw + off);
+  PSG_CUDA_TRY(cudaGetLastError());
+  return PSG_OK;
+}
+
+}  // namespace
+
+// No counterpart in the reference: see include/psgpu.h.
+extern "C" int psg_ns2d_step_noalloc(int n, int precision, double nu, double dt, int nsteps,
+                                     const void* z_in, void* z_out, void* stream) {
+  if (!(n == 16 || n == 32 || n == 64 || n == 128)) {
+    psg_set_error("psg_ns2d_step_noalloc: grid %d unsupported; the static scratch holds grids "
+                  "of 16, 32, 64 or 128 points per direction at most", n);
+    return PSG_ERR_UNSUPPORTED;
+  }
+  if (precision != 32 && precision != 64) {
+    psg_set_error("psg_ns2d_step_noalloc: precision must be 32 or 64");
+    return PSG_ERR_ARG;
+  }
+  if (nsteps < 0 || !z_in || !z_out) {
+    psg_set_error("psg_ns2d_step_noalloc: bad arguments");
+    return PSG_ERR_ARG;
+  }
+  // the largest footprint must fit the array: 4 stage registers + 3 scratch rows
+  const size_t need = kWorkOff + (size_t)16 * (4 * nkt2(kNoallocMaxN) + 3L * kNoallocMaxN * (kNoallocMaxN / 3 + 1));
+  static_assert(kWorkOff + 16ull * (4 * 3655 + 3 * 128 * 43) <= kNoallocBytes, "scratch too small");
+  (void)need;
+  unsigned char* base = nullptr;
+  int rc = noalloc_setup(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == 64 ? noalloc_run<double>(base, n, nu, dt, nsteps, z_in, z_out, s)
+                         : noalloc_run<float>(base, n, nu, dt, nsteps, z_in, z_out, s);
+}
