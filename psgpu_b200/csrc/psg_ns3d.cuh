@@ -76,6 +76,7 @@ struct Engine3DBase {
   virtual int phys(double* const* out) = 0;
   virtual int layout(int* xp, void** comps) = 0;
   virtual long launch_count() const = 0;
+  virtual int sync() = 0;  // wait for the stream and check the device error flag
   // per-pass timing (A, B, C, D, E) with CUDA events between the launches
   virtual int profile(int enable) = 0;
   virtual int profile_read(double* ms, long* counts) = 0;

@@ -89,8 +89,7 @@ extern "C" int psg_ns3d_download_phys(psg_ns3d* h, double* const* out) {
 
 extern "C" int psg_ns3d_sync(psg_ns3d* h) {
   PSG_CHECK_HANDLE(h);
-  PSG_CUDA_TRY(cudaStreamSynchronize(h->e->get_stream()));
-  return PSG_OK;
+  return h->e->sync();
 }
 
 extern "C" long psg_ns3d_launches(psg_ns3d* h) {

@@ -1,10 +1,20 @@
 // psg_ns3d_impl.cuh -- sm_100a kernels and host engine of the 3D pseudospectral step
 // (Navier-Stokes Heun/CN, Euler Heun, Navier-Stokes RK4/CN, Boussinesq RK4/CN).
 //
-// See psg_ns3d.cuh for the data layout and the pass structure.  Each scheme
-// update restates the reference kernel cited beside it; the transforms replace
-// the reference's conj -> setFFN -> cufftExecZ2D -> multReal -> cufftExecD2Z ->
-// normFF1 sequence (3D_NavierStokes/src/functions.h:26-108).
+// See psg_ns3d.cuh for the pass structure.  Each scheme update restates the
+// reference kernel cited beside it; the transforms replace the reference's
+// conj -> setFFN -> cufftExecZ2D -> multReal -> cufftExecD2Z -> normFF1
+// sequence (3D_NavierStokes/src/functions.h:26-108).
+//
+// Data layout (complex T, W = 8 kx columns per tile, XT = XP / W tiles):
+//   state / registers  S[c][xt][ky][kz][W]     pass A reads, pass E writes one tile
+//   B1 (A -> B)        [f][xt][z][ky][W]       pass B reads one [ky][W] tile
+//   B2 (B -> C)        [f][z][y][XP]           pass C reads L whole rows
+//   B3 (C -> D)        [f][xt][z][y][W]        pass D reads one [y][W] tile
+//   B4 (D -> E)        [f][xt][ky][z][W]       pass E reads one [z][W] tile
+// so that every pass's input tile is one contiguous chunk of HBM, moved into
+// shared memory by a single TMA bulk copy (cp.async.bulk) per field; outputs
+// are written as full 64-byte segments.
 #pragma once
 #include <math.h>
 #include <stdlib.h>
@@ -14,9 +24,12 @@
 #include <vector>
 
 #include "psg_ns3d.cuh"
+#include "psg_tma.cuh"
 #include "psgpu_internal.h"
 
 namespace psg {
+
+constexpr int kTileW = 8;
 
 // FFT row (0..n-1) -> box index (0..2K) or -1 when the row is truncated
 __device__ __forceinline__ int row_to_box(int r, int K, int n) {
@@ -42,47 +55,100 @@ __device__ __forceinline__ T wkinv(T wk) {
   return (T)1 / (wk > (T)0.001 ? wk : (T)0.001);
 }
 
+// exchange stride per column of a column-pass tile: congruent to 2 mod 16
+// complex words, so that the 8 columns x 4 threads of a warp fall on distinct
+// banks in both exchange directions
+template <int S>
+struct ColStride {
+  static constexpr int value = S + ((2 - (S % 16)) + 16) % 16;
+};
+// exchange stride per row of the row pass: groups of G lanes share a warp
+template <int S, int G>
+struct RowStride {
+  static constexpr int off = (G >= 16) ? 0 : (G == 8 ? 8 : 4);
+  static constexpr int value = S + ((off - (S % 16)) + 16) % 16;
+};
+
+// Load `n` contiguous chunks into shared memory with one mbarrier; returns
+// false (uniformly) if the copy did not complete within the wait bound.
+__device__ __forceinline__ bool tile_load(uint64_t* bar, int* s_ok, void* const* dst,
+                                          const void* const* src, const uint32_t* bytes, int n,
+                                          int* status) {
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int i = 0; i < n; ++i) tot += bytes[i];
+    mbar_expect_tx(bar, tot);
+    for (int i = 0; i < n; ++i) bulk_g2s(dst[i], src[i], bytes[i], bar);
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, int* s_ok, int* status) {
+  if (threadIdx.x == 0) *s_ok = mbar_wait_bounded(bar, 0, status) ? 1 : 0;
+  __syncthreads();
+  return *s_ok != 0;
+}
+
 // ---------------------------------------------------------------------------
 // pass A: z-inverse of the stage state with the velocity (and density
 // gradient) formed in registers; Hermitian completion of the kx = 0 plane.
+// grid (XT, Y): one [kz][W] tile of each state component.
 // ---------------------------------------------------------------------------
-template <typename T, int N, int W, int NC, int NF>
-__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
+template <typename T, int N, int NC, int NF>
+__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
-       int mask_vel) {
+       int mask_vel, int* status) {
   using F = LineFFT<N, +1, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
-  cpx<T>* s_in = s_tw + N;                       // [NC][Y][W]
-  cpx<T>* s_ex = s_in + NC * g.Y * W;            // [W][SMEM]
-  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + W * F::SMEM);  // [Y][W]
+  constexpr int W = kTileW;
+  constexpr int SX = ColStride<F::SMEM>::value;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);   // [NC][Y][W]
+  cpx<T>* s_mir = s_in + NC * Y * W;                      // [NC][Y] mirror column
+  cpx<T>* s_tw = s_mir + NC * Y;                          // [N]
+  cpx<T>* s_ex = s_tw + N;                                // [W][SX]
+  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + W * SX);  // [Y][W]
 
   const int tid = threadIdx.x, nth = blockDim.x;
   const int c = tid % W, gi = tid / W;
-  const int x0 = blockIdx.x * W, iky = blockIdx.y;
-  const int K = g.K, Y = g.Y, XP = g.XP;
-  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
-  for (int idx = tid; idx < Y * W; idx += nth) {
-    const int ikz = idx / W, cc = idx % W, ikx = x0 + cc;
-    int sz = ikz, sy = iky;
-    bool cj = false, zero = (ikx >= g.X);
-    if (ikx == 0) {
-      if (iky < K || (iky == K && ikz < K)) { sz = 2 * K - ikz; sy = 2 * K - iky; cj = true; }
-      else if (iky == K && ikz == K) zero = true;
-    }
-    const long src = ((long)sz * Y + sy) * XP + ikx;
-#pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      cpx<T> v = zero ? czero<T>() : in.c[q][src];
-      if (cj) v.y = -v.y;
-      s_in[(q * Y + ikz) * W + cc] = v;
-    }
-    s_ll[idx] = zero ? 0 : (unsigned char)keep_mode<T>(ikx, sy - K, sz - K, K, g.alpha);
-  }
+  const int xt = blockIdx.x, iky = blockIdx.y;
+  const long tile = ((long)xt * Y + iky) * Y * W;
+  if (tid == 0) mbar_init(&s_bar, 1);
   __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
+    for (int q = 0; q < NC; ++q)
+      bulk_g2s(s_in + q * Y * W, in.c[q] + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), &s_bar);
+  }
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  // mirror column for the Hermitian completion of kx = 0 (only tile 0, ky <= 0)
+  const bool mirror = (xt == 0) && (iky <= K);
+  if (mirror) {
+    const long mt = ((long)0 * Y + (2 * K - iky)) * Y * W;
+    for (int i = tid; i < NC * Y; i += nth) {
+      const int q = i / Y, ikz = i % Y;
+      s_mir[i] = in.c[q][mt + (long)(2 * K - ikz) * W];
+    }
+  }
+  for (int idx = tid; idx < Y * W; idx += nth) {
+    const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
+    unsigned char ll;
+    if (ikx >= g.X) ll = 0;
+    else if (ikx == 0 && mirror && !(iky == K && ikz > K))  // value taken from the mirror mode
+      ll = (iky == K && ikz == K) ? 0
+                                  : (unsigned char)keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
+    else ll = (unsigned char)keep_mode<T>(ikx, iky - K, ikz - K, K, g.alpha);
+    s_ll[idx] = ll;
+  }
+  if (!tile_wait(&s_bar, &s_ok, status)) return;
 
-  const T kx = (T)(x0 + c) * g.alpha;
+  const int ikx = xt * W + c;
+  const T kx = (T)ikx * g.alpha;
   const T ky = (T)(iky - K);
+  const bool live_col = ikx < g.X;
+  const bool mcol = mirror && c == 0;
 #pragma unroll 1
   for (int f = 0; f < NF; ++f) {
     cpx<T> v[F::E];
@@ -90,107 +156,116 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
     for (int e = 0; e < F::E; ++e) {
       const int ikz = row_to_box(F::in_index(gi, e), K, N);
       cpx<T> r = czero<T>();
-      if (ikz >= 0) {
-        const int o = ikz * W + c;
-        if (f < 3) {
-          r = s_in[f * Y * W + o];
-        } else if (f < 6) {
-          const cpx<T> xi = s_in[o], et = s_in[Y * W + o], zt = s_in[2 * Y * W + o];
-          const T kz = (T)(ikz - K);
+      if (ikz >= 0 && live_col) {
+        cpx<T> xi, et, zt, rho;
+        if (mcol) {
+          if (iky == K && ikz == K) {
+            xi = et = zt = rho = czero<T>();
+          } else if (iky == K && ikz > K) {
+            xi = s_in[ikz * W]; et = s_in[Y * W + ikz * W]; zt = s_in[2 * Y * W + ikz * W];
+            rho = (NC > 3) ? s_in[3 * Y * W + ikz * W] : czero<T>();
+          } else {
+            xi = cconj(s_mir[ikz]); et = cconj(s_mir[Y + ikz]); zt = cconj(s_mir[2 * Y + ikz]);
+            rho = (NC > 3) ? cconj(s_mir[3 * Y + ikz]) : czero<T>();
+          }
+        } else {
+          const int o = ikz * W + c;
+          xi = s_in[o]; et = s_in[Y * W + o]; zt = s_in[2 * Y * W + o];
+          rho = (NC > 3) ? s_in[3 * Y * W + o] : czero<T>();
+        }
+        const T kz = (T)(ikz - K);
+        if (f == 0) r = xi;
+        else if (f == 1) r = et;
+        else if (f == 2) r = zt;
+        else if (f < 6) {
           const T wk = kx * kx + ky * ky + kz * kz;
           T wki = wkinv(wk);
-          if (mask_vel && !s_ll[o]) wki = (T)0;
+          if (mask_vel && !s_ll[ikz * W + c]) wki = (T)0;
           // u = i k x w / k^2 (3D_NavierStokes/src/kernels.h:194-201)
           if (f == 3) r = cpx<T>{-(ky * zt.y - kz * et.y) * wki, -(kz * et.x - ky * zt.x) * wki};
           else if (f == 4) r = cpx<T>{-(kz * xi.y - kx * zt.y) * wki, -(kx * zt.x - kz * xi.x) * wki};
           else r = cpx<T>{-(kx * et.y - ky * xi.y) * wki, -(ky * xi.x - kx * et.x) * wki};
         } else {
           // i k_j rho (setFFK, 3D_Boussinesq/src/kernels.h:75-93)
-          const cpx<T> rho = s_in[3 * Y * W + o];
-          const T kk = (f == 6) ? kx : (f == 7) ? ky : (T)(ikz - K);
+          const T kk = (f == 6) ? kx : (f == 7) ? ky : kz;
           r = cpx<T>{-kk * rho.y, kk * rho.x};
         }
       }
       v[e] = r;
     }
-    F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
-    cpx<T>* o = out + ((long)f * N * Y + iky) * XP + x0 + c;
+    F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+    cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
 #pragma unroll
-    for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * XP] = v[e];
+    for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * W] = v[e];
   }
 }
 
 // ---------------------------------------------------------------------------
-// passes B and D: transform a tile of W columns along the middle (y) axis.
-//   INV: rows iky (Y of them) -> rows y (N);  !INV: rows y (N) -> rows iky (Y)
-// in/out planes: [f][z][rows][XP]
+// pass B: y-inverse.  grid (XT, N, NF): tile B1[f][xt][z] = [ky][W] -> B2 rows
 // ---------------------------------------------------------------------------
-template <typename T, int N, int W, bool INV>
-__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
-pass_y(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-       const cpx<T>* __restrict__ tw) {
-  using F = LineFFT<N, INV ? +1 : -1, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+template <typename T, int N>
+__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
+pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
+       const cpx<T>* __restrict__ tw, int* status) {
+  using F = LineFFT<N, +1, T>;
+  constexpr int W = kTileW;
+  constexpr int SX = ColStride<F::SMEM>::value;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  const int Y = g.Y, K = g.K, XP = g.XP, XT = XP / W;
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [Y][W]
+  cpx<T>* s_tw = s_in + Y * W;
   cpx<T>* s_ex = s_tw + N;
   const int tid = threadIdx.x, c = tid % W, gi = tid / W;
-  const int x0 = blockIdx.x * W, z = blockIdx.y, f = blockIdx.z;
-  const int K = g.K, Y = g.Y, XP = g.XP;
-  const int rin = INV ? Y : N, rout = INV ? N : Y;
+  const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
+  if (tid == 0) mbar_init(&s_bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&s_bar, (uint32_t)(Y * W * sizeof(cpx<T>)));
+    bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * Y * W, (uint32_t)(Y * W * sizeof(cpx<T>)),
+             &s_bar);
+  }
   for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
-  const cpx<T>* src = in + (((long)f * N + z) * rin) * XP + x0 + c;
+  if (!tile_wait(&s_bar, &s_ok, status)) return;
   cpx<T> v[F::E];
 #pragma unroll
   for (int e = 0; e < F::E; ++e) {
-    const int r = F::in_index(gi, e);
-    if (INV) {
-      const int iky = row_to_box(r, K, N);
-      v[e] = iky >= 0 ? src[(long)iky * XP] : czero<T>();
-    } else {
-      v[e] = src[(long)r * XP];
-    }
+    const int iky = row_to_box(F::in_index(gi, e), K, N);
+    v[e] = iky >= 0 ? s_in[iky * W + c] : czero<T>();
   }
-  __syncthreads();
-  F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
-  cpx<T>* dst = out + (((long)f * N + z) * rout) * XP + x0 + c;
+  F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+  cpx<T>* dst = out + (((long)f * N + z) * N) * XP + xt * W + c;
 #pragma unroll
-  for (int e = 0; e < F::E; ++e) {
-    const int k = F::out_index(gi, e);
-    if (INV) {
-      dst[(long)k * XP] = v[e];
-    } else {
-      const int iky = row_to_box(k, K, N);
-      if (iky >= 0) dst[(long)iky * XP] = v[e];
-    }
-  }
+  for (int e = 0; e < F::E; ++e) dst[(long)F::out_index(gi, e) * XP] = v[e];
 }
 
 // ---------------------------------------------------------------------------
-// pass C: x rows.  C2R of the fields (packed two real signals per complex
-// transform), the products -(u x w) (multReal, 3D_NavierStokes/src/kernels.h:
-// 281-306) and u.grad rho (3D_Boussinesq/src/kernels.h:298-328) in registers,
-// scaled by 1/N^3 (normFF1), and R2C back, keeping kx <= K.
-// in: [NF][z][y][XP], out: [NO][z][y][XP].  One row per group of G threads.
+// pass C: x rows.  C2R of the fields (two real signals per complex transform),
+// the products -(u x w) (multReal, 3D_NavierStokes/src/kernels.h:281-306) and
+// u.grad rho (3D_Boussinesq/src/kernels.h:298-328) in registers, scaled by
+// 1/N^3 (normFF1), R2C back keeping kx <= K.  L rows per block (one row per
+// group of G lanes), the block's rows of every field fetched by bulk copies.
+// out: B3 [g][xt][z][y][W]
 // ---------------------------------------------------------------------------
 template <typename T, int N>
 struct RowOps {
   using FI = LineFFT<N, +1, T>;
   using FO = LineFFT<N, -1, T, true>;  // consumes FI's output distribution
   static constexpr int G = FI::G, E = FI::E;
+  static constexpr int SX = RowStride<FI::SMEM, FI::G>::value;
 
-  // inverse transform of two real fields a, b given by their half spectra
-  static __device__ __forceinline__ void c2r_pair(const cpx<T>* __restrict__ A,
-                                                  const cpx<T>* __restrict__ B, int K, int gi,
-                                                  const cpx<T>* tw, cpx<T>* ex, T (&ra)[E],
-                                                  T (&rb)[E]) {
+  // inverse transform of two real fields a, b given by their half spectra (smem rows)
+  static __device__ __forceinline__ void c2r_pair(const cpx<T>* A, const cpx<T>* B, int K,
+                                                  int gi, const cpx<T>* tw, cpx<T>* ex,
+                                                  T (&ra)[E], T (&rb)[E]) {
     cpx<T> v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int r = FI::in_index(gi, e);
       cpx<T> z = czero<T>();
       if (r == 0) {
-        const T a = A[0].x, b = B ? B[0].x : (T)0;
-        z = cpx<T>{a, b};
+        z = cpx<T>{A[0].x, B ? B[0].x : (T)0};
       } else if (r <= K) {
         const cpx<T> a = A[r], b = B ? B[r] : czero<T>();
         z = cpx<T>{a.x - b.y, a.y + b.x};  // a + i b
@@ -205,12 +280,12 @@ struct RowOps {
     for (int e = 0; e < E; ++e) { ra[e] = v[e].x; rb[e] = v[e].y; }
   }
 
-  // forward transform of two real signals p, q; writes P_k, Q_k for k < XP
-  // (zero beyond K).  q == nullptr: single signal p.
+  // forward transform of two real signals p, q (q == nullptr: p alone); writes
+  // P_k, Q_k for k < XP into the [xt][..][W] layout (zero beyond K)
   static __device__ __forceinline__ void r2c_pair(const T (&p)[E], const T* q, int K, int XP,
                                                   int gi, const cpx<T>* tw, cpx<T>* ex,
-                                                  cpx<T>* __restrict__ P,
-                                                  cpx<T>* __restrict__ Q) {
+                                                  cpx<T>* __restrict__ P, cpx<T>* __restrict__ Q,
+                                                  long tstride) {
     cpx<T> v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = cpx<T>{p[e], q ? q[e] : (T)0};
@@ -230,8 +305,9 @@ struct RowOps {
             pk = cpx<T>{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
             qk = cpx<T>{(T)0.5 * (a.y + b.y), (T)(-0.5) * (a.x - b.x)};
           }
-          P[k] = pk;
-          Q[k] = qk;
+          const long o = (long)(k / kTileW) * tstride + (k % kTileW);
+          P[o] = pk;
+          Q[o] = qk;
         }
       }
       __syncwarp();
@@ -239,35 +315,50 @@ struct RowOps {
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int k = FO::out_index(gi, e);
-        if (k < XP) P[k] = (k <= K) ? v[e] : czero<T>();
+        if (k < XP) P[(long)(k / kTileW) * tstride + (k % kTileW)] = (k <= K) ? v[e] : czero<T>();
       }
     }
   }
 };
 
-template <typename T, int N, bool BOUS>
+template <typename T, int N, int NF>
 __global__ void __launch_bounds__(128)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump) {
+       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status) {
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
   constexpr int L = 128 / G;  // rows per block
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
+  constexpr bool BOUS = (NF == 9);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  const int K = g.K, XP = g.XP, XT = XP / kTileW;
+  cpx<T>* s_rows = reinterpret_cast<cpx<T>*>(smem_raw);  // [NF][L][XP]
+  cpx<T>* s_tw = s_rows + NF * L * XP;
   cpx<T>* s_ex = s_tw + N;
   const int tid = threadIdx.x, lr = tid / G, gi = tid % G;
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
-  __syncthreads();
-  const long row = (long)blockIdx.x * L + lr;  // z * N + y
-  const int K = g.K, XP = g.XP;
+  const long row0 = (long)blockIdx.x * L;  // rows z*N + y
   const long plane = (long)N * N * XP;
-  const cpx<T>* src = in + row * XP;
-  cpx<T>* ex = s_ex + lr * R::FI::SMEM;
+  if (tid == 0) mbar_init(&s_bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t bytes = (uint32_t)(L * XP * sizeof(cpx<T>));
+    mbar_expect_tx(&s_bar, NF * bytes);
+    for (int f = 0; f < NF; ++f) bulk_g2s(s_rows + f * L * XP, in + f * plane + row0 * XP, bytes, &s_bar);
+  }
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
+  if (!tile_wait(&s_bar, &s_ok, status)) return;
+
+  const long row = row0 + lr;
+  const int z = (int)(row / N), y = (int)(row % N);
+  const cpx<T>* src = s_rows + lr * XP;
+  const int fs = L * XP;  // field stride in shared memory
+  cpx<T>* ex = s_ex + lr * R::SX;
 
   T xi[E], et[E], zt[E], u[E], v[E], w[E];
-  R::c2r_pair(src, src + plane, K, gi, s_tw, ex, xi, et);
-  R::c2r_pair(src + 2 * plane, src + 3 * plane, K, gi, s_tw, ex, zt, u);
-  R::c2r_pair(src + 4 * plane, src + 5 * plane, K, gi, s_tw, ex, v, w);
+  R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
+  R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
+  R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
   if (dump) {
     const long base = row * N;
     const long nr = (long)N * N * N;
@@ -287,223 +378,293 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
     n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
   }
-  cpx<T>* dst = out + row * XP;
+  // B3[f][xt][z][y][W]: tile stride between successive xt = N*N*W
+  const long tstride = (long)N * N * kTileW;
+  const long fstride = (long)XT * tstride;
+  cpx<T>* dst = out + ((long)z * N + y) * kTileW;
   if (!BOUS) {
-    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + plane);
-    R::r2c_pair(n3, nullptr, K, XP, gi, s_tw, ex, dst + 2 * plane, nullptr);
+    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + fstride, tstride);
+    R::r2c_pair(n3, nullptr, K, XP, gi, s_tw, ex, dst + 2 * fstride, nullptr, tstride);
   } else {
     T rx[E], ry[E], n4[E];
-    R::c2r_pair(src + 6 * plane, src + 7 * plane, K, gi, s_tw, ex, rx, ry);
+    R::c2r_pair(src + 6 * fs, src + 7 * fs, K, gi, s_tw, ex, rx, ry);
 #pragma unroll
     for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
-    R::c2r_pair(src + 8 * plane, nullptr, K, gi, s_tw, ex, rx, ry);
+    R::c2r_pair(src + 8 * fs, nullptr, K, gi, s_tw, ex, rx, ry);
 #pragma unroll
     for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
-    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + plane);
-    R::r2c_pair(n3, n4, K, XP, gi, s_tw, ex, dst + 2 * plane, dst + 3 * plane);
+    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + fstride, tstride);
+    R::r2c_pair(n3, n4, K, XP, gi, s_tw, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
   }
 }
 
 // ---------------------------------------------------------------------------
-// pass E: z-forward of the NO fields of one ky plane tile, then the spectral
+// pass D: y-forward.  grid (XT, N, NO): tile B3[f][xt][z] = [y][W] -> B4
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
+pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
+       const cpx<T>* __restrict__ tw, int* status) {
+  using F = LineFFT<N, -1, T>;
+  constexpr int W = kTileW;
+  constexpr int SX = ColStride<F::SMEM>::value;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [N][W]
+  cpx<T>* s_tw = s_in + N * W;
+  cpx<T>* s_ex = s_tw + N;
+  const int tid = threadIdx.x, c = tid % W, gi = tid / W;
+  const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
+  if (tid == 0) mbar_init(&s_bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&s_bar, (uint32_t)(N * W * sizeof(cpx<T>)));
+    bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * N * W, (uint32_t)(N * W * sizeof(cpx<T>)),
+             &s_bar);
+  }
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
+  if (!tile_wait(&s_bar, &s_ok, status)) return;
+  cpx<T> v[F::E];
+#pragma unroll
+  for (int e = 0; e < F::E; ++e) v[e] = s_in[F::in_index(gi, e) * W + c];
+  F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+  // B4[f][xt][ky][z][W]
+  cpx<T>* dst = out + (((long)f * XT + xt) * Y * N + z) * W + c;
+#pragma unroll
+  for (int e = 0; e < F::E; ++e) {
+    const int iky = row_to_box(F::out_index(gi, e), K, N);
+    if (iky >= 0) dst[(long)iky * N * W] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pass E: z-forward of the NO fields of one (xt, ky) tile, then the spectral
 // finish and the scheme update for every mode of the tile.
-// in: [NO][z][ky][XP]
 // ---------------------------------------------------------------------------
 template <typename T>
 struct Regs {
   Fields4<T> S, X0, K1, K2, K3;
 };
 
-template <typename T, int N, int W, int NO, int SCHEME>
-__global__ void __launch_bounds__(W * LineFFT<N, 1, T>::G)
+template <typename T, int SCHEME>
+__device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R,
+                                             const StepParams<T>& p, int stage, long ik, int ikx,
+                                             int iy, int iz, T xiX, T xiY, T etX, T etY, T ztX,
+                                             T ztY, cpx<T> RKv) {
+  const T kx = (T)ikx * g.alpha, ky = (T)iy, kz = (T)iz;
+  const T wk = kx * kx + ky * ky + kz * kz;
+  const T wki = wkinv(wk);
+  const T LL = keep_mode<T>(ikx, iy, iz, g.K, g.alpha) ? (T)1 : (T)0;
+  if (SCHEME == SCHEME_NS_HEUN || SCHEME == SCHEME_EULER_HEUN) {
+    cpx<T>* S0 = R.S.c[0]; cpx<T>* S1 = R.S.c[1]; cpx<T>* S2 = R.S.c[2];
+    cpx<T>* H0 = R.K1.c[0]; cpx<T>* H1 = R.K1.c[1]; cpx<T>* H2 = R.K1.c[2];
+    const cpx<T> s0 = S0[ik], s1 = S1[ik], s2 = S2[ik];
+    if (SCHEME == SCHEME_NS_HEUN) {
+      if (kx == (T)0 && kz == p.kf && ky == p.kf) xiX += p.ampfor;
+      if (kx == (T)0 && kz == -p.kf && ky == p.kf) xiX -= p.ampfor;
+      // nuzn = (1 - nu k^2 dt/2)/dt, nu1 = dt/(1 + nu k^2 dt/2) (3D_NavierStokes/src/init.F90:194-198)
+      const T NU = p.nu * wk;
+      const T nuzn = LL * (((T)1 - (T)0.5 * NU * p.dt) / p.dt);
+      const T nu1 = LL * (p.dt / ((T)1 + (T)0.5 * NU * p.dt));
+      if (stage == STAGE_HEUN_PRED) {
+        H0[ik] = cpx<T>{xiX, xiY}; H1[ik] = cpx<T>{etX, etY}; H2[ik] = cpx<T>{ztX, ztY};
+        const T NU1 = LL * nu1;
+        S0[ik] = cpx<T>{NU1 * (nuzn * s0.x + xiX), NU1 * (nuzn * s0.y + xiY)};
+        S1[ik] = cpx<T>{NU1 * (nuzn * s1.x + etX), NU1 * (nuzn * s1.y + etY)};
+        S2[ik] = cpx<T>{NU1 * (nuzn * s2.x + ztX), NU1 * (nuzn * s2.y + ztY)};
+      } else {
+        const T NU2 = (T)0.5 * nu1;
+        const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
+        S0[ik] = cpx<T>{LL * (s0.x + NU2 * (xiX - h0.x)), LL * (s0.y + NU2 * (xiY - h0.y))};
+        S1[ik] = cpx<T>{LL * (s1.x + NU2 * (etX - h1.x)), LL * (s1.y + NU2 * (etY - h1.y))};
+        S2[ik] = cpx<T>{LL * (s2.x + NU2 * (ztX - h2.x)), LL * (s2.y + NU2 * (ztY - h2.y))};
+      }
+    } else {  // Euler (3D_Euler/src/kernels.h:324-341, 396-406)
+      if (stage == STAGE_HEUN_PRED) {
+        H0[ik] = cpx<T>{LL * xiX, LL * xiY}; H1[ik] = cpx<T>{LL * etX, LL * etY};
+        H2[ik] = cpx<T>{LL * ztX, LL * ztY};
+        S0[ik] = cpx<T>{s0.x + p.dt * xiX, s0.y + p.dt * xiY};
+        S1[ik] = cpx<T>{s1.x + p.dt * etX, s1.y + p.dt * etY};
+        S2[ik] = cpx<T>{s2.x + p.dt * ztX, s2.y + p.dt * ztY};
+      } else {
+        const T hd = (T)0.5 * p.dt;
+        const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
+        S0[ik] = cpx<T>{LL * (s0.x + hd * (xiX - h0.x)), LL * (s0.y + hd * (xiY - h0.y))};
+        S1[ik] = cpx<T>{LL * (s1.x + hd * (etX - h1.x)), LL * (s1.y + hd * (etY - h1.y))};
+        S2[ik] = cpx<T>{LL * (s2.x + hd * (ztX - h2.x)), LL * (s2.y + hd * (ztY - h2.y))};
+      }
+    }
+  } else {
+    // RK4 with per-stage CN factors (3D_Boussinesq/src/kernels.h:331-621)
+    constexpr bool BOUS = (SCHEME == SCHEME_BOUS_RK4);
+    T rXR = 0, rXC = 0;  // density right-hand side
+    const bool final_stage = (stage == STAGE_RK4);
+    const T LC = final_stage ? (T)1 : LL;
+    const cpx<T> x0 = R.X0.c[0][ik], e0 = R.X0.c[1][ik], z0 = R.X0.c[2][ik];
+    if (BOUS) {
+      const cpx<T> r0 = R.X0.c[3][ik];
+      const cpx<T> RK = RKv;
+      const T gXR = -kx * r0.y, gXC = kx * r0.x, gYR = -ky * r0.y, gYC = ky * r0.x;
+      const T gZR = -kz * r0.y, gZC = kz * r0.x;
+      xiX = LC * (xiX - p.ri * (gYR * p.sinth - gZR * p.costh));
+      xiY = LC * (xiY - p.ri * (gYC * p.sinth - gZC * p.costh));
+      etX = LC * (etX + p.ri * gXR * p.sinth);
+      etY = LC * (etY + p.ri * gXC * p.sinth);
+      ztX = LC * (ztX - p.ri * gXR * p.costh);
+      ztY = LC * (ztY - p.ri * gXC * p.costh);
+      rXR = -LC * (RK.x + (kz * x0.y - kx * z0.y) * wki * p.costh +
+                   (kx * e0.y - ky * x0.y) * wki * p.sinth);
+      rXC = -LC * (RK.y + (kx * z0.x - kz * x0.x) * wki * p.costh +
+                   (ky * x0.x - kx * e0.x) * wki * p.sinth);
+    } else {
+      xiX *= LC; xiY *= LC; etX *= LC; etY *= LC; ztX *= LC; ztY *= LC;
+    }
+    if (kx == (T)0 && kz == (T)0 && ky == p.kf) ztX += p.ampfor;
+    const T dt = p.dt;
+    const T nk = dt * p.nu * wk;
+    const T nks = BOUS ? nk / p.sc : (T)0;
+    if (stage == STAGE_DERIV) {  // RHS kernel: dz/dt = -nu k^2 z + N
+      const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
+      const T d1 = -p.nu * wk;
+      R.K1.c[0][ik] = cpx<T>{d1 * s0.x + xiX, d1 * s0.y + xiY};
+      R.K1.c[1][ik] = cpx<T>{d1 * s1.x + etX, d1 * s1.y + etY};
+      R.K1.c[2][ik] = cpx<T>{d1 * s2.x + ztX, d1 * s2.y + ztY};
+      if (BOUS) {
+        const cpx<T> s3 = R.S.c[3][ik];
+        const T d2 = -p.nu * wk / p.sc;
+        R.K1.c[3][ik] = cpx<T>{d2 * s3.x + rXR, d2 * s3.y + rXC};
+      }
+    } else if (!final_stage) {
+      const T q = (stage == STAGE_RK3) ? (T)0.5 : (T)0.25;
+      const T fr = (stage == STAGE_RK3) ? (T)1 : (T)0.5;
+      const T d1 = ((T)1 - q * nk) / ((T)1 + q * nk);
+      const Fields4<T>& KR = (stage == STAGE_RK1) ? R.K1 : (stage == STAGE_RK2) ? R.K2 : R.K3;
+      KR.c[0][ik] = cpx<T>{dt * xiX, dt * xiY};
+      KR.c[1][ik] = cpx<T>{dt * etX, dt * etY};
+      KR.c[2][ik] = cpx<T>{dt * ztX, dt * ztY};
+      const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
+      R.X0.c[0][ik] = cpx<T>{d1 * (s0.x + fr * dt * xiX), d1 * (s0.y + fr * dt * xiY)};
+      R.X0.c[1][ik] = cpx<T>{d1 * (s1.x + fr * dt * etX), d1 * (s1.y + fr * dt * etY)};
+      R.X0.c[2][ik] = cpx<T>{d1 * (s2.x + fr * dt * ztX), d1 * (s2.y + fr * dt * ztY)};
+      if (BOUS) {
+        const T d2 = ((T)1 - q * nks) / ((T)1 + q * nks);
+        KR.c[3][ik] = cpx<T>{dt * rXR, dt * rXC};
+        const cpx<T> s3 = R.S.c[3][ik];
+        R.X0.c[3][ik] = cpx<T>{d2 * (s3.x + fr * dt * rXR), d2 * (s3.y + fr * dt * rXC)};
+      }
+    } else {
+      const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
+      const T d1 = (T)1 - (T)0.5 * nk;
+      const T den = (T)1 + (T)0.5 * nk;
+      T o[4][2];
+      const T nr[3][2] = {{xiX, xiY}, {etX, etY}, {ztX, ztY}};
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const cpx<T> s = R.S.c[q][ik], a = R.K1.c[q][ik], b = R.K2.c[q][ik], cc3 = R.K3.c[q][ik];
+        o[q][0] = LL * (d1 * s.x + sixth * (a.x + dt * nr[q][0]) + third * (b.x + cc3.x)) / den;
+        o[q][1] = LL * (d1 * s.y + sixth * (a.y + dt * nr[q][1]) + third * (b.y + cc3.y)) / den;
+      }
+      if (BOUS) {
+        const T d2 = (T)1 - (T)0.5 * nks;
+        const T den2 = (T)1 + (T)0.5 * nks;
+        const cpx<T> s = R.S.c[3][ik], a = R.K1.c[3][ik], b = R.K2.c[3][ik], cc3 = R.K3.c[3][ik];
+        o[3][0] = LL * (d2 * s.x + sixth * (a.x + dt * rXR) + third * (b.x + cc3.x)) / den2;
+        o[3][1] = LL * (d2 * s.y + sixth * (a.y + dt * rXC) + third * (b.y + cc3.y)) / den2;
+        R.X0.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
+        R.S.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) R.X0.c[q][ik] = cpx<T>{o[q][0], o[q][1]};
+      // remove the divergence of the vorticity (3D_Boussinesq/src/kernels.h:597-606)
+      const T phiR = (kx * o[0][1] + ky * o[1][1] + kz * o[2][1]) * wki;
+      const T phiC = -(kx * o[0][0] + ky * o[1][0] + kz * o[2][0]) * wki;
+      R.S.c[0][ik] = cpx<T>{o[0][0] - (-kx * phiC), o[0][1] - kx * phiR};
+      R.S.c[1][ik] = cpx<T>{o[1][0] - (-ky * phiC), o[1][1] - ky * phiR};
+      R.S.c[2][ik] = cpx<T>{o[2][0] - (-kz * phiC), o[2][1] - kz * phiR};
+    }
+  }
+
+}
+
+template <typename T, int N, int NO, int SCHEME>
+__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
 pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw, Regs<T> R,
-       StepParams<T> p, int stage) {
+       StepParams<T> p, int stage, int* status) {
   using F = LineFFT<N, -1, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<T>* s_tw = reinterpret_cast<cpx<T>*>(smem_raw);
-  cpx<T>* s_res = s_tw + N;            // [NO][Y][W]
-  cpx<T>* s_ex = s_res + NO * g.Y * W;  // [W][SMEM]
+  constexpr int W = kTileW;
+  constexpr int SX = ColStride<F::SMEM>::value;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  // field f's transformed rows overwrite the start of its own input tile
+  // (every thread has read its inputs before the barrier inside F::run)
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NO][N][W]
+  cpx<T>* s_tw = s_in + NO * N * W;
+  cpx<T>* s_ex = s_tw + N;
   const int tid = threadIdx.x, nth = blockDim.x, c = tid % W, gi = tid / W;
-  const int x0 = blockIdx.x * W, iky = blockIdx.y;
-  const int K = g.K, Y = g.Y, XP = g.XP;
-  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  const int xt = blockIdx.x, iky = blockIdx.y;
+  if (tid == 0) mbar_init(&s_bar, 1);
   __syncthreads();
+  if (tid == 0) {
+    const uint32_t bytes = (uint32_t)(N * W * sizeof(cpx<T>));
+    mbar_expect_tx(&s_bar, NO * bytes);
+    for (int f = 0; f < NO; ++f)
+      bulk_g2s(s_in + f * N * W, in + (((long)f * XT + xt) * Y + iky) * N * W, bytes, &s_bar);
+  }
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  if (!tile_wait(&s_bar, &s_ok, status)) return;
 #pragma unroll 1
   for (int f = 0; f < NO; ++f) {
-    const cpx<T>* src = in + ((long)f * N * Y + iky) * XP + x0 + c;
     cpx<T> v[F::E];
 #pragma unroll
-    for (int e = 0; e < F::E; ++e) v[e] = src[(long)F::in_index(gi, e) * Y * XP];
-    F::run(v, gi, s_tw, s_ex + c * F::SMEM, BlockSync());
+    for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(gi, e)) * W + c];
+    F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
 #pragma unroll
     for (int e = 0; e < F::E; ++e) {
       const int ikz = row_to_box(F::out_index(gi, e), K, N);
-      if (ikz >= 0) s_res[(f * Y + ikz) * W + c] = v[e];
+      if (ikz >= 0) s_in[(f * N + ikz) * W + c] = v[e];
     }
   }
   __syncthreads();
-
+  const long tile = ((long)xt * Y + iky) * Y * W;
   for (int idx = tid; idx < Y * W; idx += nth) {
-    const int ikz = idx / W, cc = idx % W, ikx = x0 + cc;
+    const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
     if (ikx >= g.X) continue;
-    const long ik = ((long)ikz * Y + iky) * XP + ikx;
+    const long ik = tile + idx;
     const int iy = iky - K, iz = ikz - K;
     const T kx = (T)ikx * g.alpha, ky = (T)iy, kz = (T)iz;
-    const T wk = kx * kx + ky * ky + kz * kz;
-    const T wki = wkinv(wk);
-    const T LL = keep_mode<T>(ikx, iy, iz, K, g.alpha) ? (T)1 : (T)0;
-    const cpx<T> U = s_res[(0 * Y + ikz) * W + cc];
-    const cpx<T> V = s_res[(1 * Y + ikz) * W + cc];
-    const cpx<T> Wv = s_res[(2 * Y + ikz) * W + cc];
+    const cpx<T> U = s_in[(0 * N + ikz) * W + cc];
+    const cpx<T> V = s_in[(1 * N + ikz) * W + cc];
+    const cpx<T> Wv = s_in[(2 * N + ikz) * W + cc];
+    const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + ikz) * W + cc] : czero<T>();
     // curl of F(-(u x w)) as preStep/corStep form it (3D_NavierStokes/src/kernels.h:327-334)
-    T xiX = ky * Wv.y - kz * V.y, xiY = kz * V.x - ky * Wv.x;
-    T etX = kz * U.y - kx * Wv.y, etY = kx * Wv.x - kz * U.x;
-    T ztX = kx * V.y - ky * U.y, ztY = ky * U.x - kx * V.x;
-
-    if (SCHEME == SCHEME_NS_HEUN || SCHEME == SCHEME_EULER_HEUN) {
-      cpx<T>* S0 = R.S.c[0]; cpx<T>* S1 = R.S.c[1]; cpx<T>* S2 = R.S.c[2];
-      cpx<T>* H0 = R.K1.c[0]; cpx<T>* H1 = R.K1.c[1]; cpx<T>* H2 = R.K1.c[2];
-      const cpx<T> s0 = S0[ik], s1 = S1[ik], s2 = S2[ik];
-      if (SCHEME == SCHEME_NS_HEUN) {
-        if (kx == (T)0 && kz == p.kf && ky == p.kf) xiX += p.ampfor;
-        if (kx == (T)0 && kz == -p.kf && ky == p.kf) xiX -= p.ampfor;
-        // nuzn = (1 - nu k^2 dt/2)/dt, nu1 = dt/(1 + nu k^2 dt/2) (3D_NavierStokes/src/init.F90:194-198)
-        const T NU = p.nu * wk;
-        const T nuzn = LL * (((T)1 - (T)0.5 * NU * p.dt) / p.dt);
-        const T nu1 = LL * (p.dt / ((T)1 + (T)0.5 * NU * p.dt));
-        if (stage == STAGE_HEUN_PRED) {
-          H0[ik] = cpx<T>{xiX, xiY}; H1[ik] = cpx<T>{etX, etY}; H2[ik] = cpx<T>{ztX, ztY};
-          const T NU1 = LL * nu1;
-          S0[ik] = cpx<T>{NU1 * (nuzn * s0.x + xiX), NU1 * (nuzn * s0.y + xiY)};
-          S1[ik] = cpx<T>{NU1 * (nuzn * s1.x + etX), NU1 * (nuzn * s1.y + etY)};
-          S2[ik] = cpx<T>{NU1 * (nuzn * s2.x + ztX), NU1 * (nuzn * s2.y + ztY)};
-        } else {
-          const T NU2 = (T)0.5 * nu1;
-          const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
-          S0[ik] = cpx<T>{LL * (s0.x + NU2 * (xiX - h0.x)), LL * (s0.y + NU2 * (xiY - h0.y))};
-          S1[ik] = cpx<T>{LL * (s1.x + NU2 * (etX - h1.x)), LL * (s1.y + NU2 * (etY - h1.y))};
-          S2[ik] = cpx<T>{LL * (s2.x + NU2 * (ztX - h2.x)), LL * (s2.y + NU2 * (ztY - h2.y))};
-        }
-      } else {  // Euler (3D_Euler/src/kernels.h:324-341, 396-406)
-        if (stage == STAGE_HEUN_PRED) {
-          H0[ik] = cpx<T>{LL * xiX, LL * xiY}; H1[ik] = cpx<T>{LL * etX, LL * etY};
-          H2[ik] = cpx<T>{LL * ztX, LL * ztY};
-          S0[ik] = cpx<T>{s0.x + p.dt * xiX, s0.y + p.dt * xiY};
-          S1[ik] = cpx<T>{s1.x + p.dt * etX, s1.y + p.dt * etY};
-          S2[ik] = cpx<T>{s2.x + p.dt * ztX, s2.y + p.dt * ztY};
-        } else {
-          const T hd = (T)0.5 * p.dt;
-          const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
-          S0[ik] = cpx<T>{LL * (s0.x + hd * (xiX - h0.x)), LL * (s0.y + hd * (xiY - h0.y))};
-          S1[ik] = cpx<T>{LL * (s1.x + hd * (etX - h1.x)), LL * (s1.y + hd * (etY - h1.y))};
-          S2[ik] = cpx<T>{LL * (s2.x + hd * (ztX - h2.x)), LL * (s2.y + hd * (ztY - h2.y))};
-        }
-      }
-    } else {
-      // RK4 with per-stage CN factors (3D_Boussinesq/src/kernels.h:331-621)
-      constexpr bool BOUS = (SCHEME == SCHEME_BOUS_RK4);
-      T rXR = 0, rXC = 0;  // density right-hand side
-      const bool final_stage = (stage == STAGE_RK4);
-      const T LC = final_stage ? (T)1 : LL;
-      const cpx<T> x0 = R.X0.c[0][ik], e0 = R.X0.c[1][ik], z0 = R.X0.c[2][ik];
-      if (BOUS) {
-        const cpx<T> r0 = R.X0.c[3][ik];
-        const cpx<T> RK = s_res[(3 * Y + ikz) * W + cc];
-        const T gXR = -kx * r0.y, gXC = kx * r0.x, gYR = -ky * r0.y, gYC = ky * r0.x;
-        const T gZR = -kz * r0.y, gZC = kz * r0.x;
-        xiX = LC * (xiX - p.ri * (gYR * p.sinth - gZR * p.costh));
-        xiY = LC * (xiY - p.ri * (gYC * p.sinth - gZC * p.costh));
-        etX = LC * (etX + p.ri * gXR * p.sinth);
-        etY = LC * (etY + p.ri * gXC * p.sinth);
-        ztX = LC * (ztX - p.ri * gXR * p.costh);
-        ztY = LC * (ztY - p.ri * gXC * p.costh);
-        rXR = -LC * (RK.x + (kz * x0.y - kx * z0.y) * wki * p.costh +
-                     (kx * e0.y - ky * x0.y) * wki * p.sinth);
-        rXC = -LC * (RK.y + (kx * z0.x - kz * x0.x) * wki * p.costh +
-                     (ky * x0.x - kx * e0.x) * wki * p.sinth);
-      } else {
-        xiX *= LC; xiY *= LC; etX *= LC; etY *= LC; ztX *= LC; ztY *= LC;
-      }
-      if (kx == (T)0 && kz == (T)0 && ky == p.kf) ztX += p.ampfor;
-      const T dt = p.dt;
-      const T nk = dt * p.nu * wk;
-      const T nks = BOUS ? nk / p.sc : (T)0;
-      if (stage == STAGE_DERIV) {  // RHS kernel: dz/dt = -nu k^2 z + N
-        const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
-        const T d1 = -p.nu * wk;
-        R.K1.c[0][ik] = cpx<T>{d1 * s0.x + xiX, d1 * s0.y + xiY};
-        R.K1.c[1][ik] = cpx<T>{d1 * s1.x + etX, d1 * s1.y + etY};
-        R.K1.c[2][ik] = cpx<T>{d1 * s2.x + ztX, d1 * s2.y + ztY};
-        if (BOUS) {
-          const cpx<T> s3 = R.S.c[3][ik];
-          const T d2 = -p.nu * wk / p.sc;
-          R.K1.c[3][ik] = cpx<T>{d2 * s3.x + rXR, d2 * s3.y + rXC};
-        }
-      } else if (!final_stage) {
-        const T q = (stage == STAGE_RK3) ? (T)0.5 : (T)0.25;
-        const T fr = (stage == STAGE_RK3) ? (T)1 : (T)0.5;
-        const T d1 = ((T)1 - q * nk) / ((T)1 + q * nk);
-        const Fields4<T>& KR = (stage == STAGE_RK1) ? R.K1 : (stage == STAGE_RK2) ? R.K2 : R.K3;
-        KR.c[0][ik] = cpx<T>{dt * xiX, dt * xiY};
-        KR.c[1][ik] = cpx<T>{dt * etX, dt * etY};
-        KR.c[2][ik] = cpx<T>{dt * ztX, dt * ztY};
-        const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
-        R.X0.c[0][ik] = cpx<T>{d1 * (s0.x + fr * dt * xiX), d1 * (s0.y + fr * dt * xiY)};
-        R.X0.c[1][ik] = cpx<T>{d1 * (s1.x + fr * dt * etX), d1 * (s1.y + fr * dt * etY)};
-        R.X0.c[2][ik] = cpx<T>{d1 * (s2.x + fr * dt * ztX), d1 * (s2.y + fr * dt * ztY)};
-        if (BOUS) {
-          const T d2 = ((T)1 - q * nks) / ((T)1 + q * nks);
-          KR.c[3][ik] = cpx<T>{dt * rXR, dt * rXC};
-          const cpx<T> s3 = R.S.c[3][ik];
-          R.X0.c[3][ik] = cpx<T>{d2 * (s3.x + fr * dt * rXR), d2 * (s3.y + fr * dt * rXC)};
-        }
-      } else {
-        const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
-        const T d1 = (T)1 - (T)0.5 * nk;
-        const T den = (T)1 + (T)0.5 * nk;
-        T o[4][2];
-        const T nr[3][2] = {{xiX, xiY}, {etX, etY}, {ztX, ztY}};
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const cpx<T> s = R.S.c[q][ik], a = R.K1.c[q][ik], b = R.K2.c[q][ik], cc3 = R.K3.c[q][ik];
-          o[q][0] = LL * (d1 * s.x + sixth * (a.x + dt * nr[q][0]) + third * (b.x + cc3.x)) / den;
-          o[q][1] = LL * (d1 * s.y + sixth * (a.y + dt * nr[q][1]) + third * (b.y + cc3.y)) / den;
-        }
-        if (BOUS) {
-          const T d2 = (T)1 - (T)0.5 * nks;
-          const T den2 = (T)1 + (T)0.5 * nks;
-          const cpx<T> s = R.S.c[3][ik], a = R.K1.c[3][ik], b = R.K2.c[3][ik], cc3 = R.K3.c[3][ik];
-          o[3][0] = LL * (d2 * s.x + sixth * (a.x + dt * rXR) + third * (b.x + cc3.x)) / den2;
-          o[3][1] = LL * (d2 * s.y + sixth * (a.y + dt * rXC) + third * (b.y + cc3.y)) / den2;
-          R.X0.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
-          R.S.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
-        }
-#pragma unroll
-        for (int q = 0; q < 3; ++q) R.X0.c[q][ik] = cpx<T>{o[q][0], o[q][1]};
-        // remove the divergence of the vorticity (3D_Boussinesq/src/kernels.h:597-606)
-        const T phiR = (kx * o[0][1] + ky * o[1][1] + kz * o[2][1]) * wki;
-        const T phiC = -(kx * o[0][0] + ky * o[1][0] + kz * o[2][0]) * wki;
-        R.S.c[0][ik] = cpx<T>{o[0][0] - (-kx * phiC), o[0][1] - kx * phiR};
-        R.S.c[1][ik] = cpx<T>{o[1][0] - (-ky * phiC), o[1][1] - ky * phiR};
-        R.S.c[2][ik] = cpx<T>{o[2][0] - (-kz * phiC), o[2][1] - kz * phiR};
-      }
-    }
+    scheme_point<T, SCHEME>(g, R, p, stage, ik, ikx, iy, iz, ky * Wv.y - kz * V.y,
+                            kz * V.x - ky * Wv.x, kz * U.y - kx * Wv.y, kx * Wv.x - kz * U.x,
+                            kx * V.y - ky * U.y, ky * U.x - kx * V.x, RKv);
   }
 }
 
 // ---------------------------------------------------------------------------
-// layout conversion between the reference's FP64 boxes and the device layout
+// layout conversion between the reference's FP64 boxes and the tile layout
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>* __restrict__ dst) {
-  const long total = (long)g.Y * g.Y * g.XP;
+  const int W = kTileW;
+  const long total = (long)g.XP * g.Y * g.Y;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % g.XP);
-    const long r = i / g.XP;
+    const int w = (int)(i % W);
+    long r = i / W;
+    const int ikz = (int)(r % g.Y); r /= g.Y;
+    const int iky = (int)(r % g.Y);
+    const int xt = (int)(r / g.Y);
+    const int ikx = xt * W + w;
     cpx<T> v = czero<T>();
-    if (ix < g.X) {
-      const double2 s = src[r * g.X + ix];
+    if (ikx < g.X) {
+      const double2 s = src[((long)ikz * g.Y + iky) * g.X + ikx];
       v = cpx<T>{(T)s.x, (T)s.y};
     }
     dst[i] = v;
@@ -512,12 +673,14 @@ __global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>
 
 template <typename T>
 __global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* __restrict__ dst) {
+  const int W = kTileW;
   const long total = (long)g.Y * g.Y * g.X;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % g.X);
+    const int ikx = (int)(i % g.X);
     const long r = i / g.X;
-    const cpx<T> s = src[r * g.XP + ix];
+    const int iky = (int)(r % g.Y), ikz = (int)(r / g.Y);
+    const cpx<T> s = src[(((long)(ikx / W) * g.Y + iky) * g.Y + ikz) * W + (ikx % W)];
     dst[i] = make_double2((double)s.x, (double)s.y);
   }
 }
@@ -539,8 +702,6 @@ __global__ void copy_fields(Fields4<T> src, Fields4<T> dst, int nc, long len) {
 // ---------------------------------------------------------------------------
 // host engine
 // ---------------------------------------------------------------------------
-constexpr int kTileW = 8;
-
 template <typename T>
 struct Engine3D final : Engine3DBase {
   Geom3<T> g{};
@@ -559,6 +720,7 @@ struct Engine3D final : Engine3DBase {
   cpx<T>* B1 = nullptr;
   cpx<T>* B2 = nullptr;
   double2* stage_h = nullptr;  // device FP64 staging box
+  int* d_status = nullptr;     // device error flag of the bounded waits
   long launches = 0;
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
@@ -597,13 +759,37 @@ struct Engine3D final : Engine3DBase {
     return PSG_OK;
   }
 
+  // dynamic shared memory of each pass (must match the kernels' carve-up)
   size_t smem_a() const {
-    return sizeof(cpx<T>) * (g.n + (size_t)nc * g.Y * kTileW + kTileW * fft_smem()) + g.Y * kTileW;
+    return sizeof(cpx<T>) * ((size_t)nc * g.Y * kTileW + (size_t)nc * g.Y + g.n +
+                             kTileW * col_stride()) + g.Y * kTileW;
   }
-  size_t smem_y() const { return sizeof(cpx<T>) * (g.n + kTileW * fft_smem()); }
-  size_t smem_c() const { return sizeof(cpx<T>) * (g.n + (size_t)(128 / fft_g()) * fft_smem()); }
+  size_t smem_b() const { return sizeof(cpx<T>) * ((size_t)g.Y * kTileW + g.n + kTileW * col_stride()); }
+  size_t smem_c() const {
+    return sizeof(cpx<T>) * ((size_t)nfi * (128 / fft_g()) * g.XP + g.n +
+                             (size_t)(128 / fft_g()) * row_stride());
+  }
+  size_t smem_d() const { return sizeof(cpx<T>) * ((size_t)g.n * kTileW + g.n + kTileW * col_stride()); }
   size_t smem_e() const {
-    return sizeof(cpx<T>) * (g.n + (size_t)nfo * g.Y * kTileW + kTileW * fft_smem());
+    return sizeof(cpx<T>) * ((size_t)nfo * g.n * kTileW + g.n + kTileW * col_stride());
+  }
+  int col_stride() const {
+    switch (g.n) {
+      case 16: return ColStride<LineFFT<16, 1, T>::SMEM>::value;
+      case 32: return ColStride<LineFFT<32, 1, T>::SMEM>::value;
+      case 64: return ColStride<LineFFT<64, 1, T>::SMEM>::value;
+      case 128: return ColStride<LineFFT<128, 1, T>::SMEM>::value;
+      default: return ColStride<LineFFT<256, 1, T>::SMEM>::value;
+    }
+  }
+  int row_stride() const {
+    switch (g.n) {
+      case 16: return RowOps<T, 16>::SX;
+      case 32: return RowOps<T, 32>::SX;
+      case 64: return RowOps<T, 64>::SX;
+      case 128: return RowOps<T, 128>::SX;
+      default: return RowOps<T, 256>::SX;
+    }
   }
   int fft_g() const {
     switch (g.n) {
@@ -611,8 +797,7 @@ struct Engine3D final : Engine3DBase {
       case 32: return LineFFT<32, 1, T>::G;
       case 64: return LineFFT<64, 1, T>::G;
       case 128: return LineFFT<128, 1, T>::G;
-      case 256: return LineFFT<256, 1, T>::G;
-      default: return LineFFT<512, 1, T>::G;
+      default: return LineFFT<256, 1, T>::G;
     }
   }
   int fft_smem() const {
@@ -621,14 +806,13 @@ struct Engine3D final : Engine3DBase {
       case 32: return LineFFT<32, 1, T>::SMEM;
       case 64: return LineFFT<64, 1, T>::SMEM;
       case 128: return LineFFT<128, 1, T>::SMEM;
-      case 256: return LineFFT<256, 1, T>::SMEM;
-      default: return LineFFT<512, 1, T>::SMEM;
+      default: return LineFFT<256, 1, T>::SMEM;
     }
   }
 
   int init(int n, double alpha, int scheme_) override {
-    if (!(n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512)) {
-      psg_set_error("3D grid size %d unsupported (powers of two 16..512)", n);
+    if (!(n == 16 || n == 32 || n == 64 || n == 128 || n == 256)) {
+      psg_set_error("3D grid size %d unsupported (powers of two 16..256)", n);
       return PSG_ERR_UNSUPPORTED;
     }
     g.n = n; g.K = n / 3; g.X = g.K + 1; g.Y = 2 * g.K + 1;
@@ -664,6 +848,8 @@ struct Engine3D final : Engine3DBase {
     }
     PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
     PSG_CUDA_TRY(cudaMalloc(&stage_h, sizeof(double2) * (long)g.Y * g.Y * g.X));
+    PSG_CUDA_TRY(cudaMalloc(&d_status, sizeof(int)));
+    PSG_CUDA_TRY(cudaMemset(d_status, 0, sizeof(int)));
     if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN)
       PSG_CUDA_TRY(cudaMalloc(&dump, sizeof(T) * 3L * n * n * n));
     return set_smem_limits();
@@ -677,24 +863,35 @@ struct Engine3D final : Engine3DBase {
     if (pool) cudaFree(pool);
     if (stage_h) cudaFree(stage_h);
     if (dump) cudaFree(dump);
-    pool = nullptr; stage_h = nullptr; dump = nullptr;
+    if (d_status) cudaFree(d_status);
+    pool = nullptr; stage_h = nullptr; dump = nullptr; d_status = nullptr;
   }
 
   template <int N>
   int set_smem_limits_n() {
-    const int big = 200 * 1024;
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, kTileW, 3, 6>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, kTileW, 4, 9>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_NS_HEUN>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_EULER_HEUN>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 3, SCHEME_NS_RK4>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, kTileW, 4, SCHEME_BOUS_RK4>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    int dev = 0, big = 0;
+    PSG_CUDA_TRY(cudaGetDevice(&dev));
+    PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    big -= 1024;  // static shared memory of the kernels (mbarrier, flags)
+    const size_t need[5] = {smem_a(), smem_b(), smem_c(), smem_d(), smem_e()};
+    for (size_t x : need)
+      if (x > (size_t)big) {
+        psg_set_error("3D grid %d needs %zu bytes of shared memory per block, device allows %d",
+                      g.n, x, big);
+        return PSG_ERR_UNSUPPORTED;
+      }
+#define PSG_SMEM(kern) PSG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, big))
+    PSG_SMEM((pass_a<T, N, 3, 6>));
+    PSG_SMEM((pass_a<T, N, 4, 9>));
+    PSG_SMEM((pass_b<T, N>));
+    PSG_SMEM((pass_c<T, N, 6>));
+    PSG_SMEM((pass_c<T, N, 9>));
+    PSG_SMEM((pass_d<T, N>));
+    PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_HEUN>));
+    PSG_SMEM((pass_e<T, N, 3, SCHEME_EULER_HEUN>));
+    PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_RK4>));
+    PSG_SMEM((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
+#undef PSG_SMEM
     return PSG_OK;
   }
   int set_smem_limits() {
@@ -703,9 +900,23 @@ struct Engine3D final : Engine3DBase {
       case 32: return set_smem_limits_n<32>();
       case 64: return set_smem_limits_n<64>();
       case 128: return set_smem_limits_n<128>();
-      case 256: return set_smem_limits_n<256>();
-      default: return set_smem_limits_n<512>();
+      default: return set_smem_limits_n<256>();
     }
+  }
+
+  int sync() override { return check_status(); }
+
+  // device-side error flag (bounded waits); checked at every synchronisation
+  int check_status() {
+    int h = 0;
+    PSG_CUDA_TRY(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (h) {
+      psg_set_error("a kernel gave up waiting for its tile copy (status 0x%x)", h);
+      cudaMemsetAsync(d_status, 0, sizeof(int), stream);
+      return PSG_ERR_CUDA;
+    }
+    return PSG_OK;
   }
 
   Fields4<T> stage_input() const {
@@ -719,43 +930,43 @@ struct Engine3D final : Engine3DBase {
     using FG = LineFFT<N, 1, T>;
     const int G = FG::G;
     const dim3 blk(kTileW * G);
-    const int tiles = g.XP / kTileW;
+    const int XT = g.XP / kTileW;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
     Fields4<T> in = stage_input();
     const int mv = first_rhs;
     first_rhs = 0;
     mark(-1);
     if (bous)
-      pass_a<T, N, kTileW, 4, 9><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
+      pass_a<T, N, 4, 9><<<dim3(XT, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
     else
-      pass_a<T, N, kTileW, 3, 6><<<dim3(tiles, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv);
+      pass_a<T, N, 3, 6><<<dim3(XT, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
     mark(0);
-    pass_y<T, N, kTileW, true><<<dim3(tiles, N, nfi), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    pass_b<T, N><<<dim3(XT, N, nfi), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
     mark(1);
     const T scale = (T)1 / ((T)N * (T)N * (T)N);
     const int rows_per_block = 128 / G;
     const int cblocks = (N * N) / rows_per_block;
     T* dp = want_dump ? dump : nullptr;
     if (bous)
-      pass_c<T, N, true><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
+      pass_c<T, N, 9><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp, d_status);
     else
-      pass_c<T, N, false><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp);
+      pass_c<T, N, 6><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp, d_status);
     mark(2);
-    pass_y<T, N, kTileW, false><<<dim3(tiles, N, nfo), blk, smem_y(), stream>>>(g, B1, B2, tw);
+    pass_d<T, N><<<dim3(XT, N, nfo), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     mark(3);
-    const dim3 ge(tiles, g.Y);
+    const dim3 ge(XT, g.Y);
     switch (scheme) {
       case SCHEME_NS_HEUN:
-        pass_e<T, N, kTileW, 3, SCHEME_NS_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        pass_e<T, N, 3, SCHEME_NS_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       case SCHEME_EULER_HEUN:
-        pass_e<T, N, kTileW, 3, SCHEME_EULER_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        pass_e<T, N, 3, SCHEME_EULER_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       case SCHEME_NS_RK4:
-        pass_e<T, N, kTileW, 3, SCHEME_NS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        pass_e<T, N, 3, SCHEME_NS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       default:
-        pass_e<T, N, kTileW, 4, SCHEME_BOUS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage);
+        pass_e<T, N, 4, SCHEME_BOUS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
     }
     mark(4);
     launches += 5;
@@ -769,8 +980,7 @@ struct Engine3D final : Engine3DBase {
       case 32: return rhs_n<32>(stage, want_dump);
       case 64: return rhs_n<64>(stage, want_dump);
       case 128: return rhs_n<128>(stage, want_dump);
-      case 256: return rhs_n<256>(stage, want_dump);
-      default: return rhs_n<512>(stage, want_dump);
+      default: return rhs_n<256>(stage, want_dump);
     }
   }
 
@@ -848,6 +1058,7 @@ struct Engine3D final : Engine3DBase {
     return download_phys(out);
   }
   int download_from(double* const* comps, const Fields4<T>* src) {
+    if (int rc = check_status()) return rc;
     const long nref = (long)g.Y * g.Y * g.X;
     const Fields4<T>& F = src ? *src : R.S;
     for (int q = 0; q < nc; ++q) {
