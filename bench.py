@@ -160,6 +160,7 @@ def run_ours(args, rank, world, dist):
     stream = torch.cuda.current_stream(dev)
     eng.set_stream(stream.cuda_stream)
     eng.upload(xi, et, zt)
+    tune = eng.autotune()
     for _ in range(args.warmup):
         eng.step(DT, 1)
     torch.cuda.synchronize()
@@ -239,6 +240,9 @@ def run_ours(args, rank, world, dist):
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
             "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu,
             "clocks": clocks, "gpu_launches": int(launches),
+            "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
+                                "variants": ["L=128/G,1 stage", "L=256/G,1 stage",
+                                             "L=128/G,2 stages", "L=256/G,2 stages"]},
         }
         if out_note:
             out["note"] = out_note

@@ -69,6 +69,7 @@ def lib():
     L.psg_ns3d_launches.restype = C.c_long
     L.psg_ns3d_layout.argtypes = [vp, C.POINTER(ip), pp]
     L.psg_ns3d_profile.argtypes = [vp, i]
+    L.psg_ns3d_autotune.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_float)]
     L.psg_ns3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_long)]
     _declare_2d(L)
     _lib = L
@@ -188,6 +189,12 @@ class NS3D:
         cnt = (C.c_long * 5)()
         _check(lib().psg_ns3d_profile_read(self._h, ms, cnt))
         return {p: (ms[i], cnt[i]) for i, p in enumerate(self.PASSES)}
+
+    def autotune(self):
+        v = C.c_int()
+        ms = (C.c_float * 4)()
+        _check(lib().psg_ns3d_autotune(self._h, C.byref(v), ms))
+        return v.value, list(ms)
 
     def device_state(self):
         xp = C.c_int()

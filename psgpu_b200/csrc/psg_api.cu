@@ -60,10 +60,7 @@ int launch_linefft(const double* in, double* out, int nlines) {
   const long len = (long)nlines * N;
   psg::cpx<double>*d_in = nullptr, *d_out = nullptr, *d_tw = nullptr;
   psg::cpx<double> h_tw[N];
-  for (int j = 0; j < N; ++j) {
-    const double a = -2.0 * M_PI * (double)j / (double)N;
-    h_tw[j] = psg::cpx<double>{cos(a), sin(a)};
-  }
+  F::host_table(h_tw);
   int rc = PSG_OK;
   const int threads = 128;
   const int gpb = threads / F::G;

@@ -12,6 +12,8 @@
 // Sign convention: SIGN = -1 is the forward transform (e^{-i}), SIGN = +1 the
 // unnormalised inverse, matching cuFFT's D2Z / Z2D pair.
 #pragma once
+#include <math.h>
+
 #include "psg_common.cuh"
 
 namespace psg {
@@ -120,7 +122,17 @@ struct LineFFT {
     return g + G * b + R2 * k1;
   }
 
-  // Full transform.  tw: shared table tw[j] = exp(-2 pi i j / N), j < N.
+  // Twiddle table of this plan: TW[k2 * R1 + n1] = exp(-2 pi i n1 k2 / N), so
+  // that the R1 threads of a step-1 read for one k2 hit consecutive words.
+  static void host_table(cpx<T>* out) {
+    for (int k2 = 0; k2 < R2; ++k2)
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)(n1 * k2) / (double)N;
+        out[k2 * R1 + n1] = cpx<T>{(T)cos(a), (T)sin(a)};
+      }
+  }
+
+  // Full transform.  tw: this plan's table (host_table layout, N entries).
   // ex: this line's exchange buffer (SMEM complex words).  SYNC is a
   // callable that synchronises every thread that shares `ex` between the
   // shared-memory write and read (a warp or the whole block).
@@ -137,7 +149,7 @@ struct LineFFT {
       const int n1 = g + G * a;
 #pragma unroll
       for (int k2 = 0; k2 < R2; ++k2) {
-        cpx<T> t = tw[n1 * k2];
+        cpx<T> t = tw[k2 * R1 + n1];
         if (SIGN > 0) t.y = -t.y;
         ex[k2 * (R1 + 1) + n1] = cmul(w[k2], t);
       }

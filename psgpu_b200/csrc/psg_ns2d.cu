@@ -155,7 +155,7 @@ struct Rhs2D {
       // products (multReal, 2D_NavierStokes/src_RK4/kernels.h:187-201): p = v w, q = u w
 #pragma unroll
       for (int e = 0; e < E; ++e) v[e] = cpx<T>{v[e].x * w[e] * scale, u[e] * w[e] * scale};
-      FX::run(v, gi, tw, ex, WarpSync());
+      FX::run(v, gi, tw + N, ex, WarpSync());
 #pragma unroll
       for (int e = 0; e < E; ++e) ex[FX::out_index(gi, e)] = v[e];
       __syncwarp();
@@ -235,10 +235,11 @@ struct Rhs2D {
     }
   }
 
+  // gtw: the plain plan's twiddle table followed by the swapped plan's (2N entries)
   static __device__ void run(const Inst2D<T>& I, const cpx<T>* __restrict__ gtw, cpx<T>* smem) {
     cpx<T>* tw = smem;
-    cpx<T>* ex = smem + N + (threadIdx.x / G) * FI::SMEM;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+    cpx<T>* ex = smem + 2 * N + (threadIdx.x / G) * FI::SMEM;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = gtw[i];
     // setVelocity: Z0 = Z on kept modes, 0 elsewhere (kernels.h:112-147)
     for (int ik = threadIdx.x; ik < X * Y; ik += blockDim.x) {
       const int iky = ik / X, ikx = ik % X;
@@ -300,6 +301,17 @@ __global__ void dev_to_ref2(const cpx<T>* __restrict__ src, double2* __restrict_
 
 inline int nkt2(int n) { const int K = n / 3; return (K + 1) * (2 * K + 1); }
 
+// twiddle tables of every 2D size up to nmax, each as [plain plan | swapped plan]
+template <typename T>
+void tables2d(cpx<T>* h, int nmax = 256) {
+  long o = 0;
+  if (nmax >= 16) { LineFFT<16, 1, T>::host_table(h + o); LineFFT<16, 1, T, true>::host_table(h + o + 16); o += 32; }
+  if (nmax >= 32) { LineFFT<32, 1, T>::host_table(h + o); LineFFT<32, 1, T, true>::host_table(h + o + 32); o += 64; }
+  if (nmax >= 64) { LineFFT<64, 1, T>::host_table(h + o); LineFFT<64, 1, T, true>::host_table(h + o + 64); o += 128; }
+  if (nmax >= 128) { LineFFT<128, 1, T>::host_table(h + o); LineFFT<128, 1, T, true>::host_table(h + o + 128); o += 256; }
+  if (nmax >= 256) { LineFFT<256, 1, T>::host_table(h + o); LineFFT<256, 1, T, true>::host_table(h + o + 256); o += 512; }
+}
+
 // ---------------------------------------------------------------------------
 // batched host engine
 // ---------------------------------------------------------------------------
@@ -356,19 +368,12 @@ struct Batch2D final : Batch2DBase {
       woffs.push_back(total + work);
       work += 3L * sizes[i] * (sizes[i] / 3 + 1);
     }
-    const long twlen = 16 + 32 + 64 + 128 + 256;
+    const long twlen = 2 * (16 + 32 + 64 + 128 + 256);
     PSG_CUDA_TRY(cudaMalloc(&pool, sizeof(cpx<T>) * (total + work + twlen)));
     PSG_CUDA_TRY(cudaMemset(pool, 0, sizeof(cpx<T>) * (total + work + twlen)));
     twp = pool + total + work;
     std::vector<cpx<T>> h(twlen);
-    long o = 0;
-    for (int n = 16; n <= 256; n *= 2) {
-      for (int j = 0; j < n; ++j) {
-        const double a = -2.0 * M_PI * (double)j / (double)n;
-        h[o + j] = cpx<T>{(T)cos(a), (T)sin(a)};
-      }
-      o += n;
-    }
+    tables2d(h.data());
     PSG_CUDA_TRY(cudaMemcpy(twp, h.data(), sizeof(cpx<T>) * twlen, cudaMemcpyHostToDevice));
     PSG_CUDA_TRY(cudaMalloc(&d_insts, sizeof(Inst2D<T>) * ninst));
     PSG_CUDA_TRY(cudaMalloc(&d_next, sizeof(int)));
@@ -398,7 +403,7 @@ struct Batch2D final : Batch2DBase {
         case 128: gg = LineFFT<128, 1, T>::G; ss = LineFFT<128, 1, T>::SMEM; break;
         default: gg = LineFFT<256, 1, T>::G; ss = LineFFT<256, 1, T>::SMEM; break;
       }
-      worst = std::max(worst, (size_t)(n + (256 / gg) * ss));
+      worst = std::max(worst, (size_t)(2 * n + (256 / gg) * ss));
     }
     (void)g; (void)sm;
     smem = sizeof(cpx<T>) * worst;
@@ -443,7 +448,7 @@ struct Batch2D final : Batch2DBase {
     PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
     Twiddles2D<T> tws;
     long o = 0;
-    for (int q = 0, n = 16; q < 5; ++q, n *= 2) { tws.t[q] = twp + o; o += n; }
+    for (int q = 0, n = 16; q < 5; ++q, n *= 2) { tws.t[q] = twp + o; o += 2 * n; }
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -554,9 +559,9 @@ namespace {
 
 constexpr int kNoallocMaxN = 128;
 constexpr size_t kNoallocBytes = 512 * 1024;
-constexpr size_t kTw64Off = 0;          // 240 complex doubles (n = 16..128)
-constexpr size_t kTw32Off = 4096;       // 240 complex floats
-constexpr size_t kWorkOff = 8192;       // Z0..Z3 and row scratch
+constexpr size_t kTw64Off = 0;          // 480 complex doubles (n = 16..128, two plans each)
+constexpr size_t kTw32Off = 8192;       // 480 complex floats
+constexpr size_t kWorkOff = 12288;      // Z0..Z3 and row scratch
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
@@ -581,10 +586,10 @@ template <typename T>
 size_t noalloc_smem() {
   // the densest exchange layout among the supported sizes
   size_t worst = 0;
-  worst = std::max(worst, (size_t)(16 + (256 / LineFFT<16, 1, T>::G) * LineFFT<16, 1, T>::SMEM));
-  worst = std::max(worst, (size_t)(32 + (256 / LineFFT<32, 1, T>::G) * LineFFT<32, 1, T>::SMEM));
-  worst = std::max(worst, (size_t)(64 + (256 / LineFFT<64, 1, T>::G) * LineFFT<64, 1, T>::SMEM));
-  worst = std::max(worst, (size_t)(128 + (256 / LineFFT<128, 1, T>::G) * LineFFT<128, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(32 + (256 / LineFFT<16, 1, T>::G) * LineFFT<16, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(64 + (256 / LineFFT<32, 1, T>::G) * LineFFT<32, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(128 + (256 / LineFFT<64, 1, T>::G) * LineFFT<64, 1, T>::SMEM));
+  worst = std::max(worst, (size_t)(256 + (256 / LineFFT<128, 1, T>::G) * LineFFT<128, 1, T>::SMEM));
   return worst * sizeof(cpx<T>);
 }
 
@@ -606,17 +611,10 @@ int noalloc_setup(unsigned char** out) {
     psg_set_error("cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
     return PSG_ERR_CUDA;
   }
-  cpx<double> t64[240];
-  cpx<float> t32[240];
-  int o = 0;
-  for (int n = 16; n <= kNoallocMaxN; n *= 2) {
-    for (int j = 0; j < n; ++j) {
-      const double a = -2.0 * M_PI * (double)j / (double)n;
-      t64[o + j] = cpx<double>{cos(a), sin(a)};
-      t32[o + j] = cpx<float>{(float)cos(a), (float)sin(a)};
-    }
-    o += n;
-  }
+  cpx<double> t64[480];
+  cpx<float> t32[480];
+  tables2d<double>(t64, kNoallocMaxN);
+  tables2d<float>(t32, kNoallocMaxN);
   PSG_CUDA_TRY(cudaMemcpy((unsigned char*)addr + kTw64Off, t64, sizeof t64, cudaMemcpyHostToDevice));
   PSG_CUDA_TRY(cudaMemcpy((unsigned char*)addr + kTw32Off, t32, sizeof t32, cudaMemcpyHostToDevice));
   PSG_CUDA_TRY(cudaFuncSetAttribute(ns2d_single<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -642,7 +640,7 @@ int noalloc_run(unsigned char* base, int n, double nu, double dt, int nsteps, co
   I.work = work + 4 * nk;
   const cpx<T>* tw = reinterpret_cast<const cpx<T>*>(base + (sizeof(T) == 8 ? kTw64Off : kTw32Off));
   int off = 0;
-  for (int m = 16; m < n; m *= 2) off += m;
+  for (int m = 16; m < n; m *= 2) off += 2 * m;
   ns2d_single<T><<<1, 256, noalloc_smem<T>(), stream>>>(I, tw + off);
   PSG_CUDA_TRY(cudaGetLastError());
   return PSG_OK;
@@ -669,6 +667,7 @@ extern "C" int psg_ns2d_step_noalloc(int n, int precision, double nu, double dt,
   // the largest footprint must fit the array: 4 stage registers + 3 scratch rows
   const size_t need = kWorkOff + (size_t)16 * (4 * nkt2(kNoallocMaxN) + 3L * kNoallocMaxN * (kNoallocMaxN / 3 + 1));
   static_assert(kWorkOff + 16ull * (4 * 3655 + 3 * 128 * 43) <= kNoallocBytes, "scratch too small");
+  static_assert(kTw64Off + 480 * 16 <= kTw32Off && kTw32Off + 480 * 8 <= kWorkOff, "twiddle tables");
   (void)need;
   unsigned char* base = nullptr;
   int rc = noalloc_setup(&base);

@@ -77,6 +77,9 @@ struct Engine3DBase {
   virtual int layout(int* xp, void** comps) = 0;
   virtual long launch_count() const = 0;
   virtual int sync() = 0;  // wait for the stream and check the device error flag
+  // x-pass autotuner: run at set-up; report the chosen variant and timings
+  virtual int autotune() = 0;
+  virtual int tuning(int* variant, float* ms) = 0;
   // per-pass timing (A, B, C, D, E) with CUDA events between the launches
   virtual int profile(int enable) = 0;
   virtual int profile_read(double* ms, long* counts) = 0;

@@ -112,3 +112,10 @@ extern "C" int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts) {
   if (!ms || !counts) { psg_set_error("null output"); return PSG_ERR_ARG; }
   return h->e->profile_read(ms, counts);
 }
+
+extern "C" int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms) {
+  PSG_CHECK_HANDLE(h);
+  int rc = h->e->autotune();
+  if (rc) return rc;
+  return h->e->tuning(variant, ms);
+}

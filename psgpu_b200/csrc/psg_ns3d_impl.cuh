@@ -95,7 +95,7 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* s_ok, int* status)
 // grid (XT, Y): one [kz][W] tile of each state component.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int NC, int NF>
-__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
+__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G)
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
        int mask_vel, int* status) {
   using F = LineFFT<N, +1, T>;
@@ -108,11 +108,13 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);   // [NC][Y][W]
   cpx<T>* s_mir = s_in + NC * Y * W;                      // [NC][Y] mirror column
   cpx<T>* s_tw = s_mir + NC * Y;                          // [N]
-  cpx<T>* s_ex = s_tw + N;                                // [W][SX]
-  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + W * SX);  // [Y][W]
+  cpx<T>* s_ex = s_tw + N;                                // [2][W][SX]
+  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + 2 * W * SX);  // [Y][W]
 
+  // two groups of W x G threads transform two output fields at a time
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int c = tid % W, gi = tid / W;
+  const int half = tid / (W * F::G), ht = tid % (W * F::G);
+  const int c = ht % W, gi = ht / W;
   const int xt = blockIdx.x, iky = blockIdx.y;
   const long tile = ((long)xt * Y + iky) * Y * W;
   if (tid == 0) mbar_init(&s_bar, 1);
@@ -150,13 +152,15 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   const bool live_col = ikx < g.X;
   const bool mcol = mirror && c == 0;
 #pragma unroll 1
-  for (int f = 0; f < NF; ++f) {
+  for (int f0 = 0; f0 < NF; f0 += 2) {
+    const int f = f0 + half;
+    const bool live_f = f < NF;
     cpx<T> v[F::E];
 #pragma unroll
     for (int e = 0; e < F::E; ++e) {
       const int ikz = row_to_box(F::in_index(gi, e), K, N);
       cpx<T> r = czero<T>();
-      if (ikz >= 0 && live_col) {
+      if (ikz >= 0 && live_col && live_f) {
         cpx<T> xi, et, zt, rho;
         if (mcol) {
           if (iky == K && ikz == K) {
@@ -193,10 +197,12 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
       }
       v[e] = r;
     }
-    F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
-    cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
+    F::run(v, gi, s_tw, s_ex + (half * W + c) * SX, BlockSync());
+    if (live_f) {
+      cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
 #pragma unroll
-    for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * W] = v[e];
+      for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * W] = v[e];
+    }
   }
 }
 
@@ -321,80 +327,99 @@ struct RowOps {
   }
 };
 
-template <typename T, int N, int NF>
-__global__ void __launch_bounds__(128)
+// Template knobs picked by the engine's autotuner: L rows per tile (one group
+// of G lanes per row, so L*G threads) and ST pipeline stages (1: load then
+// compute; 2: the next tile's bulk copy overlaps this tile's transforms).
+template <typename T, int N, int NF, int L, int ST>
+__global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status) {
+       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int ntiles) {
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
-  constexpr int L = 128 / G;  // rows per block
   constexpr bool BOUS = (NF == 9);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ uint64_t s_bar;
+  __shared__ uint64_t s_bar[2];
   __shared__ int s_ok;
   const int K = g.K, XP = g.XP, XT = XP / kTileW;
-  cpx<T>* s_rows = reinterpret_cast<cpx<T>*>(smem_raw);  // [NF][L][XP]
-  cpx<T>* s_tw = s_rows + NF * L * XP;
-  cpx<T>* s_ex = s_tw + N;
+  const int tile_words = NF * L * XP;
+  cpx<T>* s_buf = reinterpret_cast<cpx<T>*>(smem_raw);  // [ST][NF][L][XP]
+  cpx<T>* s_tw = s_buf + ST * tile_words;                // [2N]: plain | swapped plan
+  cpx<T>* s_ex = s_tw + 2 * N;                           // [L][SX]
   const int tid = threadIdx.x, lr = tid / G, gi = tid % G;
-  const long row0 = (long)blockIdx.x * L;  // rows z*N + y
   const long plane = (long)N * N * XP;
-  if (tid == 0) mbar_init(&s_bar, 1);
+  const uint32_t bytes = (uint32_t)(L * XP * sizeof(cpx<T>));
+  if (tid == 0) { mbar_init(&s_bar[0], 1); mbar_init(&s_bar[1], 1); }
+  for (int i = tid; i < 2 * N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
-  if (tid == 0) {
-    const uint32_t bytes = (uint32_t)(L * XP * sizeof(cpx<T>));
-    mbar_expect_tx(&s_bar, NF * bytes);
-    for (int f = 0; f < NF; ++f) bulk_g2s(s_rows + f * L * XP, in + f * plane + row0 * XP, bytes, &s_bar);
-  }
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
-  if (!tile_wait(&s_bar, &s_ok, status)) return;
-
-  const long row = row0 + lr;
-  const int z = (int)(row / N), y = (int)(row % N);
-  const cpx<T>* src = s_rows + lr * XP;
-  const int fs = L * XP;  // field stride in shared memory
+  // tile t = rows [t*L, t*L + L) of every field, one bulk copy per field
+  auto issue = [&](int t, int b) {
+    mbar_expect_tx(&s_bar[b], NF * bytes);
+    for (int f = 0; f < NF; ++f)
+      bulk_g2s(s_buf + b * tile_words + f * L * XP, in + f * plane + (long)t * L * XP, bytes, &s_bar[b]);
+  };
+  int t = blockIdx.x;
+  if (tid == 0 && t < ntiles) issue(t, 0);
+  const long tstride = (long)N * N * kTileW;  // B3: successive xt tiles
+  const long fstride = (long)XT * tstride;
   cpx<T>* ex = s_ex + lr * R::SX;
-
-  T xi[E], et[E], zt[E], u[E], v[E], w[E];
-  R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
-  R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
-  R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
-  if (dump) {
-    const long base = row * N;
-    const long nr = (long)N * N * N;
+  for (int i = 0; t < ntiles; ++i, t += gridDim.x) {
+    const int b = (ST == 2) ? (i & 1) : 0;
+    const uint32_t parity = (ST == 2) ? ((i >> 1) & 1) : (i & 1);
+    const int tn = t + gridDim.x;
+    // two stages: buffer b^1 was released at the end of iteration i-1
+    if (ST == 2 && tid == 0 && tn < ntiles) issue(tn, b ^ 1);
+    if (tid == 0) s_ok = mbar_wait_bounded(&s_bar[b], parity, status) ? 1 : 0;
+    __syncthreads();
+    if (!s_ok) {
+      if (ST == 2 && tid == 0 && tn < ntiles)
+        mbar_wait_bounded(&s_bar[b ^ 1], ((i + 1) >> 1) & 1, nullptr);
+      return;
+    }
+    const long row = (long)t * L + lr;
+    const int z = (int)(row / N), y = (int)(row % N);
+    const cpx<T>* src = s_buf + b * tile_words + lr * XP;
+    const int fs = L * XP;  // field stride in shared memory
+    T xi[E], et[E], zt[E], u[E], v[E], w[E];
+    R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
+    R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
+    R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
+    if (dump) {
+      const long base = row * N;
+      const long nr = (long)N * N * N;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = R::FI::out_index(gi, e);
+        dump[base + x] = xi[e];
+        dump[nr + base + x] = et[e];
+        dump[2 * nr + base + x] = zt[e];
+      }
+    }
+    T n1[E], n2[E], n3[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const int x = R::FI::out_index(gi, e);
-      dump[base + x] = xi[e];
-      dump[nr + base + x] = et[e];
-      dump[2 * nr + base + x] = zt[e];
+      // U,V,W <- -(u x w)  (multReal)
+      n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * scale;
+      n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
+      n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
     }
-  }
-  T n1[E], n2[E], n3[E];
+    cpx<T>* dst = out + ((long)z * N + y) * kTileW;
+    const cpx<T>* two = s_tw + N;  // swapped plan for the forward transforms
+    if (!BOUS) {
+      R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
+      R::r2c_pair(n3, nullptr, K, XP, gi, two, ex, dst + 2 * fstride, nullptr, tstride);
+    } else {
+      T rx[E], ry[E], n4[E];
+      R::c2r_pair(src + 6 * fs, src + 7 * fs, K, gi, s_tw, ex, rx, ry);
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    // U,V,W <- -(u x w)  (multReal)
-    n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * scale;
-    n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
-    n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
-  }
-  // B3[f][xt][z][y][W]: tile stride between successive xt = N*N*W
-  const long tstride = (long)N * N * kTileW;
-  const long fstride = (long)XT * tstride;
-  cpx<T>* dst = out + ((long)z * N + y) * kTileW;
-  if (!BOUS) {
-    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + fstride, tstride);
-    R::r2c_pair(n3, nullptr, K, XP, gi, s_tw, ex, dst + 2 * fstride, nullptr, tstride);
-  } else {
-    T rx[E], ry[E], n4[E];
-    R::c2r_pair(src + 6 * fs, src + 7 * fs, K, gi, s_tw, ex, rx, ry);
+      for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
+      R::c2r_pair(src + 8 * fs, nullptr, K, gi, s_tw, ex, rx, ry);
 #pragma unroll
-    for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
-    R::c2r_pair(src + 8 * fs, nullptr, K, gi, s_tw, ex, rx, ry);
-#pragma unroll
-    for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
-    R::r2c_pair(n1, n2, K, XP, gi, s_tw, ex, dst, dst + fstride, tstride);
-    R::r2c_pair(n3, n4, K, XP, gi, s_tw, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
+      for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
+      R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
+      R::r2c_pair(n3, n4, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
+    }
+    __syncthreads();  // release buffer b
+    if (ST == 1 && tid == 0 && tn < ntiles) issue(tn, 0);
   }
 }
 
@@ -721,6 +746,9 @@ struct Engine3D final : Engine3DBase {
   cpx<T>* B2 = nullptr;
   double2* stage_h = nullptr;  // device FP64 staging box
   int* d_status = nullptr;     // device error flag of the bounded waits
+  int c_variant = 0;           // x-pass variant chosen by the autotuner
+  int c_resident[4] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
+  float c_ms[4] = {0, 0, 0, 0};      // autotuner timings (ms per launch)
   long launches = 0;
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
@@ -762,13 +790,18 @@ struct Engine3D final : Engine3DBase {
   // dynamic shared memory of each pass (must match the kernels' carve-up)
   size_t smem_a() const {
     return sizeof(cpx<T>) * ((size_t)nc * g.Y * kTileW + (size_t)nc * g.Y + g.n +
-                             kTileW * col_stride()) + g.Y * kTileW;
+                             2 * kTileW * col_stride()) + g.Y * kTileW;
   }
   size_t smem_b() const { return sizeof(cpx<T>) * ((size_t)g.Y * kTileW + g.n + kTileW * col_stride()); }
-  size_t smem_c() const {
-    return sizeof(cpx<T>) * ((size_t)nfi * (128 / fft_g()) * g.XP + g.n +
-                             (size_t)(128 / fft_g()) * row_stride());
+  // x-pass variants (rows per tile in units of 128/G, pipeline stages)
+  static constexpr int kCVariants = 4;
+  static int c_rows_mult(int v) { return (v & 1) ? 2 : 1; }
+  static int c_stages(int v) { return (v & 2) ? 2 : 1; }
+  size_t smem_c_v(int v) const {
+    const size_t L = (size_t)(128 / fft_g()) * c_rows_mult(v);
+    return sizeof(cpx<T>) * ((size_t)c_stages(v) * nfi * L * g.XP + 2 * g.n + L * row_stride());
   }
+  size_t smem_c() const { return smem_c_v(c_variant); }
   size_t smem_d() const { return sizeof(cpx<T>) * ((size_t)g.n * kTileW + g.n + kTileW * col_stride()); }
   size_t smem_e() const {
     return sizeof(cpx<T>) * ((size_t)nfo * g.n * kTileW + g.n + kTileW * col_stride());
@@ -829,7 +862,7 @@ struct Engine3D final : Engine3DBase {
     const long b3 = (long)nfo * n * n * g.XP;
     const long b2 = (long)nfi * n * n * g.XP;
     const long nb1 = b1 > b3 ? b1 : b3;
-    const long total = (long)nregs * nc * box + nb1 + b2 + n;
+    const long total = (long)nregs * nc * box + nb1 + b2 + 2 * n;
     PSG_CUDA_TRY(cudaMalloc(&pool, sizeof(cpx<T>) * total));
     PSG_CUDA_TRY(cudaMemset(pool, 0, sizeof(cpx<T>) * total));
     cpx<T>* p = pool;
@@ -840,19 +873,25 @@ struct Engine3D final : Engine3DBase {
       for (int q = 0; q < nc; ++q) { regs[r]->c[q] = p; p += box; }
     B1 = p; p += nb1;
     B2 = p; p += b2;
-    tw = p; p += n;
-    std::vector<cpx<T>> h(n);
-    for (int j = 0; j < n; ++j) {
-      const double a = -2.0 * M_PI * (double)j / (double)n;
-      h[j] = cpx<T>{(T)cos(a), (T)sin(a)};
+    tw = p; p += 2 * n;
+    // twiddle tables: the plain plan (column passes, inverse x rows) and the
+    // swapped plan (forward x rows)
+    std::vector<cpx<T>> h(2 * n);
+    switch (n) {
+      case 16: LineFFT<16, 1, T>::host_table(h.data()); LineFFT<16, 1, T, true>::host_table(h.data() + n); break;
+      case 32: LineFFT<32, 1, T>::host_table(h.data()); LineFFT<32, 1, T, true>::host_table(h.data() + n); break;
+      case 64: LineFFT<64, 1, T>::host_table(h.data()); LineFFT<64, 1, T, true>::host_table(h.data() + n); break;
+      case 128: LineFFT<128, 1, T>::host_table(h.data()); LineFFT<128, 1, T, true>::host_table(h.data() + n); break;
+      default: LineFFT<256, 1, T>::host_table(h.data()); LineFFT<256, 1, T, true>::host_table(h.data() + n); break;
     }
-    PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
+    PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(cpx<T>) * 2 * n, cudaMemcpyHostToDevice));
     PSG_CUDA_TRY(cudaMalloc(&stage_h, sizeof(double2) * (long)g.Y * g.Y * g.X));
     PSG_CUDA_TRY(cudaMalloc(&d_status, sizeof(int)));
     PSG_CUDA_TRY(cudaMemset(d_status, 0, sizeof(int)));
     if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN)
       PSG_CUDA_TRY(cudaMalloc(&dump, sizeof(T) * 3L * n * n * n));
-    return set_smem_limits();
+    if (int rc = set_smem_limits()) return rc;
+    return autotune();
   }
 
   ~Engine3D() override {
@@ -873,7 +912,7 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaGetDevice(&dev));
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     big -= 1024;  // static shared memory of the kernels (mbarrier, flags)
-    const size_t need[5] = {smem_a(), smem_b(), smem_c(), smem_d(), smem_e()};
+    const size_t need[5] = {smem_a(), smem_b(), smem_c_v(0), smem_d(), smem_e()};
     for (size_t x : need)
       if (x > (size_t)big) {
         psg_set_error("3D grid %d needs %zu bytes of shared memory per block, device allows %d",
@@ -884,14 +923,112 @@ struct Engine3D final : Engine3DBase {
     PSG_SMEM((pass_a<T, N, 3, 6>));
     PSG_SMEM((pass_a<T, N, 4, 9>));
     PSG_SMEM((pass_b<T, N>));
-    PSG_SMEM((pass_c<T, N, 6>));
-    PSG_SMEM((pass_c<T, N, 9>));
+    PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 1>));
+    PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 1>));
+    PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 2>));
+    PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 2>));
+    PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 1>));
+    PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 1>));
+    PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 2>));
+    PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 2>));
     PSG_SMEM((pass_d<T, N>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_HEUN>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_EULER_HEUN>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_RK4>));
     PSG_SMEM((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
 #undef PSG_SMEM
+    int nsm = 0;
+    PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    for (int v = 0; v < kCVariants; ++v) {
+      int occ = 0;
+      if (smem_c_v(v) <= (size_t)big) {
+        const void* k = c_kernel<N>(v);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, c_threads<N>(v), smem_c_v(v));
+      }
+      c_resident[v] = nsm * occ;  // 0: variant does not fit
+    }
+    return PSG_OK;
+  }
+
+  template <int N>
+  static int c_threads(int v) { return 128 * c_rows_mult(v); }
+  template <int N>
+  const void* c_kernel(int v) const {
+    constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    switch (v) {
+      case 0: return bous ? (const void*)pass_c<T, N, 9, L1, 1> : (const void*)pass_c<T, N, 6, L1, 1>;
+      case 1: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 1>;
+      case 2: return bous ? (const void*)pass_c<T, N, 9, L1, 2> : (const void*)pass_c<T, N, 6, L1, 2>;
+      default: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 2> : (const void*)pass_c<T, N, 6, 2 * L1, 2>;
+    }
+  }
+  template <int N>
+  int launch_c(int v, T scale, T* dp) {
+    constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
+    const int rows = L1 * c_rows_mult(v);
+    const int ntiles = (N * N) / rows;
+    const int grid = ntiles < c_resident[v] ? ntiles : c_resident[v];
+    const size_t sm = smem_c_v(v);
+    const int th = c_threads<N>(v);
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+#define PSG_LC(LL, STG)                                                                          \
+  if (bous) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
+  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles);
+    switch (v) {
+      case 0: PSG_LC(L1, 1); break;
+      case 1: PSG_LC(2 * L1, 1); break;
+      case 2: PSG_LC(L1, 2); break;
+      default: PSG_LC(2 * L1, 2); break;
+    }
+#undef PSG_LC
+    return PSG_OK;
+  }
+
+  // Autotuner: time every x-pass variant that fits on this device (one warm-up
+  // and three timed launches on the engine's own scratch buffers) and keep the
+  // fastest.  The transforms' cost does not depend on the data.
+  template <int N>
+  int autotune_n() {
+    cudaEvent_t a, b;
+    PSG_CUDA_TRY(cudaEventCreate(&a));
+    PSG_CUDA_TRY(cudaEventCreate(&b));
+    const T scale = (T)1 / ((T)N * (T)N * (T)N);
+    float best = 1e30f;
+    int pick = 0;
+    for (int v = 0; v < kCVariants; ++v) {
+      c_ms[v] = -1.f;
+      if (c_resident[v] <= 0) continue;
+      launch_c<N>(v, scale, nullptr);
+      cudaEventRecord(a, stream);
+      for (int r = 0; r < 3; ++r) launch_c<N>(v, scale, nullptr);
+      cudaEventRecord(b, stream);
+      cudaError_t e = cudaEventSynchronize(b);
+      if (e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); PSG_CUDA_TRY(e); }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      c_ms[v] = ms / 3.f;
+      if (c_ms[v] < best) { best = c_ms[v]; pick = v; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    c_variant = pick;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return check_status();
+  }
+  int autotune() override {
+    switch (g.n) {
+      case 16: return autotune_n<16>();
+      case 32: return autotune_n<32>();
+      case 64: return autotune_n<64>();
+      case 128: return autotune_n<128>();
+      default: return autotune_n<256>();
+    }
+  }
+  int tuning(int* variant, float* ms) override {
+    if (variant) *variant = c_variant;
+    if (ms)
+      for (int v = 0; v < kCVariants; ++v) ms[v] = c_ms[v];
     return PSG_OK;
   }
   int set_smem_limits() {
@@ -936,21 +1073,17 @@ struct Engine3D final : Engine3DBase {
     const int mv = first_rhs;
     first_rhs = 0;
     mark(-1);
+    const dim3 blk2(2 * kTileW * G);
     if (bous)
-      pass_a<T, N, 4, 9><<<dim3(XT, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
+      pass_a<T, N, 4, 9><<<dim3(XT, g.Y), blk2, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
     else
-      pass_a<T, N, 3, 6><<<dim3(XT, g.Y), blk, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
+      pass_a<T, N, 3, 6><<<dim3(XT, g.Y), blk2, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
     mark(0);
     pass_b<T, N><<<dim3(XT, N, nfi), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
     mark(1);
     const T scale = (T)1 / ((T)N * (T)N * (T)N);
-    const int rows_per_block = 128 / G;
-    const int cblocks = (N * N) / rows_per_block;
     T* dp = want_dump ? dump : nullptr;
-    if (bous)
-      pass_c<T, N, 9><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp, d_status);
-    else
-      pass_c<T, N, 6><<<cblocks, 128, smem_c(), stream>>>(g, B2, B1, tw, scale, dp, d_status);
+    launch_c<N>(c_variant, scale, dp);
     mark(2);
     pass_d<T, N><<<dim3(XT, N, nfo), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     mark(3);
