@@ -103,6 +103,40 @@ long psg_batch2d_launches(psg_batch2d* h);
 /* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]) */
 int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z);
 
+/* ---------------------------------------------------------------- UPO search */
+/* Batched Newton-GMRES-hookstep search for unstable periodic orbits of 2D
+ * Kolmogorov flow (2D_NavierStokes/src_RK4/src_gmres/main.F90:688-1823), all
+ * guesses in lock step, integrations in FP64 on the GPU.  jv_mode 0: exact
+ * tangent Jacobian-vector products of the discrete step; 1: the reference's
+ * forward difference (eps = 1e-7).  kmax: Krylov dimension (GMRESMAX). */
+typedef struct psg_upo2d psg_upo2d;
+
+#define PSG_UPO_ACTIVE 0
+#define PSG_UPO_CONVERGED 1
+#define PSG_UPO_GMRES_FAILED 2
+#define PSG_UPO_HOOK_FAILED 3
+#define PSG_UPO_STALLED 4
+#define PSG_UPO_TSTEP_FAILED 5
+#define PSG_UPO_PERIOD_TOO_SMALL 6
+#define PSG_UPO_NEWTON_FAILED 7
+
+int psg_upo2d_create(psg_upo2d** h, int nguess, int n, int kmax, int jv_mode);
+void psg_upo2d_destroy(psg_upo2d* h);
+/* guess i: state Z (complex128 box [2K+1][K+1]), period T, shifts (sx, sy),
+ * shift-reflect flag (RsymFLAG), viscosity nu = 1/Re, time step dt (TRUEDELT) */
+int psg_upo2d_set_guess(psg_upo2d* h, int i, const double* Z, double T, double sx, double sy,
+                        int rsym, double nu, double dt);
+/* Newton iterations until |F|/|Phi_T(z)| <= tol (NETOL) for every guess or
+ * max_newton; gmres_tol: GMTOL */
+int psg_upo2d_solve(psg_upo2d* h, int max_newton, double tol, double gmres_tol);
+/* vals[4] = {T, sx, sy, residual}; info[4] = {status, newton, gmres, hookstep} */
+int psg_upo2d_get(psg_upo2d* h, int i, double* Z, double* vals, int* info);
+/* building blocks at guess i (unshifted): mode 1 Phi_T(z) -> Zout; mode 0 also
+ * the tangent dPhi_T(z) q (q in/out); mode 2 dz/dt -> Zout */
+int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, double* q);
+long psg_upo2d_integrations(psg_upo2d* h);
+long psg_upo2d_launches(psg_upo2d* h);
+
 /* Allocation-free 2D step.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory when they step: a plugin

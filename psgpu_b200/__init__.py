@@ -92,6 +92,17 @@ def _declare_2d(L):
     L.psg_batch2d_launches.restype = C.c_long
     L.psg_batch2d_device_state.argtypes = [vp, i, C.POINTER(vp)]
     L.psg_ns2d_step_noalloc.argtypes = [i, i, C.c_double, C.c_double, i, vp, vp, vp]
+    L.psg_upo2d_create.argtypes = [C.POINTER(vp), i, i, i, i]
+    L.psg_upo2d_destroy.argtypes = [vp]
+    L.psg_upo2d_destroy.restype = None
+    L.psg_upo2d_set_guess.argtypes = [vp, i, dp, C.c_double, C.c_double, C.c_double, i, C.c_double, C.c_double]
+    L.psg_upo2d_solve.argtypes = [vp, i, C.c_double, C.c_double]
+    L.psg_upo2d_get.argtypes = [vp, i, dp, dp, ip]
+    L.psg_upo2d_apply.argtypes = [vp, i, i, dp, dp]
+    L.psg_upo2d_integrations.argtypes = [vp]
+    L.psg_upo2d_integrations.restype = C.c_long
+    L.psg_upo2d_launches.argtypes = [vp]
+    L.psg_upo2d_launches.restype = C.c_long
 
 
 def _check(rc):
@@ -261,3 +272,63 @@ class Batch2D:
     @property
     def launches(self) -> int:
         return int(lib().psg_batch2d_launches(self._h))
+
+
+UPO_STATUS = {0: "ACTIVE", 1: "CONVERGED", 2: "GMRES FAILED", 3: "H-STEP FAILED", 4: "NEWTON STALLED",
+              5: "T-STEP FAILED", 6: "PERIOD TOO SMALL", 7: "NEWTON FAILED"}
+
+
+class UPO2D:
+    """Batched Newton-GMRES-hookstep search for periodic orbits of 2D Kolmogorov
+    flow (all guesses of one grid size, FP64 integrations on the GPU)."""
+
+    def __init__(self, nguess: int, n: int, kmax: int = 60, exact_jv: bool = True):
+        h = C.c_void_p()
+        _check(lib().psg_upo2d_create(C.byref(h), nguess, n, kmax, 0 if exact_jv else 1))
+        self._h = h
+        self.n = n
+        self.grid = Grid2D(n)
+        self.nguess = nguess
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().psg_upo2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_guess(self, i, Z, T, sx=0.0, sy=0.0, rsym=0, nu=1 / 40, dt=0.005):
+        a = np.ascontiguousarray(Z, np.complex128).reshape(-1)
+        _check(lib().psg_upo2d_set_guess(self._h, i, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                         T, sx, sy, rsym, nu, dt))
+
+    def solve(self, max_newton=30, tol=1e-10, gmres_tol=1e-3):
+        _check(lib().psg_upo2d_solve(self._h, max_newton, tol, gmres_tol))
+
+    def get(self, i):
+        Z = np.zeros(self.grid.shape, np.complex128)
+        vals = np.zeros(4)
+        info = np.zeros(4, np.int32)
+        _check(lib().psg_upo2d_get(self._h, i, Z.ctypes.data_as(C.POINTER(C.c_double)),
+                                   vals.ctypes.data_as(C.POINTER(C.c_double)),
+                                   info.ctypes.data_as(C.POINTER(C.c_int))))
+        return {"Z": Z, "T": vals[0], "sx": vals[1], "sy": vals[2], "residual": vals[3],
+                "status": UPO_STATUS[int(info[0])], "newton": int(info[1]),
+                "gmres": int(info[2]), "hookstep": int(info[3])}
+
+    def apply(self, i, mode, q=None):
+        Z = np.zeros(self.grid.shape, np.complex128)
+        qq = None
+        if q is not None:
+            qq = np.ascontiguousarray(q, np.complex128).copy()
+        _check(lib().psg_upo2d_apply(self._h, i, mode, Z.ctypes.data_as(C.POINTER(C.c_double)),
+                                     qq.ctypes.data_as(C.POINTER(C.c_double)) if qq is not None else None))
+        return Z, qq
+
+    @property
+    def integrations(self):
+        return int(lib().psg_upo2d_integrations(self._h))

@@ -29,7 +29,7 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 
 # translation units of libpsgpu.so
 CORE = ["psg_api.cu", "psg_ns3d_api.cu", "psg_ns3d_f32.cu", "psg_ns3d_f64.cu",
-        "psg_ns2d.cu"]
+        "psg_ns2d.cu", "psg_newton2d.cu"]
 # drop-in libraries: name -> (source, macro)
 DROPINS = {
     "ns3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D"),

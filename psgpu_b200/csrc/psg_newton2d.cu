@@ -1,0 +1,1009 @@
+// psg_newton2d.cu -- batched Newton-GMRES-hookstep search for unstable periodic
+// orbits of 2D Kolmogorov flow.
+//
+// Restates the reference's UPO solver (2D_NavierStokes/src_RK4/src_gmres/
+// main.F90:688-1823): Newton on F(z,T,s) = shift_s(Phi_T(z)) - z with the two
+// extra unknowns period T and shift s and the two orthogonality rows <dz/dt, .>
+// and <dz/ds, .>; GMRES with modified Gram-Schmidt on the augmented Krylov
+// vectors; SVD of the Hessenberg matrix; the hookstep trust region with the
+// bisection on mu and the halve/double logic of the reference.  Differences in
+// form, not in algorithm:
+//   * all guesses advance in lock step and every integration of a phase (one
+//     per GMRES iteration, one per hookstep trial) is a single persistent
+//     launch over the guesses, in FP64;
+//   * Jv is either the exact tangent of the discrete step (integrated with the
+//     base, psg_tan2d.cuh) or the reference's forward difference (eps = 1e-7);
+//   * the Arnoldi orthogonalisation runs on the GPU in FP64, one block per
+//     guess; the small Hessenberg SVD runs on the host (one-sided Jacobi).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "psg_tan2d.cuh"
+#include "psgpu_internal.h"
+
+namespace psg {
+
+using C2 = cpx<double>;
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(256) tan2d_persistent(const InstTan2D<double>* __restrict__ insts,
+                                                        int ninst, int* __restrict__ next,
+                                                        const C2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2* smem = reinterpret_cast<C2*>(smem_raw);
+  __shared__ int s_idx;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_idx = atomicAdd(next, 1);
+    __syncthreads();
+    const int i = s_idx;
+    if (i >= ninst) break;
+    Tan2D<double, N>::run(insts[i], tw, smem);
+  }
+}
+
+// per-guess descriptor of the vector kernels
+struct VecJob {
+  const C2* a;
+  const C2* b;
+  const C2* c;
+  C2* out;
+  double ca, cb, cc;   // coefficients
+  double sx, sy;       // shift
+  int rsym;
+};
+
+__device__ __forceinline__ bool keep_ik(int ik, int K, int X) {
+  return keep2(ik % X, ik / X - K, K);
+}
+
+// out = ca a + cb b + cc c on kept modes, 0 elsewhere (b, c may be null)
+__global__ void vec_lincomb(const VecJob* jobs, int K, int X, int nkt) {
+  const VecJob J = jobs[blockIdx.y];
+  for (int ik = blockIdx.x * blockDim.x + threadIdx.x; ik < nkt; ik += gridDim.x * blockDim.x) {
+    C2 r = czero<double>();
+    if (keep_ik(ik, K, X)) {
+      const C2 a = J.a[ik];
+      r = C2{J.ca * a.x, J.ca * a.y};
+      if (J.b) { const C2 b = J.b[ik]; r.x += J.cb * b.x; r.y += J.cb * b.y; }
+      if (J.c) { const C2 c = J.c[ik]; r.x += J.cc * c.x; r.y += J.cc * c.y; }
+    }
+    J.out[ik] = r;
+  }
+}
+
+// out = exp(-i kx sx) exp(-i ky sy) * (rsym ? conj(a(kx,-ky)) : a(kx,ky)) on kept
+// modes (src_gmres/main.F90:718-731)
+__global__ void vec_shift(const VecJob* jobs, int K, int X, int nkt) {
+  const VecJob J = jobs[blockIdx.y];
+  for (int ik = blockIdx.x * blockDim.x + threadIdx.x; ik < nkt; ik += gridDim.x * blockDim.x) {
+    const int ikx = ik % X, iky = ik / X;
+    C2 r = czero<double>();
+    if (keep_ik(ik, K, X)) {
+      C2 a = J.rsym ? J.a[(2 * K - iky) * X + ikx] : J.a[ik];
+      if (J.rsym) a.y = -a.y;
+      const double ph = -(double)ikx * J.sx - (double)(iky - K) * J.sy;
+      double s, c;
+      sincos(ph, &s, &c);
+      r = C2{c * a.x - s * a.y, c * a.y + s * a.x};
+    }
+    J.out[ik] = r;
+  }
+}
+
+// out = -i kx a on kept modes (dZ/dS, src_gmres/main.F90:825-832)
+__global__ void vec_dkx(const VecJob* jobs, int K, int X, int nkt) {
+  const VecJob J = jobs[blockIdx.y];
+  for (int ik = blockIdx.x * blockDim.x + threadIdx.x; ik < nkt; ik += gridDim.x * blockDim.x) {
+    C2 r = czero<double>();
+    if (keep_ik(ik, K, X)) {
+      const C2 a = J.a[ik];
+      const double kx = (double)(ik % X);
+      r = C2{kx * a.y, -kx * a.x};
+    }
+    J.out[ik] = r;
+  }
+}
+
+__device__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) red[0] = s;
+  }
+  __syncthreads();
+  s = red[0];
+  __syncthreads();
+  return s;
+}
+
+// real inner products Re sum_kept conj(a) b for every guess (one block each)
+struct DotJob {
+  const C2* a;
+  const C2* b;
+  double* out;
+};
+__global__ void __launch_bounds__(256) vec_dot(const DotJob* jobs, int K, int X, int nkt) {
+  __shared__ double red[32];
+  const DotJob J = jobs[blockIdx.x];
+  double s = 0.0;
+  for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
+    if (keep_ik(ik, K, X)) {
+      const C2 a = J.a[ik], b = J.b[ik];
+      s += a.x * b.x + a.y * b.y;
+    }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) *J.out = s;
+}
+
+// Modified Gram-Schmidt of the augmented vector (v, vN1, vN2) against
+// (q_j, qN1_j, qN2_j), j < m, then H[m+1,m] and q_{m+1}
+// (src_gmres/main.F90:1130-1155).  One block per guess, FP64.
+struct MgsJob {
+  C2* v;
+  C2* const* q;     // device array of m+1 basis pointers (q[m] receives the new vector)
+  const double* qn; // host-mirrored extra rows: qN1[j], qN2[j] (2*(m+1))
+  double vn1, vn2;  // extra rows of v
+  int m;            // number of basis vectors to orthogonalise against
+  double* H;        // out: H[0..m] of column m (m+1 entries) + vN1, vN2 of q_{m+1}
+};
+__global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int X, int nkt) {
+  __shared__ double red[32];
+  const MgsJob J = jobs[blockIdx.x];
+  double vn1 = J.vn1, vn2 = J.vn2;
+  for (int j = 0; j < J.m; ++j) {
+    const C2* qj = J.q[j];
+    double s = 0.0;
+    for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
+      if (keep_ik(ik, K, X)) {
+        const C2 a = qj[ik], b = J.v[ik];
+        s += a.x * b.x + a.y * b.y;
+      }
+    double h = block_sum(s, red) + J.qn[2 * j] * vn1 + J.qn[2 * j + 1] * vn2;
+    for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
+      if (keep_ik(ik, K, X)) {
+        const C2 a = qj[ik];
+        C2 b = J.v[ik];
+        b.x -= h * a.x;
+        b.y -= h * a.y;
+        J.v[ik] = b;
+      }
+    vn1 -= h * J.qn[2 * j];
+    vn2 -= h * J.qn[2 * j + 1];
+    if (threadIdx.x == 0) J.H[j] = h;
+    __syncthreads();
+  }
+  double s = 0.0;
+  for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
+    if (keep_ik(ik, K, X)) {
+      const C2 b = J.v[ik];
+      s += b.x * b.x + b.y * b.y;
+    }
+  const double hn = sqrt(block_sum(s, red) + vn1 * vn1 + vn2 * vn2);
+  C2* qn = J.q[J.m];
+  for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
+    qn[ik] = keep_ik(ik, K, X) ? C2{J.v[ik].x / hn, J.v[ik].y / hn} : czero<double>();
+  if (threadIdx.x == 0) {
+    J.H[J.m] = hn;
+    J.H[J.m + 1] = vn1 / hn;
+    J.H[J.m + 2] = vn2 / hn;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+// thin SVD of the (r x c) column-major matrix A (r >= c) by one-sided Jacobi:
+// A = U diag(S) V^T with U (r x c), V (c x c)
+static void jacobi_svd(int r, int c, const std::vector<double>& A, std::vector<double>& U,
+                       std::vector<double>& S, std::vector<double>& V) {
+  U = A;
+  V.assign((size_t)c * c, 0.0);
+  for (int i = 0; i < c; ++i) V[(size_t)i * c + i] = 1.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < c - 1; ++p)
+      for (int q = p + 1; q < c; ++q) {
+        double a = 0, b = 0, d = 0;
+        for (int i = 0; i < r; ++i) {
+          const double x = U[(size_t)p * r + i], y = U[(size_t)q * r + i];
+          a += x * x; b += y * y; d += x * y;
+        }
+        if (fabs(d) <= 1e-300) continue;
+        off = std::max(off, fabs(d) / sqrt(a * b));
+        const double zeta = (b - a) / (2.0 * d);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int i = 0; i < r; ++i) {
+          const double x = U[(size_t)p * r + i], y = U[(size_t)q * r + i];
+          U[(size_t)p * r + i] = cs * x - sn * y;
+          U[(size_t)q * r + i] = sn * x + cs * y;
+        }
+        for (int i = 0; i < c; ++i) {
+          const double x = V[(size_t)p * c + i], y = V[(size_t)q * c + i];
+          V[(size_t)p * c + i] = cs * x - sn * y;
+          V[(size_t)q * c + i] = sn * x + cs * y;
+        }
+      }
+    if (off < 1e-15) break;
+  }
+  S.assign(c, 0.0);
+  for (int j = 0; j < c; ++j) {
+    double nrm = 0;
+    for (int i = 0; i < r; ++i) nrm += U[(size_t)j * r + i] * U[(size_t)j * r + i];
+    nrm = sqrt(nrm);
+    S[j] = nrm;
+    if (nrm > 0)
+      for (int i = 0; i < r; ++i) U[(size_t)j * r + i] /= nrm;
+  }
+}
+
+enum UpoStatus : int {
+  UPO_ACTIVE = 0,
+  UPO_CONVERGED = 1,
+  UPO_GMRES_FAILED = 2,
+  UPO_HOOK_FAILED = 3,
+  UPO_STALLED = 4,
+  UPO_TSTEP_FAILED = 5,
+  UPO_PERIOD_TOO_SMALL = 6,
+  UPO_NEWTON_FAILED = 7,
+};
+
+struct Guess {
+  // device vectors (nkt complex each)
+  C2 *z, *zn, *znshift, *fn, *dzdt, *dzndt, *dzds, *dznds, *v, *diff, *jdiff, *zplus, *zplus2,
+      *zn_trial, *zn2, *fnplus, *fnplus2, *scratch;
+  std::vector<C2*> q;  // Krylov basis
+  InstTan2D<double> inst;  // integration buffers
+  // host state
+  double T = 0, sx = 0, sy = 0, nu = 0, dt0 = 0, dt_true = 0;
+  int rsym = 0;
+  double delta = 0.1;
+  double normfn = 0, normz = 1, ner = 0, ner_old = 0;
+  int ner_count = 0;
+  int status = UPO_ACTIVE;
+  int newton = 0, gmres = 0, hook = 0;
+  std::vector<double> qn;  // qN1, qN2 per basis vector
+  std::vector<double> H;   // (kmax+1) x kmax column-major
+  int m = 0;               // GMRES iterations done in this Newton step
+  bool gmres_done = false;
+  // hookstep
+  std::vector<double> U, S, Vt, P;
+  double mu = 0, normb = 0;
+  double Tplus = 0, Splus = 0, Tplus2 = 0, Splus2 = 0;
+  double nfpred = 0, nfplus = 0, nfplus2 = 0;
+  double dT = 0, dS = 0;
+  bool halve = false, dbl = false, hook_done = false;
+  int ihook = 0;
+};
+
+struct Upo2D {
+  int ng = 0, n = 0, K = 0, X = 0, Y = 0, nkt = 0, kmax = 0, jv_mode = 0;
+  double eps = 1e-7, gmtol = 1e-3;
+  std::vector<Guess> G;
+  C2* pool = nullptr;
+  C2* tw = nullptr;
+  InstTan2D<double>* d_inst = nullptr;
+  VecJob* d_vec = nullptr;
+  DotJob* d_dot = nullptr;
+  MgsJob* d_mgs = nullptr;
+  double* d_scalars = nullptr;  // per-guess scalar outputs
+  C2** d_qptr = nullptr;
+  double* d_qn = nullptr;
+  double* d_H = nullptr;
+  int* d_next = nullptr;
+  cudaStream_t stream = 0;
+  size_t smem = 0;
+  long launches = 0, integrations = 0;
+  int grid_cap = 148;
+
+  ~Upo2D() {
+    if (pool) cudaFree(pool);
+    if (d_inst) cudaFree(d_inst);
+    if (d_vec) cudaFree(d_vec);
+    if (d_dot) cudaFree(d_dot);
+    if (d_mgs) cudaFree(d_mgs);
+    if (d_scalars) cudaFree(d_scalars);
+    if (d_qptr) cudaFree(d_qptr);
+    if (d_qn) cudaFree(d_qn);
+    if (d_H) cudaFree(d_H);
+    if (d_next) cudaFree(d_next);
+  }
+
+  int init(int ng_, int n_, int kmax_, int jv_mode_) {
+    ng = ng_; n = n_; kmax = kmax_; jv_mode = jv_mode_;
+    if (!(n == 16 || n == 32 || n == 64 || n == 128 || n == 256)) {
+      psg_set_error("UPO grid %d unsupported", n);
+      return PSG_ERR_UNSUPPORTED;
+    }
+    if (kmax < 1 || kmax > 500 || ng < 1) { psg_set_error("bad UPO sizes"); return PSG_ERR_ARG; }
+    K = n / 3; X = K + 1; Y = 2 * K + 1; nkt = X * Y;
+    const long nvec = 18 + (kmax + 1) + 10;
+    const long work = 6L * n * X;
+    const long per = nvec * nkt + work;
+    const long twl = 2L * n;
+    PSG_CUDA_TRY(cudaMalloc(&pool, sizeof(C2) * (per * ng + twl)));
+    PSG_CUDA_TRY(cudaMemset(pool, 0, sizeof(C2) * (per * ng + twl)));
+    G.resize(ng);
+    for (int g = 0; g < ng; ++g) {
+      C2* p = pool + per * g;
+      Guess& U_ = G[g];
+      C2** v[] = {&U_.z, &U_.zn, &U_.znshift, &U_.fn, &U_.dzdt, &U_.dzndt, &U_.dzds, &U_.dznds,
+                  &U_.v, &U_.diff, &U_.jdiff, &U_.zplus, &U_.zplus2, &U_.zn_trial, &U_.zn2,
+                  &U_.fnplus, &U_.fnplus2, &U_.scratch};
+      for (auto pp : v) { *pp = p; p += nkt; }
+      U_.q.resize(kmax + 1);
+      for (int j = 0; j <= kmax; ++j) { U_.q[j] = p; p += nkt; }
+      InstTan2D<double>& I = U_.inst;
+      I.n = n;
+      I.Z = p; p += nkt; I.Z0 = p; p += nkt; I.Z1 = p; p += nkt; I.Z2 = p; p += nkt; I.Z3 = p; p += nkt;
+      I.D = p; p += nkt; I.D0 = p; p += nkt; I.D1 = p; p += nkt; I.D2 = p; p += nkt; I.D3 = p; p += nkt;
+      I.work = p; p += work;
+      U_.qn.assign(2 * (kmax + 1), 0.0);
+      U_.H.assign((size_t)(kmax + 1) * kmax, 0.0);
+    }
+    tw = pool + per * ng;
+    std::vector<C2> h(2 * n);
+    switch (n) {
+      case 16: LineFFT<16, 1, double>::host_table(h.data()); LineFFT<16, 1, double, true>::host_table(h.data() + n); break;
+      case 32: LineFFT<32, 1, double>::host_table(h.data()); LineFFT<32, 1, double, true>::host_table(h.data() + n); break;
+      case 64: LineFFT<64, 1, double>::host_table(h.data()); LineFFT<64, 1, double, true>::host_table(h.data() + n); break;
+      case 128: LineFFT<128, 1, double>::host_table(h.data()); LineFFT<128, 1, double, true>::host_table(h.data() + n); break;
+      default: LineFFT<256, 1, double>::host_table(h.data()); LineFFT<256, 1, double, true>::host_table(h.data() + n); break;
+    }
+    PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C2) * 2 * n, cudaMemcpyHostToDevice));
+    PSG_CUDA_TRY(cudaMalloc(&d_inst, sizeof(InstTan2D<double>) * ng));
+    PSG_CUDA_TRY(cudaMalloc(&d_vec, sizeof(VecJob) * ng));
+    PSG_CUDA_TRY(cudaMalloc(&d_dot, sizeof(DotJob) * ng * 4));
+    PSG_CUDA_TRY(cudaMalloc(&d_mgs, sizeof(MgsJob) * ng));
+    PSG_CUDA_TRY(cudaMalloc(&d_scalars, sizeof(double) * ng * 4));
+    PSG_CUDA_TRY(cudaMalloc(&d_qptr, sizeof(C2*) * ng * (kmax + 1)));
+    PSG_CUDA_TRY(cudaMalloc(&d_qn, sizeof(double) * ng * 2 * (kmax + 1)));
+    PSG_CUDA_TRY(cudaMalloc(&d_H, sizeof(double) * ng * (kmax + 3)));
+    PSG_CUDA_TRY(cudaMalloc(&d_next, sizeof(int)));
+    std::vector<C2*> qp((size_t)ng * (kmax + 1));
+    for (int g = 0; g < ng; ++g)
+      for (int j = 0; j <= kmax; ++j) qp[(size_t)g * (kmax + 1) + j] = G[g].q[j];
+    PSG_CUDA_TRY(cudaMemcpy(d_qptr, qp.data(), sizeof(C2*) * qp.size(), cudaMemcpyHostToDevice));
+    int gg = 0, sm = 0;
+    switch (n) {
+      case 16: gg = LineFFT<16, 1, double>::G; sm = LineFFT<16, 1, double>::SMEM; break;
+      case 32: gg = LineFFT<32, 1, double>::G; sm = LineFFT<32, 1, double>::SMEM; break;
+      case 64: gg = LineFFT<64, 1, double>::G; sm = LineFFT<64, 1, double>::SMEM; break;
+      case 128: gg = LineFFT<128, 1, double>::G; sm = LineFFT<128, 1, double>::SMEM; break;
+      default: gg = LineFFT<256, 1, double>::G; sm = LineFFT<256, 1, double>::SMEM; break;
+    }
+    smem = sizeof(C2) * (2 * n + (256 / gg) * sm);
+    PSG_CUDA_TRY(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(), 256, smem);
+    grid_cap = nsm * std::max(occ, 1);
+    return PSG_OK;
+  }
+
+  const void* kernel() const {
+    switch (n) {
+      case 16: return (const void*)tan2d_persistent<16>;
+      case 32: return (const void*)tan2d_persistent<32>;
+      case 64: return (const void*)tan2d_persistent<64>;
+      case 128: return (const void*)tan2d_persistent<128>;
+      default: return (const void*)tan2d_persistent<256>;
+    }
+  }
+
+  // ----- batched integration: for every guess in `who`, integrate from z_in
+  // (and, mode 0, the perturbation d_in) over its period T with its time step
+  struct IntReq {
+    int g;
+    const C2* z_in;
+    const C2* d_in;
+    double T;
+    int mode;
+  };
+  int integrate(const std::vector<IntReq>& reqs) {
+    if (reqs.empty()) return PSG_OK;
+    std::vector<InstTan2D<double>> h;
+    for (const IntReq& r : reqs) {
+      Guess& U_ = G[r.g];
+      InstTan2D<double> I = U_.inst;
+      I.mode = r.mode;
+      I.nu = U_.nu;
+      if (r.mode == 2) {
+        I.nsteps = 0;
+        I.dt = 0;
+      } else {
+        // NSTOP = INT(T/DELT); DELT = T/NSTOP (src_gmres/main.F90:697-699)
+        int ns = (int)(r.T / U_.dt_true);
+        if (ns < 1) ns = 1;
+        I.nsteps = ns;
+        I.dt = r.T / (double)ns;
+      }
+      PSG_CUDA_TRY(cudaMemcpyAsync(I.Z, r.z_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
+      if (r.mode == 0)
+        PSG_CUDA_TRY(cudaMemcpyAsync(I.D, r.d_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
+      h.push_back(I);
+    }
+    // longest first
+    std::stable_sort(h.begin(), h.end(), [](const InstTan2D<double>& a, const InstTan2D<double>& b) {
+      return a.nsteps * (a.mode == 0 ? 5 : 3) > b.nsteps * (b.mode == 0 ? 5 : 3);
+    });
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_inst, h.data(), sizeof(InstTan2D<double>) * h.size(),
+                                 cudaMemcpyHostToDevice, stream));
+    PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
+    const int grid = std::min<int>((int)h.size(), grid_cap);
+    switch (n) {
+      case 16: tan2d_persistent<16><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
+      case 32: tan2d_persistent<32><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
+      case 64: tan2d_persistent<64><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
+      case 128: tan2d_persistent<128><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
+      default: tan2d_persistent<256><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
+    }
+    ++launches;
+    integrations += (long)h.size();
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  int vec_launch(void (*k)(const VecJob*, int, int, int), const std::vector<VecJob>& jobs) {
+    if (jobs.empty()) return PSG_OK;
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_vec, jobs.data(), sizeof(VecJob) * jobs.size(),
+                                 cudaMemcpyHostToDevice, stream));
+    k<<<dim3((nkt + 255) / 256, (unsigned)jobs.size()), 256, 0, stream>>>(d_vec, K, X, nkt);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  // dots[i] = <a_i, b_i> (synchronous)
+  int dots(const std::vector<std::pair<const C2*, const C2*>>& ab, std::vector<double>& out) {
+    out.assign(ab.size(), 0.0);
+    if (ab.empty()) return PSG_OK;
+    std::vector<DotJob> j(ab.size());
+    for (size_t i = 0; i < ab.size(); ++i) j[i] = DotJob{ab[i].first, ab[i].second, d_scalars + i};
+    if (ab.size() > (size_t)ng * 4) { psg_set_error("too many dot products"); return PSG_ERR_ARG; }
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_dot, j.data(), sizeof(DotJob) * j.size(), cudaMemcpyHostToDevice, stream));
+    vec_dot<<<(unsigned)j.size(), 256, 0, stream>>>(d_dot, K, X, nkt);
+    ++launches;
+    PSG_CUDA_TRY(cudaMemcpyAsync(out.data(), d_scalars, sizeof(double) * ab.size(),
+                                 cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return PSG_OK;
+  }
+
+  int shift(const std::vector<int>& who, C2* Guess::*out, const C2* Guess::*in, double Guess::*sx) {
+    std::vector<VecJob> jobs;
+    for (int g : who) {
+      VecJob J{};
+      J.a = G[g].*in; J.out = G[g].*out; J.sx = G[g].*sx; J.sy = G[g].sy; J.rsym = G[g].rsym;
+      jobs.push_back(J);
+    }
+    return vec_launch(vec_shift, jobs);
+  }
+  int shift_ptr(const std::vector<int>& who, const std::vector<const C2*>& in,
+                const std::vector<C2*>& out, const std::vector<double>& sx) {
+    std::vector<VecJob> jobs;
+    for (size_t i = 0; i < who.size(); ++i) {
+      VecJob J{};
+      J.a = in[i]; J.out = out[i]; J.sx = sx[i]; J.sy = G[who[i]].sy; J.rsym = G[who[i]].rsym;
+      jobs.push_back(J);
+    }
+    return vec_launch(vec_shift, jobs);
+  }
+  int lincomb(const std::vector<VecJob>& jobs) { return vec_launch(vec_lincomb, jobs); }
+
+  static VecJob lc(C2* out, const C2* a, double ca, const C2* b = nullptr, double cb = 0,
+                   const C2* c = nullptr, double cc = 0) {
+    VecJob J{};
+    J.out = out; J.a = a; J.ca = ca; J.b = b; J.cb = cb; J.c = c; J.cc = cc;
+    return J;
+  }
+
+  int copy_out(const std::vector<int>& who, C2* Guess::*dst, bool from_D) {
+    for (int g : who)
+      PSG_CUDA_TRY(cudaMemcpyAsync(G[g].*dst, from_D ? G[g].inst.D : G[g].inst.Z, sizeof(C2) * nkt,
+                                   cudaMemcpyDeviceToDevice, stream));
+    return PSG_OK;
+  }
+
+  // J q for every guess in `who` (q from the pointer list), written to `out`:
+  // shift(dPhi_T(z) q) - q + dZN/dS q_s + dZN/dt q_T (src_gmres/main.F90:1100-1116)
+  int apply_j(const std::vector<int>& who, const std::vector<const C2*>& q,
+              const std::vector<double>& qs, const std::vector<double>& qt, C2* Guess::*out) {
+    std::vector<IntReq> reqs;
+    std::vector<VecJob> jobs;
+    if (jv_mode == 0) {
+      for (size_t i = 0; i < who.size(); ++i)
+        reqs.push_back(IntReq{who[i], G[who[i]].z, q[i], G[who[i]].T, 0});
+      if (int rc = integrate(reqs)) return rc;
+      std::vector<const C2*> src;
+      std::vector<C2*> dst;
+      std::vector<double> sx;
+      for (int g : who) { src.push_back(G[g].inst.D); dst.push_back(G[g].*out); sx.push_back(G[g].sx); }
+      if (int rc = shift_ptr(who, src, dst, sx)) return rc;
+    } else {
+      // forward difference with eps = 1e-7 (src_gmres/main.F90:1048-1108)
+      for (size_t i = 0; i < who.size(); ++i) jobs.push_back(lc(G[who[i]].scratch, G[who[i]].z, 1.0, q[i], eps));
+      if (int rc = lincomb(jobs)) return rc;
+      for (int g : who) reqs.push_back(IntReq{g, G[g].scratch, nullptr, G[g].T, 1});
+      if (int rc = integrate(reqs)) return rc;
+      jobs.clear();
+      for (int g : who) jobs.push_back(lc(G[g].scratch, G[g].inst.Z, 1.0 / eps, G[g].zn, -1.0 / eps));
+      if (int rc = lincomb(jobs)) return rc;
+      std::vector<const C2*> src;
+      std::vector<C2*> dst;
+      std::vector<double> sx;
+      for (int g : who) { src.push_back(G[g].scratch); dst.push_back(G[g].*out); sx.push_back(G[g].sx); }
+      if (int rc = shift_ptr(who, src, dst, sx)) return rc;
+    }
+    jobs.clear();
+    for (size_t i = 0; i < who.size(); ++i)
+      jobs.push_back(lc(G[who[i]].*out, G[who[i]].*out, 1.0, q[i], -1.0, G[who[i]].dznds, qs[i]));
+    if (int rc = lincomb(jobs)) return rc;
+    jobs.clear();
+    for (size_t i = 0; i < who.size(); ++i)
+      jobs.push_back(lc(G[who[i]].*out, G[who[i]].*out, 1.0, G[who[i]].dzndt, qt[i]));
+    return lincomb(jobs);
+  }
+
+  // F = shift(Phi_T(z)) - z, norms and residual for the guesses in `who`
+  int residual(const std::vector<int>& who) {
+    std::vector<IntReq> reqs;
+    for (int g : who) reqs.push_back(IntReq{g, G[g].z, nullptr, G[g].T, 1});
+    if (int rc = integrate(reqs)) return rc;
+    if (int rc = copy_out(who, &Guess::zn, false)) return rc;
+    if (int rc = shift(who, &Guess::znshift, (const C2* Guess::*)&Guess::zn, &Guess::sx)) return rc;
+    std::vector<VecJob> jobs;
+    for (int g : who) jobs.push_back(lc(G[g].fn, G[g].znshift, 1.0, G[g].z, -1.0));
+    if (int rc = lincomb(jobs)) return rc;
+    std::vector<std::pair<const C2*, const C2*>> ab;
+    for (int g : who) { ab.push_back({G[g].zn, G[g].zn}); ab.push_back({G[g].fn, G[g].fn}); }
+    std::vector<double> d;
+    if (int rc = dots(ab, d)) return rc;
+    for (size_t i = 0; i < who.size(); ++i) {
+      Guess& U_ = G[who[i]];
+      U_.normz = sqrt(d[2 * i]);
+      U_.normfn = sqrt(d[2 * i + 1]);
+      U_.ner = U_.normfn / U_.normz;
+    }
+    return PSG_OK;
+  }
+
+  // x(mu) = P S / (mu + S^2), its norm
+  static double xnorm(const Guess& U_, int m, double mu, std::vector<double>& x) {
+    x.assign(m, 0.0);
+    double s = 0;
+    for (int j = 0; j < m; ++j) {
+      x[j] = (mu == 0.0) ? U_.P[j] / U_.S[j] : U_.P[j] * U_.S[j] / (mu + U_.S[j] * U_.S[j]);
+      s += x[j] * x[j];
+    }
+    return sqrt(s);
+  }
+
+  // mu so that delta/sqrt2 < |x| < sqrt2 delta (src_gmres/main.F90:1283-1335);
+  // returns the step y = V x in the Krylov basis
+  static void hook_step(Guess& U_, int m, std::vector<double>& y) {
+    const double root2 = sqrt(2.0);
+    std::vector<double> x;
+    double nx = xnorm(U_, m, 0.0, x);
+    U_.mu = 0.0;
+    if (nx > root2 * U_.delta) {
+      double mu1 = 0.0, mu2 = *std::max_element(U_.S.begin(), U_.S.begin() + m);
+      nx = xnorm(U_, m, mu2, x);
+      for (int it = 0; it < 2000 && !(nx < U_.delta); ++it) {
+        mu1 = mu2;
+        mu2 = 2.0 * mu2;
+        nx = xnorm(U_, m, mu2, x);
+      }
+      double mid = mu2;
+      for (int it = 0; it < 2000 && !(nx < root2 * U_.delta && nx > U_.delta / root2); ++it) {
+        mid = 0.5 * (mu2 + mu1);
+        nx = xnorm(U_, m, mid, x);
+        if (nx > U_.delta) mu1 = mid;
+        else mu2 = mid;
+      }
+      U_.mu = mid;
+    }
+    y.assign(m, 0.0);
+    for (int i = 0; i < m; ++i) {
+      double a = 0;
+      for (int j = 0; j < m; ++j) a += U_.Vt[(size_t)j * m + i] * x[j];
+      y[i] = a;
+    }
+  }
+
+  int solve(int max_newton, double tol) {
+    std::vector<int> act;
+    for (int g = 0; g < ng; ++g)
+      if (G[g].status == UPO_ACTIVE) act.push_back(g);
+    if (int rc = residual(act)) return rc;
+    for (int g : act)
+      if (G[g].ner <= tol) G[g].status = UPO_CONVERGED;
+    std::vector<C2*> qdev;
+    for (int it = 0; it < max_newton; ++it) {
+      act.clear();
+      for (int g = 0; g < ng; ++g)
+        if (G[g].status == UPO_ACTIVE) act.push_back(g);
+      if (act.empty()) break;
+      std::vector<VecJob> jobs;
+      for (int g : act) {
+        Guess& U_ = G[g];
+        U_.newton += 1;
+        U_.normb = U_.normfn;
+        U_.m = 0;
+        U_.gmres_done = false;
+        std::fill(U_.H.begin(), U_.H.end(), 0.0);
+        std::fill(U_.qn.begin(), U_.qn.end(), 0.0);
+        jobs.push_back(lc(U_.q[0], U_.fn, -1.0 / U_.normb));
+      }
+      if (int rc = lincomb(jobs)) return rc;
+      // dZN/dt and dz/dt (TIMEDERIV), dZN/dS and dz/dS
+      {
+        std::vector<IntReq> reqs;
+        for (int g : act) reqs.push_back(IntReq{g, G[g].znshift, nullptr, 0.0, 2});
+        if (int rc = integrate(reqs)) return rc;
+        if (int rc = copy_out(act, &Guess::dzndt, true)) return rc;
+        reqs.clear();
+        for (int g : act) reqs.push_back(IntReq{g, G[g].z, nullptr, 0.0, 2});
+        if (int rc = integrate(reqs)) return rc;
+        if (int rc = copy_out(act, &Guess::dzdt, true)) return rc;
+        std::vector<VecJob> dj;
+        for (int g : act) { VecJob J{}; J.a = G[g].znshift; J.out = G[g].dznds; dj.push_back(J); }
+        if (int rc = vec_launch(vec_dkx, dj)) return rc;
+        dj.clear();
+        for (int g : act) { VecJob J{}; J.a = G[g].z; J.out = G[g].dzds; dj.push_back(J); }
+        if (int rc = vec_launch(vec_dkx, dj)) return rc;
+      }
+      // ------------------------------------------------------------- GMRES
+      for (int k = 0; k < kmax; ++k) {
+        std::vector<int> ga;
+        for (int g : act)
+          if (!G[g].gmres_done) ga.push_back(g);
+        if (ga.empty()) break;
+        std::vector<const C2*> q;
+        std::vector<double> qs, qt;
+        for (int g : ga) { q.push_back(G[g].q[k]); qt.push_back(G[g].qn[2 * k]); qs.push_back(G[g].qn[2 * k + 1]); }
+        if (int rc = apply_j(ga, q, qs, qt, &Guess::v)) return rc;
+        std::vector<std::pair<const C2*, const C2*>> ab;
+        for (int g : ga) { ab.push_back({G[g].dzdt, G[g].q[k]}); ab.push_back({G[g].dzds, G[g].q[k]}); }
+        std::vector<double> vn;
+        if (int rc = dots(ab, vn)) return rc;
+        std::vector<MgsJob> mj;
+        std::vector<double> qnh;
+        for (size_t i = 0; i < ga.size(); ++i) {
+          const int g = ga[i];
+          MgsJob J{};
+          J.v = G[g].v;
+          J.q = d_qptr + (size_t)g * (kmax + 1);
+          J.qn = d_qn + (size_t)i * 2 * (kmax + 1);
+          J.vn1 = vn[2 * i];
+          J.vn2 = vn[2 * i + 1];
+          J.m = k + 1;
+          J.H = d_H + (size_t)i * (kmax + 3);
+          mj.push_back(J);
+          qnh.insert(qnh.end(), G[g].qn.begin(), G[g].qn.end());
+        }
+        PSG_CUDA_TRY(cudaMemcpyAsync(d_qn, qnh.data(), sizeof(double) * qnh.size(), cudaMemcpyHostToDevice, stream));
+        PSG_CUDA_TRY(cudaMemcpyAsync(d_mgs, mj.data(), sizeof(MgsJob) * mj.size(), cudaMemcpyHostToDevice, stream));
+        // MgsJob.q points at the basis pointer array: q[0..k] existing, q[k+1] new
+        mgs_kernel<<<(unsigned)mj.size(), 256, 0, stream>>>(d_mgs, K, X, nkt);
+        ++launches;
+        std::vector<double> hh(ga.size() * (kmax + 3));
+        PSG_CUDA_TRY(cudaMemcpyAsync(hh.data(), d_H, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, stream));
+        PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+        PSG_CUDA_TRY(cudaGetLastError());
+        for (size_t i = 0; i < ga.size(); ++i) {
+          Guess& U_ = G[ga[i]];
+          const double* h = hh.data() + i * (kmax + 3);
+          const int rows = kmax + 1;
+          for (int j = 0; j <= k + 1; ++j) U_.H[(size_t)k * rows + j] = h[j];
+          U_.qn[2 * (k + 1)] = h[k + 2];
+          U_.qn[2 * (k + 1) + 1] = h[k + 3];
+          // SVD of H(1:k+2, 1:k+1) and the GMRES residual (src_gmres/main.F90:1161-1228)
+          const int r = k + 2, c = k + 1;
+          std::vector<double> A((size_t)r * c);
+          for (int cc = 0; cc < c; ++cc)
+            for (int rr = 0; rr < r; ++rr) A[(size_t)cc * r + rr] = U_.H[(size_t)cc * rows + rr];
+          std::vector<double> Um, Sm, Vm;
+          jacobi_svd(r, c, A, Um, Sm, Vm);
+          U_.P.assign(c, 0.0);
+          for (int j = 0; j < c; ++j) U_.P[j] = U_.normb * Um[(size_t)j * r + 0];
+          U_.S = Sm;
+          U_.Vt.assign((size_t)c * c, 0.0);
+          for (int a = 0; a < c; ++a)
+            for (int b = 0; b < c; ++b) U_.Vt[(size_t)a * c + b] = Vm[(size_t)a * c + b];
+          // GMR = | H y - |b| e1 | / |b| with y = V x, x = P / S
+          std::vector<double> y(c, 0.0), hy(r, 0.0);
+          for (int ii = 0; ii < c; ++ii) {
+            double a = 0;
+            for (int j = 0; j < c; ++j) a += Vm[(size_t)j * c + ii] * (Sm[j] > 0 ? U_.P[j] / Sm[j] : 0.0);
+            y[ii] = a;
+          }
+          for (int rr = 0; rr < r; ++rr) {
+            double a = 0;
+            for (int cc = 0; cc < c; ++cc) a += U_.H[(size_t)cc * rows + rr] * y[cc];
+            hy[rr] = a;
+          }
+          hy[0] -= U_.normb;
+          double gmr = 0;
+          for (double t : hy) gmr += t * t;
+          gmr = sqrt(gmr) / U_.normb;
+          if (gmr <= gmtol || k + 1 == kmax) {
+            U_.m = k + 1;
+            U_.gmres_done = true;
+            U_.gmres += k + 1;
+            if (gmr > gmtol) U_.status = UPO_GMRES_FAILED;
+          }
+        }
+      }
+      // ------------------------------------------------------------- hookstep
+      std::vector<int> ha;
+      for (int g : act)
+        if (G[g].status == UPO_ACTIVE) {
+          G[g].ihook = 0; G[g].halve = false; G[g].dbl = false; G[g].hook_done = false;
+          ha.push_back(g);
+        }
+      for (int round = 0; round < 64; ++round) {
+        std::vector<int> hr;
+        for (int g : ha)
+          if (!G[g].hook_done) hr.push_back(g);
+        if (hr.empty()) break;
+        std::vector<int> live;
+        for (int g : hr) {
+          Guess& U_ = G[g];
+          U_.ihook += 1;
+          if (U_.ihook > 50) { U_.status = UPO_HOOK_FAILED; U_.hook_done = true; continue; }
+          live.push_back(g);
+        }
+        if (live.empty()) break;
+        // step y in the Krylov basis; DIFF = Q y, DIFFT, DIFFS
+        std::vector<double> coef((size_t)live.size() * (kmax + 1), 0.0);
+        std::vector<VecJob> jobs2;
+        for (size_t i = 0; i < live.size(); ++i) {
+          Guess& U_ = G[live[i]];
+          std::vector<double> y;
+          hook_step(U_, U_.m, y);
+          U_.dT = 0; U_.dS = 0;
+          for (int j = 0; j < U_.m; ++j) { U_.dT += U_.qn[2 * j] * y[j]; U_.dS += U_.qn[2 * j + 1] * y[j]; }
+          // diff = sum_j y_j q_j, accumulated three basis vectors per launch
+          for (int j = 0; j < U_.m; ++j) coef[i * (kmax + 1) + j] = y[j];
+        }
+        for (int j = 0; j < kmax; ++j) {
+          jobs2.clear();
+          bool any = false;
+          for (size_t i = 0; i < live.size(); ++i) {
+            Guess& U_ = G[live[i]];
+            if (j >= U_.m) continue;
+            any = true;
+            const double cj = coef[i * (kmax + 1) + j];
+            jobs2.push_back(j == 0 ? lc(U_.diff, U_.q[0], cj) : lc(U_.diff, U_.diff, 1.0, U_.q[j], cj));
+          }
+          if (!any) break;
+          if (int rc = lincomb(jobs2)) return rc;
+        }
+        // J DIFF and the predicted residual
+        std::vector<const C2*> dq;
+        std::vector<double> qs, qt;
+        for (int g : live) { dq.push_back(G[g].diff); qs.push_back(G[g].dS); qt.push_back(G[g].dT); }
+        if (int rc = apply_j(live, dq, qs, qt, &Guess::jdiff)) return rc;
+        jobs2.clear();
+        for (int g : live) jobs2.push_back(lc(G[g].scratch, G[g].fn, 1.0, G[g].jdiff, 1.0));
+        if (int rc = lincomb(jobs2)) return rc;
+        // trial: z + DIFF over T + DIFFT with shift s + DIFFS
+        jobs2.clear();
+        for (int g : live) jobs2.push_back(lc(G[g].zplus, G[g].z, 1.0, G[g].diff, 1.0));
+        if (int rc = lincomb(jobs2)) return rc;
+        std::vector<IntReq> reqs;
+        for (int g : live) {
+          G[g].Tplus = G[g].T + G[g].dT;
+          G[g].Splus = G[g].sx + G[g].dS;
+          reqs.push_back(IntReq{g, G[g].zplus, nullptr, G[g].Tplus, 1});
+        }
+        if (int rc = integrate(reqs)) return rc;
+        if (int rc = copy_out(live, &Guess::zn_trial, false)) return rc;
+        {
+          std::vector<const C2*> src;
+          std::vector<C2*> dst;
+          std::vector<double> sx;
+          for (int g : live) { src.push_back(G[g].zn_trial); dst.push_back(G[g].fnplus); sx.push_back(G[g].Splus); }
+          if (int rc = shift_ptr(live, src, dst, sx)) return rc;
+        }
+        jobs2.clear();
+        for (int g : live) jobs2.push_back(lc(G[g].fnplus, G[g].fnplus, 1.0, G[g].zplus, -1.0));
+        if (int rc = lincomb(jobs2)) return rc;
+        std::vector<std::pair<const C2*, const C2*>> ab;
+        for (int g : live) { ab.push_back({G[g].scratch, G[g].scratch}); ab.push_back({G[g].fnplus, G[g].fnplus}); }
+        std::vector<double> d;
+        if (int rc = dots(ab, d)) return rc;
+        // accept / retry logic (src_gmres/main.F90:1523-1622)
+        for (size_t i = 0; i < live.size(); ++i) {
+          Guess& U_ = G[live[i]];
+          U_.nfpred = sqrt(d[2 * i]);
+          U_.nfplus = sqrt(d[2 * i + 1]);
+          const double normb_pred = U_.normfn;  // |FN + 0*J DIFF|
+          auto save = [&]() {
+            cudaMemcpyAsync(U_.zplus2, U_.zplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(U_.zn2, U_.zn_trial, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(U_.fnplus2, U_.fnplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            U_.Tplus2 = U_.Tplus; U_.Splus2 = U_.Splus; U_.nfplus2 = U_.nfplus;
+          };
+          auto revert = [&]() {
+            cudaMemcpyAsync(U_.zplus, U_.zplus2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(U_.zn_trial, U_.zn2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(U_.fnplus, U_.fnplus2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+            U_.Tplus = U_.Tplus2; U_.Splus = U_.Splus2; U_.nfplus = U_.nfplus2;
+          };
+          if (U_.nfplus != U_.nfplus || U_.nfpred != U_.nfpred) {
+            U_.delta *= 0.5; U_.halve = true;
+            continue;
+          }
+          if (U_.nfplus >= normb_pred) {
+            if (U_.dbl) { revert(); U_.delta *= 0.5; U_.hook_done = true; continue; }
+            U_.delta *= 0.5; U_.halve = true;
+          } else {
+            if (U_.halve) { U_.hook_done = true; continue; }
+            if (U_.dbl && U_.nfplus > U_.nfplus2) { revert(); U_.delta *= 0.5; U_.hook_done = true; continue; }
+            if (U_.mu == 0.0) { U_.hook_done = true; }
+            else if (fabs(U_.nfpred - U_.nfplus) < 0.1 * fabs(U_.nfplus - U_.normfn)) {
+              U_.delta *= 2.0; U_.dbl = true; save();
+            } else if (U_.nfplus < U_.nfpred) {
+              U_.delta *= 2.0; U_.dbl = true; save();
+            } else {
+              U_.hook_done = true;
+            }
+          }
+        }
+      }
+      // ------------------------------------------------------------- update
+      std::vector<int> up;
+      for (int g : ha) {
+        Guess& U_ = G[g];
+        U_.hook += U_.ihook;
+        if (U_.status != UPO_ACTIVE) continue;
+        up.push_back(g);
+        cudaMemcpyAsync(U_.zn, U_.zn_trial, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(U_.z, U_.zplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(U_.fn, U_.fnplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
+        U_.T = U_.Tplus;
+        U_.sx = U_.Splus;
+        U_.normfn = U_.nfplus;
+      }
+      if (int rc = shift(up, &Guess::znshift, (const C2* Guess::*)&Guess::zn, &Guess::sx)) return rc;
+      std::vector<std::pair<const C2*, const C2*>> ab;
+      for (int g : up) ab.push_back({G[g].zn, G[g].zn});
+      std::vector<double> d;
+      if (int rc = dots(ab, d)) return rc;
+      for (size_t i = 0; i < up.size(); ++i) {
+        Guess& U_ = G[up[i]];
+        U_.normz = sqrt(d[i]);
+        const double ner = U_.normfn / U_.normz;
+        if (ner != ner) { U_.status = UPO_TSTEP_FAILED; continue; }
+        // stall detection (src_gmres/main.F90:1752-1765)
+        const double rel = fabs((ner - U_.ner_old) / ner);
+        if (rel < 0.001) {
+          if (++U_.ner_count > 3) U_.status = UPO_STALLED;
+        } else {
+          U_.ner_count = 0;
+        }
+        U_.ner_old = ner;
+        U_.ner = ner;
+        if (ner <= tol) U_.status = UPO_CONVERGED;
+        else if (U_.T < 0.1) U_.status = UPO_PERIOD_TOO_SMALL;
+        else if (U_.newton >= max_newton && U_.status == UPO_ACTIVE) U_.status = UPO_NEWTON_FAILED;
+      }
+    }
+    for (int g = 0; g < ng; ++g)
+      if (G[g].status == UPO_ACTIVE) G[g].status = UPO_NEWTON_FAILED;
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return PSG_OK;
+  }
+};
+
+}  // namespace psg
+
+using namespace psg;
+
+struct psg_upo2d {
+  Upo2D* u = nullptr;
+};
+
+#define PSG_U2(h)                                                                  \
+  do {                                                                             \
+    if (!(h) || !(h)->u) { psg_set_error("null UPO handle"); return PSG_ERR_ARG; } \
+  } while (0)
+
+extern "C" int psg_upo2d_create(psg_upo2d** out, int nguess, int n, int kmax, int jv_mode) {
+  if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  *out = nullptr;
+  if (jv_mode != 0 && jv_mode != 1) { psg_set_error("jv_mode: 0 exact tangent, 1 finite difference"); return PSG_ERR_ARG; }
+  psg_upo2d* h = new psg_upo2d();
+  h->u = new Upo2D();
+  int rc = h->u->init(nguess, n, kmax, jv_mode);
+  if (rc) { delete h->u; delete h; return rc; }
+  *out = h;
+  return PSG_OK;
+}
+
+extern "C" void psg_upo2d_destroy(psg_upo2d* h) {
+  if (!h) return;
+  delete h->u;
+  delete h;
+}
+
+extern "C" int psg_upo2d_set_guess(psg_upo2d* h, int i, const double* Z, double T, double sx,
+                                   double sy, int rsym, double nu, double dt) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  if (i < 0 || i >= U.ng || !Z || T <= 0 || dt <= 0) { psg_set_error("bad guess"); return PSG_ERR_ARG; }
+  Guess& g = U.G[i];
+  std::vector<C2> z((size_t)U.nkt);
+  const int K = U.K, X = U.X;
+  for (int ik = 0; ik < U.nkt; ++ik) {
+    const int ikx = ik % X, ky = ik / X - K;
+    const bool keep = !(ikx == 0 && ky <= 0) && 4 * (ikx * ikx + ky * ky) <= (2 * K - 1) * (2 * K - 1);
+    z[ik] = keep ? C2{Z[2 * ik], Z[2 * ik + 1]} : C2{0.0, 0.0};
+  }
+  PSG_CUDA_TRY(cudaMemcpy(g.z, z.data(), sizeof(C2) * U.nkt, cudaMemcpyHostToDevice));
+  g.T = T; g.sx = sx; g.sy = sy; g.rsym = rsym; g.nu = nu; g.dt0 = dt; g.dt_true = dt;
+  // a guess period from a run with this time step is taken as exact
+  // (src_gmres/main.F90:688-695)
+  if (fabs(T - nearbyint(T / dt) * dt) < 1e-10) g.T = nearbyint(T / dt) * dt;
+  g.delta = 0.1; g.status = UPO_ACTIVE; g.newton = g.gmres = g.hook = 0;
+  g.ner_old = 0; g.ner_count = 0;
+  return PSG_OK;
+}
+
+extern "C" int psg_upo2d_solve(psg_upo2d* h, int max_newton, double tol, double gmres_tol) {
+  PSG_U2(h);
+  h->u->gmtol = gmres_tol;
+  return h->u->solve(max_newton, tol);
+}
+
+extern "C" int psg_upo2d_get(psg_upo2d* h, int i, double* Z, double* vals, int* info) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  if (i < 0 || i >= U.ng) { psg_set_error("guess %d out of range", i); return PSG_ERR_ARG; }
+  Guess& g = U.G[i];
+  if (Z) PSG_CUDA_TRY(cudaMemcpy(Z, g.z, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
+  if (vals) { vals[0] = g.T; vals[1] = g.sx; vals[2] = g.sy; vals[3] = g.ner; }
+  if (info) { info[0] = g.status; info[1] = g.newton; info[2] = g.gmres; info[3] = g.hook; }
+  return PSG_OK;
+}
+
+// building blocks at guess i: Phi_T(z) (mode 1), the tangent dPhi_T(z) q
+// (mode 0, q in/out) or dz/dt (mode 2); all unshifted
+extern "C" int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, double* q) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  if (i < 0 || i >= U.ng || mode < 0 || mode > 2) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  Guess& g = U.G[i];
+  if (mode == 0) {
+    if (!q) { psg_set_error("null perturbation"); return PSG_ERR_ARG; }
+    PSG_CUDA_TRY(cudaMemcpy(g.scratch, q, sizeof(C2) * U.nkt, cudaMemcpyHostToDevice));
+  }
+  std::vector<Upo2D::IntReq> r{Upo2D::IntReq{i, g.z, g.scratch, g.T, mode}};
+  if (int rc = U.integrate(r)) return rc;
+  PSG_CUDA_TRY(cudaStreamSynchronize(U.stream));
+  if (Zout && mode != 2) PSG_CUDA_TRY(cudaMemcpy(Zout, g.inst.Z, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
+  if (mode == 0) PSG_CUDA_TRY(cudaMemcpy(q, g.inst.D, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
+  if (mode == 2 && Zout) PSG_CUDA_TRY(cudaMemcpy(Zout, g.inst.D, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
+  return PSG_OK;
+}
+
+extern "C" long psg_upo2d_integrations(psg_upo2d* h) { return (h && h->u) ? h->u->integrations : -1; }
+extern "C" long psg_upo2d_launches(psg_upo2d* h) { return (h && h->u) ? h->u->launches : -1; }

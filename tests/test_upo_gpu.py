@@ -1,0 +1,82 @@
+"""The UPO solver's building blocks and a converging Newton-GMRES-hookstep run.
+
+* dz/dt against the oracle's restatement of TIMEDERIV (FP64; the reference
+  driver builds nu k^2 as 10**(log10 nu + 2 log10 |k|), identical to round-off);
+* Phi_T(z) of the FP64 integrator against the oracle step;
+* the exact tangent dPhi_T(z) q against central differences of the oracle step
+  (truncation O(eps^2) = 1e-10 with eps = 1e-5), and its linearity;
+* Newton-GMRES-hookstep from a perturbed laminar state at Re = 5 (stable laminar
+  flow) reaching |F|/|Phi_T(z)| <= 1e-10 with exact and finite-difference Jv.
+"""
+import numpy as np
+import pytest
+
+import psgpu_b200 as P
+from oracle import pyoracle as O
+from psgpu_b200.fields import Grid2D, kolmogorov_ic2d
+from tests.golden_cases import relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def _masked_random(n, seed, amp=1.0):
+    g = Grid2D(n)
+    rng = np.random.default_rng(seed)
+    q = (rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * g.mask()
+    return amp * q / np.sqrt(np.sum(np.abs(q) ** 2))
+
+
+def test_timederiv_matches_oracle():
+    n, nu = 32, 1 / 40
+    Z = kolmogorov_ic2d(n, 3)
+    u = P.UPO2D(1, n, kmax=4)
+    u.set_guess(0, Z, T=0.1, nu=nu, dt=0.005)
+    d, _ = u.apply(0, 2)
+    ref = O.ns2d_timederiv(Z, n, nu)
+    assert relerr(d, ref) < 1e-12
+
+
+def test_phi_matches_oracle():
+    n, nu, dt, T = 32, 1 / 40, 0.005, 0.2
+    Z = kolmogorov_ic2d(n, 4)
+    u = P.UPO2D(1, n, kmax=4)
+    u.set_guess(0, Z, T=T, nu=nu, dt=dt)
+    phi, _ = u.apply(0, 1)
+    ref, _ = O.ns2d_timestep(Z, n, nu, dt, int(round(T / dt)))
+    assert relerr(phi, ref) < 1e-12
+
+
+def test_tangent_matches_central_differences():
+    n, nu, dt, T = 32, 1 / 40, 0.005, 0.2
+    ns = int(round(T / dt))
+    Z = kolmogorov_ic2d(n, 5) * 3.0
+    q = _masked_random(n, 6)
+    u = P.UPO2D(1, n, kmax=4)
+    u.set_guess(0, Z, T=T, nu=nu, dt=dt)
+    _, jq = u.apply(0, 0, q)
+    eps = 1e-5
+    zp, _ = O.ns2d_timestep(Z + eps * q, n, nu, dt, ns)
+    zm, _ = O.ns2d_timestep(Z - eps * q, n, nu, dt, ns)
+    fd = (zp - zm) / (2 * eps)
+    assert relerr(jq, fd) < 1e-7
+    _, j2 = u.apply(0, 0, 2.0 * q)
+    assert relerr(j2, 2.0 * jq) < 1e-14
+
+
+@pytest.mark.parametrize("exact", [True, False], ids=["exact-jv", "fd-jv"])
+def test_newton_converges_to_laminar_state(exact):
+    n, nu, dt = 32, 1 / 5, 0.005
+    g = Grid2D(n)
+    K = g.kt
+    lam = np.zeros(g.shape, np.complex128)
+    lam[K + 4, 0] = -0.125 / nu
+    Z = lam + _masked_random(n, 7, amp=0.05)
+    u = P.UPO2D(2, n, kmax=30, exact_jv=exact)
+    u.set_guess(0, Z, T=1.0, nu=nu, dt=dt)
+    u.set_guess(1, lam + _masked_random(n, 8, amp=0.02), T=0.75, nu=nu, dt=dt)
+    u.solve(max_newton=20, tol=1e-10)
+    for i in range(2):
+        r = u.get(i)
+        assert r["status"] == "CONVERGED", r
+        assert r["residual"] <= 1e-10
+        assert relerr(r["Z"], lam) < 1e-8
