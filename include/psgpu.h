@@ -79,6 +79,9 @@ int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts);
  * this device); variant receives the choice, ms[4] the timing of each variant
  * (-1: does not fit) */
 int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
+/* the autotuner's current choice and timings, without re-running it
+ * (PSG_XPASS_VARIANT=0..3 in the environment pins the choice at set-up) */
+int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms);
 
 /* ---------------------------------------------------------------- 2D */
 /* A batch of independent 2D Kolmogorov-flow instances (sizes 16..256, any

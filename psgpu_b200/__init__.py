@@ -70,6 +70,7 @@ def lib():
     L.psg_ns3d_layout.argtypes = [vp, C.POINTER(ip), pp]
     L.psg_ns3d_profile.argtypes = [vp, i]
     L.psg_ns3d_autotune.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_float)]
+    L.psg_ns3d_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_float)]
     L.psg_ns3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_long)]
     _declare_2d(L)
     _lib = L
@@ -201,10 +202,12 @@ class NS3D:
         _check(lib().psg_ns3d_profile_read(self._h, ms, cnt))
         return {p: (ms[i], cnt[i]) for i, p in enumerate(self.PASSES)}
 
-    def autotune(self):
+    def autotune(self, rerun: bool = True):
+        """x-pass autotuner: (chosen variant, ms per launch of each variant)"""
         v = C.c_int()
         ms = (C.c_float * 4)()
-        _check(lib().psg_ns3d_autotune(self._h, C.byref(v), ms))
+        fn = lib().psg_ns3d_autotune if rerun else lib().psg_ns3d_tuning
+        _check(fn(self._h, C.byref(v), ms))
         return v.value, list(ms)
 
     def device_state(self):

@@ -119,3 +119,8 @@ extern "C" int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms) {
   if (rc) return rc;
   return h->e->tuning(variant, ms);
 }
+
+extern "C" int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->tuning(variant, ms);
+}

@@ -633,11 +633,27 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   const int xt = blockIdx.x, iky = blockIdx.y;
   if (tid == 0) mbar_init(&s_bar, 1);
   __syncthreads();
+  const long tile = ((long)xt * Y + iky) * Y * W;
   if (tid == 0) {
     const uint32_t bytes = (uint32_t)(N * W * sizeof(cpx<T>));
     mbar_expect_tx(&s_bar, NO * bytes);
     for (int f = 0; f < NO; ++f)
       bulk_g2s(s_in + f * N * W, in + (((long)f * XT + xt) * Y + iky) * N * W, bytes, &s_bar);
+    // the state tiles the update will read: fetch them into L2 while the
+    // transforms run
+    const uint32_t sb = (uint32_t)(Y * W * sizeof(cpx<T>));
+    const int nc = (NO > 3) ? 4 : 3;
+    for (int q = 0; q < nc; ++q) {
+      if (R.S.c[q]) bulk_prefetch_l2(R.S.c[q] + tile, sb);
+      const bool heun = (SCHEME == SCHEME_NS_HEUN || SCHEME == SCHEME_EULER_HEUN);
+      if (heun && stage == STAGE_HEUN_CORR && R.K1.c[q]) bulk_prefetch_l2(R.K1.c[q] + tile, sb);
+      if (SCHEME == SCHEME_BOUS_RK4 && R.X0.c[q]) bulk_prefetch_l2(R.X0.c[q] + tile, sb);
+      if (!heun && stage == STAGE_RK4) {
+        if (R.K1.c[q]) bulk_prefetch_l2(R.K1.c[q] + tile, sb);
+        if (R.K2.c[q]) bulk_prefetch_l2(R.K2.c[q] + tile, sb);
+        if (R.K3.c[q]) bulk_prefetch_l2(R.K3.c[q] + tile, sb);
+      }
+    }
   }
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
@@ -654,7 +670,6 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
     }
   }
   __syncthreads();
-  const long tile = ((long)xt * Y + iky) * Y * W;
   for (int idx = tid; idx < Y * W; idx += nth) {
     const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
     if (ikx >= g.X) continue;
@@ -990,6 +1005,15 @@ struct Engine3D final : Engine3DBase {
   // fastest.  The transforms' cost does not depend on the data.
   template <int N>
   int autotune_n() {
+    // PSG_XPASS_VARIANT=0..3 pins the choice (reproducible profiling runs)
+    if (const char* pin = getenv("PSG_XPASS_VARIANT")) {
+      const int v = atoi(pin);
+      if (v >= 0 && v < kCVariants && c_resident[v] > 0) {
+        c_variant = v;
+        for (int k = 0; k < kCVariants; ++k) c_ms[k] = -1.f;
+        return PSG_OK;
+      }
+    }
     cudaEvent_t a, b;
     PSG_CUDA_TRY(cudaEventCreate(&a));
     PSG_CUDA_TRY(cudaEventCreate(&b));
