@@ -1,10 +1,10 @@
 // psg_ns3d.cuh -- the 3D pseudospectral right-hand side as five fused passes.
 //
-// State layout in HBM (per component, complex T):
-//   S[ikz][iky][ikx], ikz,iky in [0, 2K], ikx in [0, XP) with XP = IKTX rounded
-//   up to the tile width (padding columns hold zeros).  This is the
-//   reference's truncated box (kx fastest, 3D_NavierStokes/src/init.F90:25-36)
-//   with padded rows so that every tile row is an aligned 64-byte segment.
+// State layout in HBM (per component, complex T): the reference's truncated
+// box (kx fastest, 3D_NavierStokes/src/init.F90:25-36) cut into tiles of W = 8
+// adjacent kx columns, S[xt][iky][ikz][W], ikz, iky in [0, 2K], xt in
+// [0, XP / W) with XP = IKTX rounded up to W (padding columns hold zeros), so
+// that the z-line tile of one (xt, iky) is one contiguous chunk.
 //
 // One evaluation of N(w) = curl(u x w) (plus buoyancy / density advection for
 // the Boussinesq system) is
