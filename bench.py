@@ -139,10 +139,11 @@ def algorithmic_bytes(n, word=8):
 def stage_bytes(n, stage, word=8):
     """state/register traffic of pass E for RK4 stage 0..3 (3 components each):
     stages 0-2 read S and write K_s and X0; the final stage reads S, K1, K2, K3
-    and writes S and X0."""
+    and the carried rounding error of the FP32 state, and writes S, X0 and that
+    error."""
     K = n // 3
     nkt = (K + 1) * (2 * K + 1) ** 2
-    arrays = 3 if stage < 3 else 6
+    arrays = 3 if stage < 3 else 8
     return arrays * 3 * nkt * word
 
 
@@ -368,6 +369,72 @@ def run_reference(args, rank, world, dist):
     }
 
 
+# ------------------------------------------------------------ accuracy study
+def run_accuracy(args):
+    """FP32 against FP64 on the bench workload: energy / enstrophy / dissipation
+    histories every step and the final vorticity after `args.accuracy` steps;
+    with the reference build present, both are also compared with the
+    reference's own FP64 step on the same initial state."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import taylor_green3d
+
+    torch.cuda.set_device(0)
+    nsteps = args.accuracy
+    xi, et, zt = taylor_green3d(N, 1234, amp=1e-3)
+    hist = {}
+    final = {}
+    for prec in (64, 32):
+        eng = P.NS3D(N, P.SCHEME_NS_RK4, precision=prec, nu=NU)
+        eng.upload(xi, et, zt)
+        h = np.zeros((nsteps + 1, 2))
+        h[0] = eng.energetics()[:2]
+        for s in range(nsteps):
+            eng.step(DT, 1)
+            h[s + 1] = eng.energetics()[:2]
+        hist[prec] = h
+        final[prec] = np.stack(eng.download())
+        eng.close()
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    def rel2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    h32, h64 = hist[32], hist[64]
+    out = {
+        "mode": "accuracy", "workload": "3D NS 256^3 Taylor-Green + 1e-3 perturbation, RK4/CN, "
+        "nu=1/1600, dt=1e-3", "steps": nsteps,
+        "energy_def": "sum over kept modes |w|^2/k^2 (reference computeStats)",
+        "enstrophy_def": "sum over kept modes |w|^2; dissipation = 2 nu * enstrophy",
+        "fp32_vs_fp64": {
+            "energy_max_rel": float(np.max(np.abs(h32[:, 0] - h64[:, 0]) / h64[:, 0])),
+            "enstrophy_max_rel": float(np.max(np.abs(h32[:, 1] - h64[:, 1]) / h64[:, 1])),
+            "dissipation_max_rel": float(np.max(np.abs(h32[:, 1] - h64[:, 1]) / h64[:, 1])),
+            "vorticity_maxnorm_rel": rel(final[32], final[64]),
+            "vorticity_l2_rel": rel2(final[32], final[64]),
+        },
+        "energy_start_end": [float(h64[0, 0]), float(h64[-1, 0])],
+        "enstrophy_start_end": [float(h64[0, 1]), float(h64[-1, 1])],
+    }
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_bous3d.so")
+    if os.path.exists(path) and not args.no_ref:
+        lib = TimestepLibrary(path, "bous3d")
+        comps = [a.copy() for a in (xi, et, zt, np.zeros_like(xi))]
+        t0 = time.perf_counter()
+        lib.bous3d_inplace(comps, N, NU, DT, nsteps * DT)
+        ref = np.stack(comps[:3])
+        out["reference_fp64_seconds"] = round(time.perf_counter() - t0, 2)
+        out["reference_steps"] = rk4_evaluations(0.0, nsteps * DT, DT)
+        out["fp64_vs_reference"] = {"vorticity_maxnorm_rel": rel(final[64], ref),
+                                    "vorticity_l2_rel": rel2(final[64], ref)}
+        out["fp32_vs_reference"] = {"vorticity_maxnorm_rel": rel(final[32], ref),
+                                    "vorticity_l2_rel": rel2(final[32], ref)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,6 +445,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI end-to-end leg")
     ap.add_argument("--grid", type=int, default=256,
                     help="grid size (256 is the benchmark; smaller grids are for profiling)")
+    ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
+                    help="run the FP32-vs-FP64 accuracy study over STEPS steps instead")
+    ap.add_argument("--no-ref", action="store_true",
+                    help="accuracy study without the reference FP64 run")
     args = ap.parse_args()
     global N
     N = args.grid
@@ -386,6 +457,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
+    if args.accuracy:
+        if rank == 0:
+            print(json.dumps(run_accuracy(args)), flush=True)
+        return
     if args.impl == "reference":
         # rank 0 alone times the reference; the other ranks exit without work
         if rank != 0:

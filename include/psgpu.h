@@ -82,6 +82,16 @@ int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
 /* the autotuner's current choice and timings, without re-running it
  * (PSG_XPASS_VARIANT=0..3 in the environment pins the choice at set-up) */
 int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms);
+/* the state from / to device arrays: FP64 complex boxes in the reference
+ * layout (IKTX*IKTY*IKTZ double2 per component), ordered on the engine's
+ * stream without a host synchronisation */
+int psg_ns3d_upload_device(psg_ns3d* h, void* const* comps);
+int psg_ns3d_download_device(psg_ns3d* h, void* const* comps);
+/* global sums over the kept modes, accumulated in FP64 on the device:
+ * out[0] = sum |w|^2 / max(k^2, 0.001) (the reference's energy,
+ * 3D_NavierStokes/src/functions.h:139-152), out[1] = sum |w|^2 (enstrophy),
+ * out[2] = sum |rho|^2 (Boussinesq; 0 otherwise) */
+int psg_ns3d_energetics(psg_ns3d* h, double* out);
 
 /* ---------------------------------------------------------------- 2D */
 /* A batch of independent 2D Kolmogorov-flow instances (sizes 16..256, any
@@ -103,7 +113,10 @@ int psg_batch2d_download(psg_batch2d* h, int i, double* Z);
 int psg_batch2d_run(psg_batch2d* h, const double* nu, const double* dt, const int* nsteps);
 int psg_batch2d_sync(psg_batch2d* h);
 long psg_batch2d_launches(psg_batch2d* h);
-/* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]) */
+/* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]).
+ * The FP32 batch keeps, right after the state, an array of the same shape with
+ * the rounding error its updates carry (state value = Z + Zlow); a caller that
+ * writes Z directly must zero that array too (or use psg_batch2d_upload). */
 int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z);
 
 /* ---------------------------------------------------------------- UPO search */

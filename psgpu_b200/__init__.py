@@ -72,6 +72,9 @@ def lib():
     L.psg_ns3d_autotune.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_float)]
     L.psg_ns3d_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_float)]
     L.psg_ns3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    L.psg_ns3d_upload_device.argtypes = [vp, C.POINTER(vp)]
+    L.psg_ns3d_download_device.argtypes = [vp, C.POINTER(vp)]
+    L.psg_ns3d_energetics.argtypes = [vp, C.POINTER(C.c_double)]
     _declare_2d(L)
     _lib = L
     return L
@@ -186,6 +189,27 @@ class NS3D:
 
     def sync(self):
         _check(lib().psg_ns3d_sync(self._h))
+
+    def energetics(self):
+        """(energy, enstrophy, density variance): FP64 sums over the kept modes of
+        |w|^2/k^2, |w|^2 and |rho|^2 (the reference's computeStats sums)."""
+        out = (C.c_double * 3)()
+        _check(lib().psg_ns3d_energetics(self._h, out))
+        return out[0], out[1], out[2]
+
+    def upload_device(self, ptrs):
+        """state from device FP64 complex boxes (reference layout), one pointer per
+        component; ordered on the engine's stream"""
+        if len(ptrs) != self.ncomp:
+            raise ValueError(f"expected {self.ncomp} components")
+        arr = (C.c_void_p * self.ncomp)(*[int(p) for p in ptrs])
+        _check(lib().psg_ns3d_upload_device(self._h, arr))
+
+    def download_device(self, ptrs):
+        if len(ptrs) != self.ncomp:
+            raise ValueError(f"expected {self.ncomp} components")
+        arr = (C.c_void_p * self.ncomp)(*[int(p) for p in ptrs])
+        _check(lib().psg_ns3d_download_device(self._h, arr))
 
     @property
     def launches(self) -> int:

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "psg_ns2d.cuh"
@@ -43,15 +44,25 @@ ns2d_persistent(const Inst2D<T>* __restrict__ insts, int ninst, int* __restrict_
   }
 }
 
+// FP64 reference boxes <-> state; `low` (FP32 engine) holds the part of each
+// value below the state's precision
 template <typename T>
-__global__ void ref_to_dev2(const double2* __restrict__ src, cpx<T>* __restrict__ dst, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dst[i] = cpx<T>{(T)src[i].x, (T)src[i].y};
+__global__ void ref_to_dev2(const double2* __restrict__ src, cpx<T>* __restrict__ dst, long n,
+                            cpx<T>* __restrict__ low) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const cpx<T> v = cpx<T>{(T)src[i].x, (T)src[i].y};
+    dst[i] = v;
+    if (low) low[i] = cpx<T>{(T)(src[i].x - (double)v.x), (T)(src[i].y - (double)v.y)};
+  }
 }
 template <typename T>
-__global__ void dev_to_ref2(const cpx<T>* __restrict__ src, double2* __restrict__ dst, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dst[i] = make_double2((double)src[i].x, (double)src[i].y);
+__global__ void dev_to_ref2(const cpx<T>* __restrict__ src, double2* __restrict__ dst, long n,
+                            const cpx<T>* __restrict__ low) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double2 v = make_double2((double)src[i].x, (double)src[i].y);
+    if (low) { v.x += (double)low[i].x; v.y += (double)low[i].y; }
+    dst[i] = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -103,7 +114,7 @@ struct Batch2D final : Batch2DBase {
         return PSG_ERR_UNSUPPORTED;
       }
       offs.push_back(total);
-      total += 5L * nkt2(n);
+      total += (std::is_same<T, float>::value ? 6L : 5L) * nkt2(n);
       maxk = std::max<long>(maxk, nkt2(n));
     }
     for (int i = 0; i < ninst; ++i) {
@@ -154,11 +165,17 @@ struct Batch2D final : Batch2DBase {
     return PSG_OK;
   }
 
+  // carried rounding error of instance i's state (FP32 engine), or null
+  cpx<T>* comp(int i) {
+    if (!std::is_same<T, float>::value) return nullptr;
+    return pool + offs[i] + 5L * nkt2(sizes[i]);
+  }
+
   int upload(int i, const double* Z) override {
     if (i < 0 || i >= ninst) { psg_set_error("instance %d out of range", i); return PSG_ERR_ARG; }
     const long nk = nkt2(sizes[i]);
     PSG_CUDA_TRY(cudaMemcpyAsync(staging, Z, sizeof(double2) * nk, cudaMemcpyHostToDevice, stream));
-    ref_to_dev2<T><<<148, 256, 0, stream>>>(staging, pool + offs[i], nk);
+    ref_to_dev2<T><<<148, 256, 0, stream>>>(staging, pool + offs[i], nk, comp(i));
     ++launches;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
@@ -167,7 +184,7 @@ struct Batch2D final : Batch2DBase {
   int download(int i, double* Z) override {
     if (i < 0 || i >= ninst) { psg_set_error("instance %d out of range", i); return PSG_ERR_ARG; }
     const long nk = nkt2(sizes[i]);
-    dev_to_ref2<T><<<148, 256, 0, stream>>>(pool + offs[i], staging, nk);
+    dev_to_ref2<T><<<148, 256, 0, stream>>>(pool + offs[i], staging, nk, comp(i));
     ++launches;
     PSG_CUDA_TRY(cudaMemcpyAsync(Z, staging, sizeof(double2) * nk, cudaMemcpyDeviceToHost, stream));
     PSG_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -184,6 +201,7 @@ struct Batch2D final : Batch2DBase {
       cpx<T>* b = pool + offs[i];
       I.Z = b; I.Z0 = b + nk; I.Z1 = b + 2 * nk; I.Z2 = b + 3 * nk; I.Z3 = b + 4 * nk;
       I.work = pool + woffs[i];
+      I.ZC = comp(i);
     }
     PSG_CUDA_TRY(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst2D<T>) * ninst,
                                  cudaMemcpyHostToDevice, stream));
@@ -380,6 +398,7 @@ int noalloc_run(unsigned char* base, int n, double nu, double dt, int nsteps, co
   I.Z = reinterpret_cast<cpx<T>*>(z_out);
   I.Z0 = work; I.Z1 = work + nk; I.Z2 = work + 2 * nk; I.Z3 = work + 3 * nk;
   I.work = work + 4 * nk;
+  I.ZC = nullptr;
   const cpx<T>* tw = reinterpret_cast<const cpx<T>*>(base + (sizeof(T) == 8 ? kTw64Off : kTw32Off));
   int off = 0;
   for (int m = 16; m < n; m *= 2) off += 2 * m;

@@ -32,6 +32,7 @@ struct Inst2D {
   cpx<T>* Z2;
   cpx<T>* Z3;
   cpx<T>* work;  // [3][n][K+1] row scratch
+  cpx<T>* ZC;    // carried rounding error of the state updates (FP32), or null
 };
 
 __device__ __forceinline__ int row_to_box2(int r, int K, int n) {
@@ -195,6 +196,7 @@ struct Rhs2D {
         if (!keep2(ikx, ky, K)) {
           // masked modes: Z = 0, Z0 untouched (kernels.h:285-295)
           I.Z[ik] = czero<T>();
+          if (I.ZC) I.ZC[ik] = czero<T>();
           continue;
         }
         const T kx = (T)ikx, kyT = (T)ky;
@@ -214,13 +216,28 @@ struct Rhs2D {
           I.Z3[ik] = d;
           I.Z0[ik] = cpx<T>{z.x + d.x, z.y + d.y};
         } else {
+          // ((1 - x/2) z + incr) / (1 + x/2), x = nu k^2 dt, evaluated as
+          // (z - eS z) + (incr - eI incr) so that only the small eS, eI are
+          // rounded (the factor repeats every step and its rounding would
+          // compound over a run)
           const T wk = kx * kx + kyT * kyT;
-          const T damp1 = (T)1 - (T)0.5 * dt * I.nu * wk;
-          const T damp2 = (T)1 / ((T)1 + (T)0.5 * dt * I.nu * wk);
+          const T x = dt * I.nu * wk, hx = (T)0.5 * x;
+          const T eS = x / ((T)1 + hx), eI = hx / ((T)1 + hx);
           const cpx<T> z1 = I.Z1[ik], z2 = I.Z2[ik], z3 = I.Z3[ik];
-          const cpx<T> zn = cpx<T>{
-              damp2 * (damp1 * z.x + (z1.x + (T)2 * z2.x + (T)2 * z3.x + d.x) / (T)6),
-              damp2 * (damp1 * z.y + (z1.y + (T)2 * z2.y + (T)2 * z3.y + d.y) / (T)6)};
+          const T ix = (z1.x + (T)2 * z2.x + (T)2 * z3.x + d.x) / (T)6;
+          const T iy = (z1.y + (T)2 * z2.y + (T)2 * z3.y + d.y) / (T)6;
+          const T yx = (ix - eI * ix) - eS * z.x, yy = (iy - eI * iy) - eS * z.y;
+          cpx<T> zn;
+          if (I.ZC) {  // carry the rounding error of z + y to the next step
+            const cpx<T> c = I.ZC[ik];
+            const T ax = yx + c.x, ay = yy + c.y;
+            zn.x = z.x + ax;
+            zn.y = z.y + ay;
+            const T bx = zn.x - z.x, by = zn.y - z.y;
+            I.ZC[ik] = cpx<T>{(z.x - (zn.x - bx)) + (ax - bx), (z.y - (zn.y - by)) + (ay - by)};
+          } else {
+            zn = cpx<T>{z.x + yx, z.y + yy};
+          }
           I.Z[ik] = zn;
           I.Z0[ik] = zn;
         }

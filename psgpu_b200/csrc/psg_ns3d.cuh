@@ -71,6 +71,9 @@ struct Engine3DBase {
   virtual int upload(const double* const* comps) = 0;
   virtual int download(double* const* comps) = 0;
   virtual int download_stage(double* const* comps) = 0;
+  virtual int upload_device(const void* const* comps) = 0;
+  virtual int download_device(void* const* comps) = 0;
+  virtual int energetics(double* out) = 0;
   virtual int steps(double dt, int nsteps, int dump_last) = 0;
   virtual int timederiv(double* const* out) = 0;
   virtual int phys(double* const* out) = 0;

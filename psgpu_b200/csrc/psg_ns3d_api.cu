@@ -124,3 +124,19 @@ extern "C" int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms) {
   PSG_CHECK_HANDLE(h);
   return h->e->tuning(variant, ms);
 }
+
+extern "C" int psg_ns3d_upload_device(psg_ns3d* h, void* const* comps) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->upload_device((const void* const*)comps);
+}
+
+extern "C" int psg_ns3d_download_device(psg_ns3d* h, void* const* comps) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->download_device(comps);
+}
+
+extern "C" int psg_ns3d_energetics(psg_ns3d* h, double* out) {
+  PSG_CHECK_HANDLE(h);
+  if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  return h->e->energetics(out);
+}

@@ -471,7 +471,44 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
 template <typename T>
 struct Regs {
   Fields4<T> S, X0, K1, K2, K3;
+  // FP32 engine: the rounding error of every state update, carried to the
+  // next one (state = S + SC), so that increments far below one ulp of the
+  // state still add up over a long run; null pointers in FP64
+  Fields4<T> SC;
 };
+
+// s + y as a rounded sum and its exact error (Knuth's TwoSum)
+template <typename T>
+__device__ __forceinline__ void two_sum(T a, T b, T& s, T& err) {
+  s = a + b;
+  const T bp = s - a;
+  err = (a - (s - bp)) + (b - bp);
+}
+
+// state value s (+ carried error c) plus the small increment y: returns the
+// new state and stores the new carried error; plain s + y without SC, and for
+// a mode the update does not keep (its carried error is cleared)
+template <typename T>
+__device__ __forceinline__ cpx<T> comp_add(const Fields4<T>& SC, int q, long ik, cpx<T> s, cpx<T> y,
+                                           bool keep = true) {
+  if (!SC.c[q]) return cpx<T>{s.x + y.x, s.y + y.y};
+  if (!keep) {
+    SC.c[q][ik] = czero<T>();
+    return cpx<T>{s.x + y.x, s.y + y.y};
+  }
+  const cpx<T> c = SC.c[q][ik];
+  cpx<T> r, e;
+  two_sum(s.x, y.x + c.x, r.x, e.x);
+  two_sum(s.y, y.y + c.y, r.y, e.y);
+  SC.c[q][ik] = e;
+  return r;
+}
+
+// v (1 - e) evaluated as v - e v
+template <typename T>
+__device__ __forceinline__ cpx<T> damp(cpx<T> v, T e) {
+  return cpx<T>{v.x - e * v.x, v.y - e * v.y};
+}
 
 template <typename T, int SCHEME>
 __device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R,
@@ -495,30 +532,48 @@ __device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R
       const T nu1 = LL * (p.dt / ((T)1 + (T)0.5 * NU * p.dt));
       if (stage == STAGE_HEUN_PRED) {
         H0[ik] = cpx<T>{xiX, xiY}; H1[ik] = cpx<T>{etX, etY}; H2[ik] = cpx<T>{ztX, ztY};
+        // nu1 (nuzn s + N) = (s - e s) + nu1 N with nu1 nuzn = 1 - e,
+        // e = NU dt / (1 + NU dt / 2): only the small e is rounded
+        (void)nuzn;
+        const T x = NU * p.dt;
+        const T e = x / ((T)1 + (T)0.5 * x);
         const T NU1 = LL * nu1;
-        S0[ik] = cpx<T>{NU1 * (nuzn * s0.x + xiX), NU1 * (nuzn * s0.y + xiY)};
-        S1[ik] = cpx<T>{NU1 * (nuzn * s1.x + etX), NU1 * (nuzn * s1.y + etY)};
-        S2[ik] = cpx<T>{NU1 * (nuzn * s2.x + ztX), NU1 * (nuzn * s2.y + ztY)};
+        const T eL = LL * e;
+        const bool kp = LL != (T)0;
+        S0[ik] = comp_add(R.SC, 0, ik, cpx<T>{LL * s0.x, LL * s0.y},
+                          cpx<T>{NU1 * xiX - eL * s0.x, NU1 * xiY - eL * s0.y}, kp);
+        S1[ik] = comp_add(R.SC, 1, ik, cpx<T>{LL * s1.x, LL * s1.y},
+                          cpx<T>{NU1 * etX - eL * s1.x, NU1 * etY - eL * s1.y}, kp);
+        S2[ik] = comp_add(R.SC, 2, ik, cpx<T>{LL * s2.x, LL * s2.y},
+                          cpx<T>{NU1 * ztX - eL * s2.x, NU1 * ztY - eL * s2.y}, kp);
       } else {
-        const T NU2 = (T)0.5 * nu1;
+        const T NU2 = LL * (T)0.5 * nu1;
         const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
-        S0[ik] = cpx<T>{LL * (s0.x + NU2 * (xiX - h0.x)), LL * (s0.y + NU2 * (xiY - h0.y))};
-        S1[ik] = cpx<T>{LL * (s1.x + NU2 * (etX - h1.x)), LL * (s1.y + NU2 * (etY - h1.y))};
-        S2[ik] = cpx<T>{LL * (s2.x + NU2 * (ztX - h2.x)), LL * (s2.y + NU2 * (ztY - h2.y))};
+        const bool kp = LL != (T)0;
+        S0[ik] = comp_add(R.SC, 0, ik, cpx<T>{LL * s0.x, LL * s0.y},
+                          cpx<T>{NU2 * (xiX - h0.x), NU2 * (xiY - h0.y)}, kp);
+        S1[ik] = comp_add(R.SC, 1, ik, cpx<T>{LL * s1.x, LL * s1.y},
+                          cpx<T>{NU2 * (etX - h1.x), NU2 * (etY - h1.y)}, kp);
+        S2[ik] = comp_add(R.SC, 2, ik, cpx<T>{LL * s2.x, LL * s2.y},
+                          cpx<T>{NU2 * (ztX - h2.x), NU2 * (ztY - h2.y)}, kp);
       }
     } else {  // Euler (3D_Euler/src/kernels.h:324-341, 396-406)
       if (stage == STAGE_HEUN_PRED) {
         H0[ik] = cpx<T>{LL * xiX, LL * xiY}; H1[ik] = cpx<T>{LL * etX, LL * etY};
         H2[ik] = cpx<T>{LL * ztX, LL * ztY};
-        S0[ik] = cpx<T>{s0.x + p.dt * xiX, s0.y + p.dt * xiY};
-        S1[ik] = cpx<T>{s1.x + p.dt * etX, s1.y + p.dt * etY};
-        S2[ik] = cpx<T>{s2.x + p.dt * ztX, s2.y + p.dt * ztY};
+        S0[ik] = comp_add(R.SC, 0, ik, s0, cpx<T>{p.dt * xiX, p.dt * xiY});
+        S1[ik] = comp_add(R.SC, 1, ik, s1, cpx<T>{p.dt * etX, p.dt * etY});
+        S2[ik] = comp_add(R.SC, 2, ik, s2, cpx<T>{p.dt * ztX, p.dt * ztY});
       } else {
-        const T hd = (T)0.5 * p.dt;
+        const T hd = LL * (T)0.5 * p.dt;
         const cpx<T> h0 = H0[ik], h1 = H1[ik], h2 = H2[ik];
-        S0[ik] = cpx<T>{LL * (s0.x + hd * (xiX - h0.x)), LL * (s0.y + hd * (xiY - h0.y))};
-        S1[ik] = cpx<T>{LL * (s1.x + hd * (etX - h1.x)), LL * (s1.y + hd * (etY - h1.y))};
-        S2[ik] = cpx<T>{LL * (s2.x + hd * (ztX - h2.x)), LL * (s2.y + hd * (ztY - h2.y))};
+        const bool kp = LL != (T)0;
+        S0[ik] = comp_add(R.SC, 0, ik, cpx<T>{LL * s0.x, LL * s0.y},
+                          cpx<T>{hd * (xiX - h0.x), hd * (xiY - h0.y)}, kp);
+        S1[ik] = comp_add(R.SC, 1, ik, cpx<T>{LL * s1.x, LL * s1.y},
+                          cpx<T>{hd * (etX - h1.x), hd * (etY - h1.y)}, kp);
+        S2[ik] = comp_add(R.SC, 2, ik, cpx<T>{LL * s2.x, LL * s2.y},
+                          cpx<T>{hd * (ztX - h2.x), hd * (ztY - h2.y)}, kp);
       }
     }
   } else {
@@ -562,41 +617,58 @@ __device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R
         R.K1.c[3][ik] = cpx<T>{d2 * s3.x + rXR, d2 * s3.y + rXC};
       }
     } else if (!final_stage) {
+      // X0 = d (S + fr dt N) with d = (1 - q nk)/(1 + q nk), applied as
+      // v - e v, e = 2 q nk / (1 + q nk): the factor is the same every step,
+      // so its rounding would compound coherently over a run; written this
+      // way only e (small) is rounded
       const T q = (stage == STAGE_RK3) ? (T)0.5 : (T)0.25;
       const T fr = (stage == STAGE_RK3) ? (T)1 : (T)0.5;
-      const T d1 = ((T)1 - q * nk) / ((T)1 + q * nk);
+      const T e1 = (T)2 * q * nk / ((T)1 + q * nk);
       const Fields4<T>& KR = (stage == STAGE_RK1) ? R.K1 : (stage == STAGE_RK2) ? R.K2 : R.K3;
       KR.c[0][ik] = cpx<T>{dt * xiX, dt * xiY};
       KR.c[1][ik] = cpx<T>{dt * etX, dt * etY};
       KR.c[2][ik] = cpx<T>{dt * ztX, dt * ztY};
       const cpx<T> s0 = R.S.c[0][ik], s1 = R.S.c[1][ik], s2 = R.S.c[2][ik];
-      R.X0.c[0][ik] = cpx<T>{d1 * (s0.x + fr * dt * xiX), d1 * (s0.y + fr * dt * xiY)};
-      R.X0.c[1][ik] = cpx<T>{d1 * (s1.x + fr * dt * etX), d1 * (s1.y + fr * dt * etY)};
-      R.X0.c[2][ik] = cpx<T>{d1 * (s2.x + fr * dt * ztX), d1 * (s2.y + fr * dt * ztY)};
+      R.X0.c[0][ik] = damp(cpx<T>{s0.x + fr * dt * xiX, s0.y + fr * dt * xiY}, e1);
+      R.X0.c[1][ik] = damp(cpx<T>{s1.x + fr * dt * etX, s1.y + fr * dt * etY}, e1);
+      R.X0.c[2][ik] = damp(cpx<T>{s2.x + fr * dt * ztX, s2.y + fr * dt * ztY}, e1);
       if (BOUS) {
-        const T d2 = ((T)1 - q * nks) / ((T)1 + q * nks);
+        const T e2 = (T)2 * q * nks / ((T)1 + q * nks);
         KR.c[3][ik] = cpx<T>{dt * rXR, dt * rXC};
         const cpx<T> s3 = R.S.c[3][ik];
-        R.X0.c[3][ik] = cpx<T>{d2 * (s3.x + fr * dt * rXR), d2 * (s3.y + fr * dt * rXC)};
+        R.X0.c[3][ik] = damp(cpx<T>{s3.x + fr * dt * rXR, s3.y + fr * dt * rXC}, e2);
       }
     } else {
+      // S' = ((1 - nk/2) S + incr) / (1 + nk/2) = (S - eS S) + (incr - eI incr)
+      // with eS = nk / (1 + nk/2), eI = (nk/2) / (1 + nk/2)
       const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
-      const T d1 = (T)1 - (T)0.5 * nk;
-      const T den = (T)1 + (T)0.5 * nk;
+      const T hn = (T)0.5 * nk;
+      const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
       T o[4][2];
       const T nr[3][2] = {{xiX, xiY}, {etX, etY}, {ztX, ztY}};
+      const bool kp = LL != (T)0;
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const cpx<T> s = R.S.c[q][ik], a = R.K1.c[q][ik], b = R.K2.c[q][ik], cc3 = R.K3.c[q][ik];
-        o[q][0] = LL * (d1 * s.x + sixth * (a.x + dt * nr[q][0]) + third * (b.x + cc3.x)) / den;
-        o[q][1] = LL * (d1 * s.y + sixth * (a.y + dt * nr[q][1]) + third * (b.y + cc3.y)) / den;
+        const T ix = sixth * (a.x + dt * nr[q][0]) + third * (b.x + cc3.x);
+        const T iy = sixth * (a.y + dt * nr[q][1]) + third * (b.y + cc3.y);
+        const cpx<T> r = comp_add(R.SC, q, ik, cpx<T>{LL * s.x, LL * s.y},
+                                  cpx<T>{LL * ((ix - eI * ix) - eS * s.x),
+                                         LL * ((iy - eI * iy) - eS * s.y)}, kp);
+        o[q][0] = r.x;
+        o[q][1] = r.y;
       }
       if (BOUS) {
-        const T d2 = (T)1 - (T)0.5 * nks;
-        const T den2 = (T)1 + (T)0.5 * nks;
+        const T hs = (T)0.5 * nks;
+        const T eS2 = nks / ((T)1 + hs), eI2 = hs / ((T)1 + hs);
         const cpx<T> s = R.S.c[3][ik], a = R.K1.c[3][ik], b = R.K2.c[3][ik], cc3 = R.K3.c[3][ik];
-        o[3][0] = LL * (d2 * s.x + sixth * (a.x + dt * rXR) + third * (b.x + cc3.x)) / den2;
-        o[3][1] = LL * (d2 * s.y + sixth * (a.y + dt * rXC) + third * (b.y + cc3.y)) / den2;
+        const T ix = sixth * (a.x + dt * rXR) + third * (b.x + cc3.x);
+        const T iy = sixth * (a.y + dt * rXC) + third * (b.y + cc3.y);
+        const cpx<T> r = comp_add(R.SC, 3, ik, cpx<T>{LL * s.x, LL * s.y},
+                                  cpx<T>{LL * ((ix - eI2 * ix) - eS2 * s.x),
+                                         LL * ((iy - eI2 * iy) - eS2 * s.y)}, kp);
+        o[3][0] = r.x;
+        o[3][1] = r.y;
         R.X0.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
         R.S.c[3][ik] = cpx<T>{o[3][0], o[3][1]};
       }
@@ -648,6 +720,7 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
       const bool heun = (SCHEME == SCHEME_NS_HEUN || SCHEME == SCHEME_EULER_HEUN);
       if (heun && stage == STAGE_HEUN_CORR && R.K1.c[q]) bulk_prefetch_l2(R.K1.c[q] + tile, sb);
       if (SCHEME == SCHEME_BOUS_RK4 && R.X0.c[q]) bulk_prefetch_l2(R.X0.c[q] + tile, sb);
+      if (R.SC.c[q] && (heun || stage == STAGE_RK4)) bulk_prefetch_l2(R.SC.c[q] + tile, sb);
       if (!heun && stage == STAGE_RK4) {
         if (R.K1.c[q]) bulk_prefetch_l2(R.K1.c[q] + tile, sb);
         if (R.K2.c[q]) bulk_prefetch_l2(R.K2.c[q] + tile, sb);
@@ -688,10 +761,66 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
 }
 
 // ---------------------------------------------------------------------------
+// global energetics in FP64: sum over kept modes of |w|^2 / max(k^2, 0.001)
+// (energy) and |w|^2 (enstrophy), as computeStats forms them
+// (3D_NavierStokes/src/functions.h:139-152), plus |rho|^2 for a fourth
+// component.  One partial per block, summed by energetics_final in a fixed
+// order so that the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) energetics_partial(Geom3<T> g, Fields4<T> S, int nc,
+                                                          double* __restrict__ part) {
+  const int W = kTileW;
+  const long total = (long)g.XP * g.Y * g.Y;
+  double e = 0.0, z = 0.0, r = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % W);
+    long q = i / W;
+    const int ikz = (int)(q % g.Y); q /= g.Y;
+    const int iky = (int)(q % g.Y);
+    const int ikx = (int)(q / g.Y) * W + w;
+    if (ikx >= g.X || !keep_mode<T>(ikx, iky - g.K, ikz - g.K, g.K, g.alpha)) continue;
+    const double kx = (double)ikx * (double)g.alpha, ky = iky - g.K, kz = ikz - g.K;
+    double wk = kx * kx + ky * ky + kz * kz;
+    wk = wk > 0.001 ? wk : 0.001;
+    double v = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> a = S.c[c][i];
+      v += (double)a.x * (double)a.x + (double)a.y * (double)a.y;
+    }
+    z += v;
+    e += v / wk;
+    if (nc > 3) {
+      const cpx<T> a = S.c[3][i];
+      r += (double)a.x * (double)a.x + (double)a.y * (double)a.y;
+    }
+  }
+  __shared__ double s[3][256];
+  s[0][threadIdx.x] = e; s[1][threadIdx.x] = z; s[2][threadIdx.x] = r;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) part[blockIdx.x * 3 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+static __global__ void energetics_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  if (threadIdx.x < 3) {
+    double a = 0.0;
+    for (int b = 0; b < nblk; ++b) a += part[b * 3 + threadIdx.x];
+    out[threadIdx.x] = a;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // layout conversion between the reference's FP64 boxes and the tile layout
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>* __restrict__ dst) {
+__global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>* __restrict__ dst,
+                             cpx<T>* __restrict__ low = nullptr) {
   const int W = kTileW;
   const long total = (long)g.XP * g.Y * g.Y;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
@@ -702,17 +831,20 @@ __global__ void box_from_ref(Geom3<T> g, const double2* __restrict__ src, cpx<T>
     const int iky = (int)(r % g.Y);
     const int xt = (int)(r / g.Y);
     const int ikx = xt * W + w;
-    cpx<T> v = czero<T>();
+    cpx<T> v = czero<T>(), lo = czero<T>();
     if (ikx < g.X) {
       const double2 s = src[((long)ikz * g.Y + iky) * g.X + ikx];
       v = cpx<T>{(T)s.x, (T)s.y};
+      lo = cpx<T>{(T)(s.x - (double)v.x), (T)(s.y - (double)v.y)};
     }
     dst[i] = v;
+    if (low) low[i] = lo;
   }
 }
 
 template <typename T>
-__global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* __restrict__ dst) {
+__global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* __restrict__ dst,
+                           const cpx<T>* __restrict__ low = nullptr) {
   const int W = kTileW;
   const long total = (long)g.Y * g.Y * g.X;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
@@ -720,8 +852,15 @@ __global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* 
     const int ikx = (int)(i % g.X);
     const long r = i / g.X;
     const int iky = (int)(r % g.Y), ikz = (int)(r / g.Y);
-    const cpx<T> s = src[(((long)(ikx / W) * g.Y + iky) * g.Y + ikz) * W + (ikx % W)];
-    dst[i] = make_double2((double)s.x, (double)s.y);
+    const long j = (((long)(ikx / W) * g.Y + iky) * g.Y + ikz) * W + (ikx % W);
+    const cpx<T> s = src[j];
+    double2 v = make_double2((double)s.x, (double)s.y);
+    if (low) {
+      const cpx<T> c = low[j];
+      v.x += (double)c.x;
+      v.y += (double)c.y;
+    }
+    dst[i] = v;
   }
 }
 
@@ -761,6 +900,7 @@ struct Engine3D final : Engine3DBase {
   cpx<T>* B2 = nullptr;
   double2* stage_h = nullptr;  // device FP64 staging box
   int* d_status = nullptr;     // device error flag of the bounded waits
+  double* d_energ = nullptr;   // energetics partial sums
   int c_variant = 0;           // x-pass variant chosen by the autotuner
   int c_resident[4] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
   float c_ms[4] = {0, 0, 0, 0};      // autotuner timings (ms per launch)
@@ -877,15 +1017,20 @@ struct Engine3D final : Engine3DBase {
     const long b3 = (long)nfo * n * n * g.XP;
     const long b2 = (long)nfi * n * n * g.XP;
     const long nb1 = b1 > b3 ? b1 : b3;
-    const long total = (long)nregs * nc * box + nb1 + b2 + 2 * n;
+    // the FP32 engine carries the rounding error of its state updates
+    const int ncomp_regs = std::is_same<T, float>::value ? 1 : 0;
+    const long total = (long)(nregs + ncomp_regs) * nc * box + nb1 + b2 + 2 * n;
     PSG_CUDA_TRY(cudaMalloc(&pool, sizeof(cpx<T>) * total));
     PSG_CUDA_TRY(cudaMemset(pool, 0, sizeof(cpx<T>) * total));
     cpx<T>* p = pool;
     Fields4<T>* regs[5] = {&R.S, &R.K1, &R.X0, &R.K2, &R.K3};
     for (int r = 0; r < 5; ++r)
       for (int q = 0; q < 4; ++q) regs[r]->c[q] = nullptr;
+    for (int q = 0; q < 4; ++q) R.SC.c[q] = nullptr;
     for (int r = 0; r < nregs; ++r)
       for (int q = 0; q < nc; ++q) { regs[r]->c[q] = p; p += box; }
+    if (ncomp_regs)
+      for (int q = 0; q < nc; ++q) { R.SC.c[q] = p; p += box; }
     B1 = p; p += nb1;
     B2 = p; p += b2;
     tw = p; p += 2 * n;
@@ -918,6 +1063,8 @@ struct Engine3D final : Engine3DBase {
     if (stage_h) cudaFree(stage_h);
     if (dump) cudaFree(dump);
     if (d_status) cudaFree(d_status);
+    if (d_energ) cudaFree(d_energ);
+    d_energ = nullptr;
     pool = nullptr; stage_h = nullptr; dump = nullptr; d_status = nullptr;
   }
 
@@ -1163,7 +1310,7 @@ struct Engine3D final : Engine3DBase {
     for (int q = 0; q < nc; ++q) {
       PSG_CUDA_TRY(cudaMemcpyAsync(stage_h, comps[q], sizeof(double2) * nref,
                                    cudaMemcpyHostToDevice, stream));
-      box_from_ref<T><<<592, 256, 0, stream>>>(g, stage_h, R.S.c[q]);
+      box_from_ref<T><<<592, 256, 0, stream>>>(g, stage_h, R.S.c[q], R.SC.c[q]);
       ++launches;
     }
     if (R.X0.c[0]) {
@@ -1176,6 +1323,43 @@ struct Engine3D final : Engine3DBase {
   }
 
   int download(double* const* comps) override { return download_from(comps, nullptr); }
+
+  // device FP64 boxes (reference layout) <-> state, ordered on the engine's
+  // stream, no host synchronisation
+  int upload_device(const void* const* comps) override {
+    for (int q = 0; q < nc; ++q) {
+      box_from_ref<T><<<592, 256, 0, stream>>>(g, (const double2*)comps[q], R.S.c[q], R.SC.c[q]);
+      ++launches;
+    }
+    if (R.X0.c[0]) {
+      copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
+      ++launches;
+    }
+    first_rhs = 1;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+  int download_device(void* const* comps) override {
+    for (int q = 0; q < nc; ++q) {
+      box_to_ref<T><<<592, 256, 0, stream>>>(g, R.S.c[q], (double2*)comps[q], R.SC.c[q]);
+      ++launches;
+    }
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  int energetics(double* out) override {
+    constexpr int kBlk = 296;
+    if (!d_energ) PSG_CUDA_TRY(cudaMalloc(&d_energ, sizeof(double) * (3 * kBlk + 3)));
+    energetics_partial<T><<<kBlk, 256, 0, stream>>>(g, R.S, nc, d_energ);
+    energetics_final<<<1, 32, 0, stream>>>(d_energ, kBlk, d_energ + 3 * kBlk);
+    launches += 2;
+    PSG_CUDA_TRY(cudaGetLastError());
+    PSG_CUDA_TRY(cudaMemcpyAsync(out, d_energ + 3 * kBlk, sizeof(double) * 3,
+                                 cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return check_status();
+  }
   int download_stage(double* const* comps) override {
     if (!R.X0.c[0]) { psg_set_error("scheme keeps no stage state"); return PSG_ERR_STATE; }
     return download_from(comps, &R.X0);
@@ -1219,7 +1403,7 @@ struct Engine3D final : Engine3DBase {
     const long nref = (long)g.Y * g.Y * g.X;
     const Fields4<T>& F = src ? *src : R.S;
     for (int q = 0; q < nc; ++q) {
-      box_to_ref<T><<<592, 256, 0, stream>>>(g, F.c[q], stage_h);
+      box_to_ref<T><<<592, 256, 0, stream>>>(g, F.c[q], stage_h, src ? nullptr : R.SC.c[q]);
       ++launches;
       PSG_CUDA_TRY(cudaMemcpyAsync(comps[q], stage_h, sizeof(double2) * nref,
                                    cudaMemcpyDeviceToHost, stream));
