@@ -223,6 +223,8 @@ def run_ours(args, rank, world, dist):
     e2e = None if args.no_e2e else run_e2e(args, dev, dist, world, rank)
     eng.close()
 
+    upo = run_upo(args) if (world == 1 and not args.no_upo) else None
+
     out = None
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu else None
@@ -239,7 +241,7 @@ def run_ours(args, rank, world, dist):
                                    "nu=1/1600, dt=1e-3, 2/3 dealias",
                        "grid": N, "replicas": world, "parallelism": f"replicas{world}",
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
-            "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu, "upo": upo,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
                                 "variants": ["L=128/G,1 stage", "L=256/G,1 stage",
@@ -247,6 +249,82 @@ def run_ours(args, rank, world, dist):
         }
         if out_note:
             out["note"] = out_note
+    return out
+
+
+# ------------------------------------------------------ UPO Newton iterations
+UPO_N, UPO_NU, UPO_DT, UPO_GUESSES, UPO_KMAX = 128, 1.0 / 40.0, 0.005, 64, 60
+
+
+def run_upo(args):
+    """Batched Newton-GMRES-hookstep on 2D Kolmogorov flow, Re = 40, 128^2:
+    64 guesses from seeded turbulent states after a 500 time-unit spin-up
+    (one persistent launch), periods uniform in [5, 20], Krylov dimension 60,
+    FP64 integrations and Arnoldi, target residual 1e-10.  Newton iterations
+    per second with the exact tangent Jv and with the forward-difference Jv,
+    and the reference's plain form (one guess at a time, one timestep_cuda_
+    call per Krylov vector) from its measured time per integration."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import kolmogorov_ic2d
+
+    n, nu, dt, G = UPO_N, UPO_NU, UPO_DT, UPO_GUESSES
+    spin = P.Batch2D([n] * G, precision=32)
+    for i in range(G):
+        spin.upload(i, kolmogorov_ic2d(n, 5000 + i))
+    t0 = time.perf_counter()
+    spin.run([nu] * G, [dt] * G, [int(round(500.0 / dt))] * G)
+    spin.sync()
+    spin_s = time.perf_counter() - t0
+    guesses = [spin.download(i) for i in range(G)]
+    spin.close()
+    periods = np.random.default_rng(77).uniform(5.0, 20.0, G)
+    out = {"workload": "2D Kolmogorov Re=40 128^2, 64 guesses from turbulent states after a "
+                       "500 time-unit spin-up, periods U[5,20], Krylov 60, FP64, tol 1e-10",
+           "spinup_seconds": round(spin_s, 2), "newton_per_guess": args.upo_newton}
+    per_guess_integrations = None
+    for name, exact in (("exact_jv", True), ("fd_jv", False)):
+        u = P.UPO2D(G, n, kmax=UPO_KMAX, exact_jv=exact)
+        for i in range(G):
+            u.set_guess(i, guesses[i], T=float(periods[i]), nu=nu, dt=dt)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u.solve(max_newton=args.upo_newton, tol=1e-10, gmres_tol=1e-3)
+        sec = time.perf_counter() - t0
+        info = [u.get(i) for i in range(G)]
+        newton = sum(x["newton"] for x in info)
+        res = np.array([x["residual"] for x in info])
+        out[name] = {"newton_iters_per_s": round(newton / sec, 4), "newton_iters": newton,
+                     "gmres_iters": sum(x["gmres"] for x in info),
+                     "integrations": u.integrations, "seconds": round(sec, 2),
+                     "converged": sum(x["status"] == "CONVERGED" for x in info),
+                     "median_rel_residual": float(np.median(res))}
+        if exact:
+            per_guess_integrations = [x["gmres"] + x["hookstep"] + x["newton"] for x in info]
+        u.close()
+    # plain form: the reference's own 2D step, one integration per call
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
+    if os.path.exists(path):
+        lib = TimestepLibrary(path, "ns2d")
+        Z = guesses[0].copy()
+        lib.ns2d(Z, n, nu, dt, 10)
+        nst = int(round(12.5 / dt))
+        t0 = time.perf_counter()
+        lib.ns2d(Z, n, nu, dt, nst)
+        call_s = time.perf_counter() - t0
+        step_s = call_s / nst
+        plain_s = sum(k * (periods[i] / dt) * step_s for i, k in enumerate(per_guess_integrations))
+        newton = out["exact_jv"]["newton_iters"]
+        out["plain_reference"] = {
+            "newton_iters_per_s": round(newton / plain_s, 5),
+            "seconds_model": round(plain_s, 1),
+            "how": "the same Newton iterations as the exact-Jv run, each integration a "
+                   "reference timestep_cuda_ call (FP64 cuFFT, one guess at a time) costed at "
+                   f"its measured {1e3 * step_s:.4f} ms/step (one call of {nst} steps incl. "
+                   "its set-up); host Arnoldi/SVD time not included"}
+        out["exact_vs_plain"] = round(out["exact_jv"]["newton_iters_per_s"] /
+                                      out["plain_reference"]["newton_iters_per_s"], 2)
     return out
 
 
@@ -445,6 +523,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI end-to-end leg")
     ap.add_argument("--grid", type=int, default=256,
                     help="grid size (256 is the benchmark; smaller grids are for profiling)")
+    ap.add_argument("--no-upo", action="store_true", help="skip the UPO Newton leg")
+    ap.add_argument("--upo-newton", type=int, default=1,
+                    help="Newton iterations per guess in the UPO leg")
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
                     help="run the FP32-vs-FP64 accuracy study over STEPS steps instead")
     ap.add_argument("--no-ref", action="store_true",

@@ -75,6 +75,7 @@ def lib():
     L.psg_ns3d_upload_device.argtypes = [vp, C.POINTER(vp)]
     L.psg_ns3d_download_device.argtypes = [vp, C.POINTER(vp)]
     L.psg_ns3d_energetics.argtypes = [vp, C.POINTER(C.c_double)]
+    L.psg_ns3d_linear.argtypes = [vp, i, d, C.POINTER(vp), C.POINTER(vp)]
     _declare_2d(L)
     _lib = L
     return L
@@ -204,6 +205,24 @@ class NS3D:
             raise ValueError(f"expected {self.ncomp} components")
         arr = (C.c_void_p * self.ncomp)(*[int(p) for p in ptrs])
         _check(lib().psg_ns3d_upload_device(self._h, arr))
+
+    LIN_TANGENT_STEP, LIN_ADJOINT_STEP, LIN_TANGENT_RHS, LIN_ADJOINT_RHS = 0, 1, 2, 3
+
+    def linear(self, mode: int, x, dt: float = 0.0, out=None):
+        """Tangent / adjoint step or right-hand side (see psg_ns3d_linear) applied to
+        x, a torch CUDA complex128 tensor of shape (3, IKTZ, IKTY, IKTX) in the
+        reference layout; returns `out` (a new tensor unless given).  Ordered on
+        the engine's stream (set_stream) -- the caller synchronises."""
+        import torch
+        if x.dtype != torch.complex128 or not x.is_cuda or x.shape[0] != 3:
+            raise ValueError("x must be a CUDA complex128 tensor of 3 components")
+        x = x.contiguous()
+        if out is None:
+            out = torch.empty_like(x)
+        ip = (C.c_void_p * 3)(*[x[q].data_ptr() for q in range(3)])
+        op = (C.c_void_p * 3)(*[out[q].data_ptr() for q in range(3)])
+        _check(lib().psg_ns3d_linear(self._h, mode, dt, ip, op))
+        return out
 
     def download_device(self, ptrs):
         if len(ptrs) != self.ncomp:

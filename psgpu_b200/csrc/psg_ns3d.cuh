@@ -28,6 +28,7 @@ enum Scheme3D : int {
   SCHEME_EULER_HEUN = 1,  // 3D_Euler/src/kernels.h:296-439
   SCHEME_NS_RK4 = 2,      // 3D_Boussinesq/src/kernels.h:331-621 without density
   SCHEME_BOUS_RK4 = 3,    // 3D_Boussinesq/src/kernels.h:331-621
+  SCHEME_RAW = 4,         // pass E writes the masked transform itself (bilinear products)
 };
 
 // stage codes of pass E
@@ -74,6 +75,7 @@ struct Engine3DBase {
   virtual int upload_device(const void* const* comps) = 0;
   virtual int download_device(void* const* comps) = 0;
   virtual int energetics(double* out) = 0;
+  virtual int linear(int mode, double dt, const void* const* in, void* const* out) = 0;
   virtual int steps(double dt, int nsteps, int dump_last) = 0;
   virtual int timederiv(double* const* out) = 0;
   virtual int phys(double* const* out) = 0;

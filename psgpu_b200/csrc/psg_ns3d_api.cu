@@ -140,3 +140,9 @@ extern "C" int psg_ns3d_energetics(psg_ns3d* h, double* out) {
   if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
   return h->e->energetics(out);
 }
+
+extern "C" int psg_ns3d_linear(psg_ns3d* h, int mode, double dt, void* const* in, void* const* out) {
+  PSG_CHECK_HANDLE(h);
+  if (!in || !out) { psg_set_error("null vector"); return PSG_ERR_ARG; }
+  return h->e->linear(mode, dt, (const void* const*)in, out);
+}

@@ -93,11 +93,29 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* s_ok, int* status)
 // pass A: z-inverse of the stage state with the velocity (and density
 // gradient) formed in registers; Hermitian completion of the kx = 0 plane.
 // grid (XT, Y): one [kz][W] tile of each state component.
+//
+// MODE 1 (pair): the two 3-vectors of a bilinear product, b = in (written to
+// the w slots 0-2 that pass C reads as w) and a = in2 (the u slots 3-5), each
+// passed through the spectral operator of `ops` (bits 0-3 for b, 4-7 for a:
+// OP_ID, OP_CURL = i k x, OP_BS = i k x / k^2) and masked to the kept modes.
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NC, int NF>
+enum SpecOp : int { OP_ID = 0, OP_CURL = 1, OP_BS = 2 };
+
+template <typename T>
+__device__ __forceinline__ cpx<T> spec_op(int op, int comp, const cpx<T>* x, T kx, T ky, T kz, T wki) {
+  if (op == OP_ID) return x[comp];
+  cpx<T> r;  // (i k x x)_comp
+  if (comp == 0) r = cpx<T>{-(ky * x[2].y - kz * x[1].y), ky * x[2].x - kz * x[1].x};
+  else if (comp == 1) r = cpx<T>{-(kz * x[0].y - kx * x[2].y), kz * x[0].x - kx * x[2].x};
+  else r = cpx<T>{-(kx * x[1].y - ky * x[0].y), kx * x[1].x - ky * x[0].x};
+  if (op == OP_BS) { r.x *= wki; r.y *= wki; }
+  return r;
+}
+
+template <typename T, int N, int NC, int NF, int MODE = 0>
 __global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G)
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
-       int mask_vel, int* status) {
+       int mask_vel, int* status, Fields4<T> in2 = Fields4<T>{}, int ops = 0) {
   using F = LineFFT<N, +1, T>;
   constexpr int W = kTileW;
   constexpr int SX = ColStride<F::SMEM>::value;
@@ -119,10 +137,14 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   const long tile = ((long)xt * Y + iky) * Y * W;
   if (tid == 0) mbar_init(&s_bar, 1);
   __syncthreads();
+  auto src_comp = [&](int q) -> const cpx<T>* {
+    if (MODE == 1 && q >= 3) return in2.c[q - 3];
+    return in.c[q];
+  };
   if (tid == 0) {
     mbar_expect_tx(&s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
     for (int q = 0; q < NC; ++q)
-      bulk_g2s(s_in + q * Y * W, in.c[q] + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), &s_bar);
+      bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), &s_bar);
   }
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   // mirror column for the Hermitian completion of kx = 0 (only tile 0, ky <= 0)
@@ -131,7 +153,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
     const long mt = ((long)0 * Y + (2 * K - iky)) * Y * W;
     for (int i = tid; i < NC * Y; i += nth) {
       const int q = i / Y, ikz = i % Y;
-      s_mir[i] = in.c[q][mt + (long)(2 * K - ikz) * W];
+      s_mir[i] = src_comp(q)[mt + (long)(2 * K - ikz) * W];
     }
   }
   for (int idx = tid; idx < Y * W; idx += nth) {
@@ -160,7 +182,22 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
     for (int e = 0; e < F::E; ++e) {
       const int ikz = row_to_box(F::in_index(gi, e), K, N);
       cpx<T> r = czero<T>();
-      if (ikz >= 0 && live_col && live_f) {
+      if (MODE == 1) {
+        if (ikz >= 0 && live_col && live_f && s_ll[ikz * W + c]) {
+          const int sl = f / 3, comp = f % 3;
+          cpx<T> x[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int q = 3 * sl + j;
+            if (mcol && !(iky == K && ikz > K)) x[j] = cconj(s_mir[q * Y + ikz]);
+            else if (mcol) x[j] = s_in[q * Y * W + ikz * W];
+            else x[j] = s_in[q * Y * W + ikz * W + c];
+          }
+          const T kz = (T)(ikz - K);
+          const T wki = wkinv(kx * kx + ky * ky + kz * kz);
+          r = spec_op<T>((ops >> (4 * sl)) & 15, comp, x, kx, ky, kz, wki);
+        }
+      } else if (ikz >= 0 && live_col && live_f) {
         cpx<T> xi, et, zt, rho;
         if (mcol) {
           if (iky == K && ikz == K) {
@@ -753,6 +790,13 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
     const cpx<T> V = s_in[(1 * N + ikz) * W + cc];
     const cpx<T> Wv = s_in[(2 * N + ikz) * W + cc];
     const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + ikz) * W + cc] : czero<T>();
+    if (SCHEME == SCHEME_RAW) {
+      const T LL = keep_mode<T>(ikx, iy, iz, g.K, g.alpha) ? (T)1 : (T)0;
+      R.K1.c[0][ik] = cpx<T>{LL * U.x, LL * U.y};
+      R.K1.c[1][ik] = cpx<T>{LL * V.x, LL * V.y};
+      R.K1.c[2][ik] = cpx<T>{LL * Wv.x, LL * Wv.y};
+      continue;
+    }
     // curl of F(-(u x w)) as preStep/corStep form it (3D_NavierStokes/src/kernels.h:327-334)
     scheme_point<T, SCHEME>(g, R, p, stage, ik, ikx, iy, iz, ky * Wv.y - kz * V.y,
                             kz * V.x - ky * Wv.x, kz * U.y - kx * Wv.y, kx * Wv.x - kz * U.x,
@@ -878,6 +922,195 @@ __global__ void copy_fields(Fields4<T> src, Fields4<T> dst, int nc, long len) {
     for (int q = 0; q < nc; ++q) dst.c[q][i] = src.c[q][i];
 }
 
+
+// ---------------------------------------------------------------------------
+// tangent-linear and adjoint of the RK4/CN step (SCHEME_NS_RK4)
+//
+// With E the inverse transform of a stored half spectrum (Hermitian
+// completion), F = (1/N^3) FFT restricted to the kept modes, B = i k x / k^2
+// (Biot-Savart), C = i k x (curl), the right-hand side is
+//   N(w) = C F(E(B w) x E(w)),
+// bilinear in w, so N'(w) d = C F(E(B d) x E(w)) + C F(E(B w) x E(d)).  Under
+// the real inner product of the stored coefficients E^T = 2 N^3 F and
+// F^T = E / (2 N^3), B and C are self-adjoint, and a.(b x c) = b.(c x a), so
+//   N'(w)^T l = B F(E(w) x E(C l)) + F(E(C l) x E(B w)).
+// Every term is one bilinear product P(a, b) = F(-(E(a) x E(b))) of the five
+// passes (pass A in pair mode, pass E in raw mode); the kernels below combine
+// the products and apply the stage arithmetic of scheme_point's RK4 branch.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct TileMode {
+  bool ok, keep;
+  T kx, ky, kz, wk;
+};
+
+// mode of element i of a tile-major box [xt][iky][ikz][W]
+template <typename T>
+__device__ __forceinline__ TileMode<T> tile_mode(const Geom3<T>& g, long i) {
+  TileMode<T> m;
+  const int W = kTileW;
+  const int w = (int)(i % W);
+  long q = i / W;
+  const int ikz = (int)(q % g.Y); q /= g.Y;
+  const int iky = (int)(q % g.Y);
+  const int ikx = (int)(q / g.Y) * W + w;
+  m.ok = ikx < g.X;
+  m.keep = m.ok && keep_mode<T>(ikx, iky - g.K, ikz - g.K, g.K, g.alpha);
+  m.kx = (T)ikx * g.alpha; m.ky = (T)(iky - g.K); m.kz = (T)(ikz - g.K);
+  m.wk = m.kx * m.kx + m.ky * m.ky + m.kz * m.kz;
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ void load3(const Fields4<T>& F, long i, cpx<T> (&x)[3]) {
+  x[0] = F.c[0][i]; x[1] = F.c[1][i]; x[2] = F.c[2][i];
+}
+
+// out = -LL C (Pa + Pb)                       (tangent right-hand side)
+// out = -LL (B Pa + Pb)                       (adjoint right-hand side)
+template <typename T>
+__global__ void lin_combine(Geom3<T> g, int adjoint, Fields4<T> Pa, Fields4<T> Pb, Fields4<T> out,
+                            long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    cpx<T> a[3], b[3], r[3];
+    load3(Pa, i, a);
+    load3(Pb, i, b);
+    if (!adjoint) {
+      cpx<T> s[3];
+      for (int c = 0; c < 3; ++c) s[c] = cpx<T>{a[c].x + b[c].x, a[c].y + b[c].y};
+      for (int c = 0; c < 3; ++c) r[c] = spec_op<T>(OP_CURL, c, s, m.kx, m.ky, m.kz, (T)0);
+    } else {
+      const T wki = wkinv(m.wk);
+      for (int c = 0; c < 3; ++c) {
+        const cpx<T> ba = spec_op<T>(OP_BS, c, a, m.kx, m.ky, m.kz, wki);
+        r[c] = cpx<T>{ba.x + b[c].x, ba.y + b[c].y};
+      }
+    }
+    const T LL = m.keep ? (T)-1 : (T)0;
+    for (int c = 0; c < 3; ++c) out.c[c][i] = cpx<T>{LL * r[c].x, LL * r[c].y};
+  }
+}
+
+// CN factor of an RK stage, (1 - q nk)/(1 + q nk) = 1 - e
+template <typename T>
+__device__ __forceinline__ T stage_e(T q, T nk) { return (T)2 * q * nk / ((T)1 + q * nk); }
+
+// tangent stage: K = dt LL n, Z = (1 - e)(D + fr K)
+template <typename T>
+__global__ void tan_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> n, Fields4<T> D,
+                          Fields4<T> Kout, Fields4<T> Zout, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    const T LL = m.keep ? (T)1 : (T)0;
+    const T e = stage_e(q, dt * nu * m.wk);
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> nn = n.c[c][i], d = D.c[c][i];
+      const cpx<T> k = cpx<T>{dt * LL * nn.x, dt * LL * nn.y};
+      const cpx<T> v = cpx<T>{d.x + fr * k.x, d.y + fr * k.y};
+      Kout.c[c][i] = k;
+      Zout.c[c][i] = cpx<T>{v.x - e * v.x, v.y - e * v.y};
+    }
+  }
+}
+
+// divergence removal of scheme_point's final stage, o - k (k.o) / k^2
+template <typename T>
+__device__ __forceinline__ void remove_div(const TileMode<T>& m, cpx<T> (&o)[3]) {
+  const T wki = wkinv(m.wk);
+  const T pr = (m.kx * o[0].x + m.ky * o[1].x + m.kz * o[2].x) * wki;
+  const T pi = (m.kx * o[0].y + m.ky * o[1].y + m.kz * o[2].y) * wki;
+  o[0] = cpx<T>{o[0].x - m.kx * pr, o[0].y - m.kx * pi};
+  o[1] = cpx<T>{o[1].x - m.ky * pr, o[1].y - m.ky * pi};
+  o[2] = cpx<T>{o[2].x - m.kz * pr, o[2].y - m.kz * pi};
+}
+
+// tangent final stage:
+// D' = Pdiv LL [(1 - eS) D + (1 - eI)(K1/6 + dt n/6 + (K2 + K3)/3)]
+template <typename T>
+__global__ void tan_final(Geom3<T> g, T dt, T nu, Fields4<T> n, Fields4<T> K1, Fields4<T> K2,
+                          Fields4<T> K3, Fields4<T> D, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    const T LL = m.keep ? (T)1 : (T)0;
+    const T nk = dt * nu * m.wk, hn = (T)0.5 * nk;
+    const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
+    const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
+    cpx<T> o[3];
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> d = D.c[c][i], a = K1.c[c][i], b = K2.c[c][i], k3 = K3.c[c][i], nn = n.c[c][i];
+      const T ix = sixth * (a.x + dt * nn.x) + third * (b.x + k3.x);
+      const T iy = sixth * (a.y + dt * nn.y) + third * (b.y + k3.y);
+      o[c] = cpx<T>{LL * ((d.x - eS * d.x) + (ix - eI * ix)), LL * ((d.y - eS * d.y) + (iy - eI * iy))};
+    }
+    remove_div(m, o);
+    for (int c = 0; c < 3; ++c) D.c[c][i] = o[c];
+  }
+}
+
+// adjoint of the final stage: a = LL Pdiv L', Lz = (1 - eS) a, b = (1 - eI) a,
+// Lk1 = b/6, Lk2 = Lk3 = b/3, Ln = dt b/6
+template <typename T>
+__global__ void adj_final(Geom3<T> g, T dt, T nu, Fields4<T> Lin, Fields4<T> Lz, Fields4<T> Lk1,
+                          Fields4<T> Lk2, Fields4<T> Lk3, Fields4<T> Ln, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    const T LL = m.keep ? (T)1 : (T)0;
+    const T nk = dt * nu * m.wk, hn = (T)0.5 * nk;
+    const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
+    cpx<T> a[3];
+    load3(Lin, i, a);
+    remove_div(m, a);
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> x = cpx<T>{LL * a[c].x, LL * a[c].y};
+      const cpx<T> b = cpx<T>{x.x - eI * x.x, x.y - eI * x.y};
+      Lz.c[c][i] = cpx<T>{x.x - eS * x.x, x.y - eS * x.y};
+      Lk1.c[c][i] = cpx<T>{b.x / (T)6, b.y / (T)6};
+      Lk2.c[c][i] = cpx<T>{b.x / (T)3, b.y / (T)3};
+      Lk3.c[c][i] = cpx<T>{b.x / (T)3, b.y / (T)3};
+      Ln.c[c][i] = cpx<T>{dt * b.x / (T)6, dt * b.y / (T)6};
+    }
+  }
+}
+
+// adjoint of an RK stage Z = (1 - e)(D + fr K) given Ls, the adjoint of Z:
+// Lz += (1 - e) Ls, Lk += fr (1 - e) Ls, and Ln = dt LL Lk, the input of the
+// adjoint right-hand side of the stage that produced K
+template <typename T>
+__global__ void adj_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> Ls, Fields4<T> Lz,
+                          Fields4<T> Lk, Fields4<T> Ln, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    const T LL = m.keep ? (T)1 : (T)0;
+    const T e = stage_e(q, dt * nu * m.wk);
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> l = Ls.c[c][i];
+      const cpx<T> dl = cpx<T>{l.x - e * l.x, l.y - e * l.y};
+      const cpx<T> z = Lz.c[c][i], k = Lk.c[c][i];
+      Lz.c[c][i] = cpx<T>{z.x + dl.x, z.y + dl.y};
+      const cpx<T> kn = cpx<T>{k.x + fr * dl.x, k.y + fr * dl.y};
+      Lk.c[c][i] = kn;
+      Ln.c[c][i] = cpx<T>{dt * LL * kn.x, dt * LL * kn.y};
+    }
+  }
+}
+
+// y += a x
+template <typename T>
+__global__ void lin_axpy(Fields4<T> y, T a, Fields4<T> x, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x)
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> u = y.c[c][i], v = x.c[c][i];
+      y.c[c][i] = cpx<T>{u.x + a * v.x, u.y + a * v.y};
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host engine
 // ---------------------------------------------------------------------------
@@ -901,6 +1134,10 @@ struct Engine3D final : Engine3DBase {
   double2* stage_h = nullptr;  // device FP64 staging box
   int* d_status = nullptr;     // device error flag of the bounded waits
   double* d_energ = nullptr;   // energetics partial sums
+  // linearised step (tangent / adjoint), allocated on first use
+  cpx<T>* lin = nullptr;
+  Fields4<T> Zb[4]{};          // base stage states z, z1, z2, z3
+  Fields4<T> LA{}, LN{}, LS{}, LZ{}, LK1{}, LK2{}, LK3{}, PA{}, PB{}, LD{};
   int c_variant = 0;           // x-pass variant chosen by the autotuner
   int c_resident[4] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
   float c_ms[4] = {0, 0, 0, 0};      // autotuner timings (ms per launch)
@@ -1064,6 +1301,8 @@ struct Engine3D final : Engine3DBase {
     if (dump) cudaFree(dump);
     if (d_status) cudaFree(d_status);
     if (d_energ) cudaFree(d_energ);
+    if (lin) cudaFree(lin);
+    lin = nullptr;
     d_energ = nullptr;
     pool = nullptr; stage_h = nullptr; dump = nullptr; d_status = nullptr;
   }
@@ -1344,6 +1583,186 @@ struct Engine3D final : Engine3DBase {
       box_to_ref<T><<<592, 256, 0, stream>>>(g, R.S.c[q], (double2*)comps[q], R.SC.c[q]);
       ++launches;
     }
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  // ---------------------------------------------------------------- linearised step
+  size_t smem_pair() const {
+    return sizeof(cpx<T>) * ((size_t)6 * g.Y * kTileW + (size_t)6 * g.Y + g.n +
+                             2 * kTileW * col_stride()) + g.Y * kTileW;
+  }
+
+  template <int N>
+  int lin_attrs() {
+    int dev = 0, big = 0;
+    PSG_CUDA_TRY(cudaGetDevice(&dev));
+    PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    big -= 1024;
+    if (smem_pair() > (size_t)big) {
+      psg_set_error("linearised step at grid %d needs %zu bytes of shared memory per block", g.n,
+                    smem_pair());
+      return PSG_ERR_UNSUPPORTED;
+    }
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, 6, 6, 1>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, 3, SCHEME_RAW>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    return PSG_OK;
+  }
+
+  int lin_init() {
+    if (lin) return PSG_OK;
+    if (scheme != SCHEME_NS_RK4) {
+      psg_set_error("tangent and adjoint steps are defined for the Navier-Stokes RK4/CN scheme");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    int rc;
+    switch (g.n) {
+      case 16: rc = lin_attrs<16>(); break;
+      case 32: rc = lin_attrs<32>(); break;
+      case 64: rc = lin_attrs<64>(); break;
+      case 128: rc = lin_attrs<128>(); break;
+      default: rc = lin_attrs<256>(); break;
+    }
+    if (rc) return rc;
+    constexpr int kFields = 14;
+    PSG_CUDA_TRY(cudaMalloc(&lin, sizeof(cpx<T>) * kFields * 3 * box));
+    PSG_CUDA_TRY(cudaMemsetAsync(lin, 0, sizeof(cpx<T>) * kFields * 3 * box, stream));
+    cpx<T>* p = lin;
+    Fields4<T>* all[kFields] = {&Zb[0], &Zb[1], &Zb[2], &Zb[3], &LA, &LN, &LS,
+                                &LZ, &LK1, &LK2, &LK3, &PA, &PB, &LD};
+    for (Fields4<T>* f : all) {
+      for (int q = 0; q < 4; ++q) f->c[q] = nullptr;
+      for (int q = 0; q < 3; ++q) { f->c[q] = p; p += box; }
+    }
+    return PSG_OK;
+  }
+
+  // out = P(a, b) = F(-(E(op_a a) x E(op_b b))), a in pass C's u slots, b in its w slots
+  template <int N>
+  int bilinear_n(Fields4<T> b, int op_b, Fields4<T> a, int op_a, Fields4<T> out) {
+    using FG = LineFFT<N, 1, T>;
+    const dim3 blk(kTileW * FG::G), blk2(2 * kTileW * FG::G);
+    const int XT = g.XP / kTileW;
+    pass_a<T, N, 6, 6, 1><<<dim3(XT, g.Y), blk2, smem_pair(), stream>>>(
+        g, b, B1, tw, 0, d_status, a, op_b | (op_a << 4));
+    pass_b<T, N><<<dim3(XT, N, 6), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
+    launch_c<N>(c_variant, (T)1 / ((T)N * (T)N * (T)N), nullptr);
+    pass_d<T, N><<<dim3(XT, N, 3), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
+    Regs<T> Rr{};
+    Rr.K1 = out;
+    pass_e<T, N, 3, SCHEME_RAW><<<dim3(XT, g.Y), blk, smem_e(), stream>>>(g, B2, tw, Rr, prm, 0,
+                                                                          d_status);
+    launches += 5;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+  int bilinear(Fields4<T> b, int op_b, Fields4<T> a, int op_a, Fields4<T> out) {
+    switch (g.n) {
+      case 16: return bilinear_n<16>(b, op_b, a, op_a, out);
+      case 32: return bilinear_n<32>(b, op_b, a, op_a, out);
+      case 64: return bilinear_n<64>(b, op_b, a, op_a, out);
+      case 128: return bilinear_n<128>(b, op_b, a, op_a, out);
+      default: return bilinear_n<256>(b, op_b, a, op_a, out);
+    }
+  }
+
+  // out = N'(z) x (tangent) or N'(z)^T x (adjoint)
+  int lin_rhs(int adjoint, Fields4<T> z, Fields4<T> x, Fields4<T> out) {
+    int rc;
+    if (!adjoint) {
+      if ((rc = bilinear(z, OP_ID, x, OP_BS, PA))) return rc;  // F(-(E(B x) x E(z)))
+      if ((rc = bilinear(x, OP_ID, z, OP_BS, PB))) return rc;  // F(-(E(B z) x E(x)))
+    } else {
+      if ((rc = bilinear(x, OP_CURL, z, OP_ID, PA))) return rc;  // F(-(E(z) x E(C x)))
+      if ((rc = bilinear(z, OP_BS, x, OP_CURL, PB))) return rc;  // F(-(E(C x) x E(B z)))
+    }
+    lin_combine<T><<<592, 256, 0, stream>>>(g, adjoint, PA, PB, out, box);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  // one forward step from S with X0 = S, keeping the four stage states
+  int base_stages(T dt) {
+    prm.dt = dt;
+    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, 3, box);
+    copy_fields<T><<<592, 256, 0, stream>>>(R.S, Zb[0], 3, box);
+    launches += 2;
+    const int stg[3] = {STAGE_RK1, STAGE_RK2, STAGE_RK3};
+    for (int s = 0; s < 3; ++s) {
+      if (int rc = rhs(stg[s])) return rc;
+      copy_fields<T><<<592, 256, 0, stream>>>(R.X0, Zb[s + 1], 3, box);
+      ++launches;
+    }
+    return rhs(STAGE_RK4);
+  }
+
+  // D <- dPhi(S) D, S <- Phi(S)
+  int tangent_step_t(T dt, Fields4<T> D) {
+    int rc;
+    if ((rc = base_stages(dt))) return rc;
+    const T nu = prm.nu;
+    const T qs[3] = {(T)0.25, (T)0.25, (T)0.5}, frs[3] = {(T)0.5, (T)0.5, (T)1};
+    Fields4<T> Ks[3] = {LK1, LK2, LK3};
+    Fields4<T> in = D;
+    for (int s = 0; s < 3; ++s) {
+      if ((rc = lin_rhs(0, Zb[s], in, LN))) return rc;
+      tan_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LN, D, Ks[s], LA, box);
+      ++launches;
+      in = LA;
+    }
+    if ((rc = lin_rhs(0, Zb[3], LA, LN))) return rc;
+    tan_final<T><<<592, 256, 0, stream>>>(g, dt, nu, LN, LK1, LK2, LK3, D, box);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  // L <- dPhi(S)^T L, S <- Phi(S)
+  int adjoint_step_t(T dt, Fields4<T> L) {
+    int rc;
+    if ((rc = base_stages(dt))) return rc;
+    const T nu = prm.nu;
+    adj_final<T><<<592, 256, 0, stream>>>(g, dt, nu, L, LZ, LK1, LK2, LK3, LN, box);
+    ++launches;
+    const T qs[3] = {(T)0.5, (T)0.25, (T)0.25}, frs[3] = {(T)1, (T)0.5, (T)0.5};
+    Fields4<T> Ks[3] = {LK3, LK2, LK1};
+    for (int s = 0; s < 3; ++s) {
+      if ((rc = lin_rhs(1, Zb[3 - s], LN, LS))) return rc;
+      adj_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LS, LZ, Ks[s], LN, box);
+      ++launches;
+    }
+    if ((rc = lin_rhs(1, Zb[0], LN, LS))) return rc;
+    lin_axpy<T><<<592, 256, 0, stream>>>(LZ, (T)1, LS, box);
+    copy_fields<T><<<592, 256, 0, stream>>>(LZ, L, 3, box);
+    launches += 2;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  // mode 0: tangent step, 1: adjoint step, 2: tangent right-hand side N'(S) x,
+  // 3: adjoint right-hand side N'(S)^T x.  in / out: device FP64 boxes in the
+  // reference layout (3 components), ordered on the engine's stream.
+  int linear(int mode, double dt, const void* const* in, void* const* out) override {
+    int rc;
+    if ((rc = lin_init())) return rc;
+    for (int q = 0; q < 3; ++q)
+      box_from_ref<T><<<592, 256, 0, stream>>>(g, (const double2*)in[q], LD.c[q], nullptr);
+    launches += 3;
+    Fields4<T> res = LD;
+    switch (mode) {
+      case 0: rc = tangent_step_t((T)dt, LD); break;
+      case 1: rc = adjoint_step_t((T)dt, LD); break;
+      case 2: rc = lin_rhs(0, R.S, LD, LS); res = LS; break;
+      case 3: rc = lin_rhs(1, R.S, LD, LS); res = LS; break;
+      default: psg_set_error("linear mode %d unknown", mode); return PSG_ERR_ARG;
+    }
+    if (rc) return rc;
+    for (int q = 0; q < 3; ++q)
+      box_to_ref<T><<<592, 256, 0, stream>>>(g, res.c[q], (double2*)out[q], nullptr);
+    launches += 3;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
