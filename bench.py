@@ -224,6 +224,7 @@ def run_ours(args, rank, world, dist):
     eng.close()
 
     upo = run_upo(args) if (world == 1 and not args.no_upo) else None
+    ens = run_ensemble2d(args) if (world == 1 and not args.no_ensemble) else None
 
     out = None
     if rank == 0:
@@ -242,6 +243,7 @@ def run_ours(args, rank, world, dist):
                        "grid": N, "replicas": world, "parallelism": f"replicas{world}",
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
             "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu, "upo": upo,
+            "ensemble2d": ens,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
                                 "variants": ["L=128/G,1 stage", "L=256/G,1 stage",
@@ -250,6 +252,56 @@ def run_ours(args, rank, world, dist):
         if out_note:
             out["note"] = out_note
     return out
+
+
+class quiet_stdout:
+    """Send what native code writes to file descriptor 1 (the reference's
+    progress lines) to stderr, so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
+        self._libc = ctypes.CDLL(None)
+        self._libc.fflush(None)
+        self._saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self._libc.fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        return False
+
+
+def ref2d_step_ms(steps, n=None):
+    """ms per step of the reference's 2D timestep_cuda_ (n^2, default 128^2, one
+    call of `steps` steps including its per-call set-up), in a fresh process"""
+    cmd = [sys.executable, os.path.abspath(__file__), "--ref2d-probe", str(steps)]
+    if n:
+        cmd += ["--grid2d", str(n)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)["ms_per_step"]
+    raise RuntimeError("reference 2D probe failed: " + r.stderr[-400:])
+
+
+def run_ref2d_probe(steps, n=None):
+    import torch
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import kolmogorov_ic2d
+
+    torch.cuda.set_device(0)
+    n = n or UPO_N
+    lib = TimestepLibrary(os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so"), "ns2d")
+    Z = kolmogorov_ic2d(n, 4242)
+    with quiet_stdout():
+        lib.ns2d(Z, n, UPO_NU, UPO_DT, 10)
+        t0 = time.perf_counter()
+        lib.ns2d(Z, n, UPO_NU, UPO_DT, steps)
+        sec = time.perf_counter() - t0
+    return {"ms_per_step": 1e3 * sec / steps, "steps": steps, "n": n}
 
 
 # ------------------------------------------------------ UPO Newton iterations
@@ -306,14 +358,8 @@ def run_upo(args):
     # plain form: the reference's own 2D step, one integration per call
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
     if os.path.exists(path):
-        lib = TimestepLibrary(path, "ns2d")
-        Z = guesses[0].copy()
-        lib.ns2d(Z, n, nu, dt, 10)
         nst = int(round(12.5 / dt))
-        t0 = time.perf_counter()
-        lib.ns2d(Z, n, nu, dt, nst)
-        call_s = time.perf_counter() - t0
-        step_s = call_s / nst
+        step_s = ref2d_step_ms(nst) / 1e3
         plain_s = sum(k * (periods[i] / dt) * step_s for i, k in enumerate(per_guess_integrations))
         newton = out["exact_jv"]["newton_iters"]
         out["plain_reference"] = {
@@ -322,9 +368,77 @@ def run_upo(args):
             "how": "the same Newton iterations as the exact-Jv run, each integration a "
                    "reference timestep_cuda_ call (FP64 cuFFT, one guess at a time) costed at "
                    f"its measured {1e3 * step_s:.4f} ms/step (one call of {nst} steps incl. "
-                   "its set-up); host Arnoldi/SVD time not included"}
+                   "its set-up, timed in a separate process); host Arnoldi/SVD time not "
+                   "included"}
         out["exact_vs_plain"] = round(out["exact_jv"]["newton_iters_per_s"] /
                                       out["plain_reference"]["newton_iters_per_s"], 2)
+    return out
+
+
+# ------------------------------------------------------------ 2D ensemble
+def run_ensemble2d(args):
+    """512 independent 2D Kolmogorov runs in one persistent launch replayed as a
+    CUDA graph: sizes uniform over {64^2, 128^2, 256^2}, Re uniform in [20, 100],
+    forcing wavenumber 4, seeded initial vorticity (modes 1 <= |k| <= 8, phases
+    uniform, amplitude ~ 1/|k|, enstrophy 1), dt = 0.005, 1000 steps each, FP32;
+    block size picked by the autotuner.  Instance-steps per second on the device
+    and end to end (initial states uploaded from the host and final states
+    downloaded inside the timed region), beside the reference's 2D step run one
+    instance at a time (its ms/step per size measured on a 200-step call)."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.fields import kolmogorov_ic2d
+
+    M, steps = 512, 1000
+    rng = np.random.default_rng(2048)
+    sizes = rng.choice([64, 128, 256], M)
+    nu = 1.0 / rng.uniform(20.0, 100.0, M)
+    ics = [kolmogorov_ic2d(int(n), 9000 + i) for i, n in enumerate(sizes)]
+    b = P.Batch2D(sizes, precision=32)
+    for i in range(M):
+        b.upload(i, ics[i])
+    b.set_params(nu, 0.005, steps)
+    tune = b.autotune()
+    stream = torch.cuda.current_stream()
+    b.set_stream(stream.cuda_stream)
+    b.launch()  # warm-up: captures the graph
+    b.sync()
+    for i in range(M):
+        b.upload(i, ics[i])
+    l0 = b.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_s = e0.elapsed_time(e1) / 1e3
+    launches = b.launches - l0
+    # end to end: upload every initial state, integrate, download every result
+    t0 = time.perf_counter()
+    for i in range(M):
+        b.upload(i, ics[i])
+    b.launch()
+    outs = [b.download(i) for i in range(M)]
+    e2e_s = time.perf_counter() - t0
+    finite = all(np.isfinite(o).all() for o in outs)
+    b.close()
+    out = {"workload": "512 x 2D Kolmogorov, sizes U{64,128,256}^2, Re U[20,100], kf=4, "
+                       "dt=0.005, 1000 steps, FP32, one persistent launch (CUDA graph)",
+           "instance_steps_per_s": round(M * steps / dev_s, 1), "seconds": round(dev_s, 4),
+           "e2e_instance_steps_per_s": round(M * steps / e2e_s, 1), "e2e_seconds": round(e2e_s, 3),
+           "gpu_launches": launches, "finite": bool(finite),
+           "block_autotune": {"variant": tune[0], "ms_per_2_steps": [round(x, 4) for x in tune[1]],
+                              "threads": [128, 256, 512]}}
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
+    if os.path.exists(path):
+        ms = {int(n): ref2d_step_ms(200, int(n)) for n in (64, 128, 256)}
+        ref_s = sum(steps * ms[int(n)] / 1e3 for n in sizes)
+        out["plain_reference"] = {"instance_steps_per_s": round(M * steps / ref_s, 2),
+                                  "ms_per_step": {str(k): round(v, 4) for k, v in ms.items()},
+                                  "how": "one reference timestep_cuda_ call per instance, costed "
+                                         "at its measured ms/step per size (200-step call in a "
+                                         "separate process)"}
     return out
 
 
@@ -423,7 +537,8 @@ def run_reference(args, rank, world, dist):
     clk = ClockSampler(dev.index)
     clk.start()
     clk.wait_first()
-    e2e = time_abi_calls(lib, args, dev, dist, world, rank, ours=False)
+    with quiet_stdout():
+        e2e = time_abi_calls(lib, args, dev, dist, world, rank, ours=False)
     clocks = clk.stop()
     if rank != 0:
         return None
@@ -502,7 +617,8 @@ def run_accuracy(args):
         lib = TimestepLibrary(path, "bous3d")
         comps = [a.copy() for a in (xi, et, zt, np.zeros_like(xi))]
         t0 = time.perf_counter()
-        lib.bous3d_inplace(comps, N, NU, DT, nsteps * DT)
+        with quiet_stdout():
+            lib.bous3d_inplace(comps, N, NU, DT, nsteps * DT)
         ref = np.stack(comps[:3])
         out["reference_fp64_seconds"] = round(time.perf_counter() - t0, 2)
         out["reference_steps"] = rk4_evaluations(0.0, nsteps * DT, DT)
@@ -595,6 +711,9 @@ def main():
                     help="run the 128^3 gradient study over STEPS steps instead")
     ap.add_argument("--adjoint-dirs", type=int, default=16,
                     help="finite-difference directions of the gradient study")
+    ap.add_argument("--ref2d-probe", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--grid2d", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 2D ensemble leg")
     ap.add_argument("--no-ref", action="store_true",
                     help="accuracy study without the reference FP64 run")
     args = ap.parse_args()
@@ -605,6 +724,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
+    if args.ref2d_probe:
+        print(json.dumps(run_ref2d_probe(args.ref2d_probe, args.grid2d or None)), flush=True)
+        return
     if args.accuracy:
         if rank == 0:
             print(json.dumps(run_accuracy(args)), flush=True)

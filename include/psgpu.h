@@ -127,6 +127,17 @@ int psg_batch2d_download(psg_batch2d* h, int i, double* Z);
 /* enqueue nsteps[i] steps of length dt[i] with viscosity nu[i] for every
  * instance, in one kernel launch on the handle's stream */
 int psg_batch2d_run(psg_batch2d* h, const double* nu, const double* dt, const int* nsteps);
+/* psg_batch2d_run in two parts: set the per-instance parameters (waits for the
+ * small host-to-device copy), then launch the integration as one CUDA graph
+ * (reset of the work counter + the persistent kernel), which later launches
+ * replay without host work; the graph is captured on first launch */
+int psg_batch2d_set_params(psg_batch2d* h, const double* nu, const double* dt, const int* nsteps);
+int psg_batch2d_launch(psg_batch2d* h);
+/* time the persistent kernel at 128, 256 and 512 threads per block on the
+ * current parameters (2-step runs, states restored afterwards) and keep the
+ * fastest; variant 0/1/2, ms[3] per run (-1: does not fit) */
+int psg_batch2d_autotune(psg_batch2d* h, int* variant, float* ms);
+int psg_batch2d_tuning(psg_batch2d* h, int* variant, float* ms);
 int psg_batch2d_sync(psg_batch2d* h);
 long psg_batch2d_launches(psg_batch2d* h);
 /* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]).

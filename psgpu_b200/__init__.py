@@ -92,6 +92,10 @@ def _declare_2d(L):
     L.psg_batch2d_upload.argtypes = [vp, i, dp]
     L.psg_batch2d_download.argtypes = [vp, i, dp]
     L.psg_batch2d_run.argtypes = [vp, dp, dp, ip]
+    L.psg_batch2d_set_params.argtypes = [vp, dp, dp, ip]
+    L.psg_batch2d_launch.argtypes = [vp]
+    L.psg_batch2d_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
+    L.psg_batch2d_tuning.argtypes = [vp, ip, C.POINTER(C.c_float)]
     L.psg_batch2d_sync.argtypes = [vp]
     L.psg_batch2d_launches.argtypes = [vp]
     L.psg_batch2d_launches.restype = C.c_long
@@ -303,14 +307,35 @@ class Batch2D:
         _check(lib().psg_batch2d_download(self._h, i, a.ctypes.data_as(C.POINTER(C.c_double))))
         return a
 
-    def run(self, nu, dt, nsteps):
+    def _params(self, nu, dt, nsteps):
         m = len(self.sizes)
         nu = np.broadcast_to(np.asarray(nu, np.float64), (m,)).copy()
         dt = np.broadcast_to(np.asarray(dt, np.float64), (m,)).copy()
         ns = np.broadcast_to(np.asarray(nsteps, np.int32), (m,)).copy()
-        _check(lib().psg_batch2d_run(self._h, nu.ctypes.data_as(C.POINTER(C.c_double)),
-                                     dt.ctypes.data_as(C.POINTER(C.c_double)),
-                                     ns.ctypes.data_as(C.POINTER(C.c_int))))
+        return (nu, dt, ns), (nu.ctypes.data_as(C.POINTER(C.c_double)),
+                              dt.ctypes.data_as(C.POINTER(C.c_double)),
+                              ns.ctypes.data_as(C.POINTER(C.c_int)))
+
+    def run(self, nu, dt, nsteps):
+        """integrate every instance i by nsteps[i] steps of dt[i] at viscosity nu[i]"""
+        keep, args = self._params(nu, dt, nsteps)
+        _check(lib().psg_batch2d_run(self._h, *args))
+
+    def set_params(self, nu, dt, nsteps):
+        keep, args = self._params(nu, dt, nsteps)
+        _check(lib().psg_batch2d_set_params(self._h, *args))
+
+    def launch(self):
+        """one integration with the current parameters, as a replayed CUDA graph"""
+        _check(lib().psg_batch2d_launch(self._h))
+
+    def autotune(self):
+        """block size of the persistent kernel: (variant, ms per 2-step run for 128,
+        256, 512 threads)"""
+        v = C.c_int()
+        ms = (C.c_float * 3)()
+        _check(lib().psg_batch2d_autotune(self._h, C.byref(v), ms))
+        return v.value, list(ms)
 
     def sync(self):
         _check(lib().psg_batch2d_sync(self._h))

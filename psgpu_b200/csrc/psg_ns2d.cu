@@ -20,8 +20,11 @@ struct Twiddles2D {
   const cpx<T>* t[5];  // n = 16, 32, 64, 128, 256
 };
 
-template <typename T>
-__global__ void __launch_bounds__(256)
+// block sizes of the persistent kernel the autotuner chooses from
+constexpr int kBlock2D[3] = {128, 256, 512};
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT)
 ns2d_persistent(const Inst2D<T>* __restrict__ insts, int ninst, int* __restrict__ next,
                 Twiddles2D<T> tws) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -73,6 +76,10 @@ struct Batch2DBase {
   virtual int upload(int i, const double* Z) = 0;
   virtual int download(int i, double* Z) = 0;
   virtual int run(const double* nu, const double* dt, const int* nsteps) = 0;
+  virtual int set_params(const double* nu, const double* dt, const int* nsteps) = 0;
+  virtual int launch() = 0;
+  virtual int autotune(int* variant, float* ms) = 0;
+  virtual int tuning(int* variant, float* ms) const = 0;
   virtual int sync() = 0;
   virtual long launch_count() const = 0;
   virtual void set_stream(cudaStream_t s) = 0;
@@ -94,9 +101,20 @@ struct Batch2D final : Batch2DBase {
   cudaStream_t stream = 0;
   long launches = 0;
   std::vector<int> order;     // instances sorted by cost, largest first
-  size_t smem = 0;
+  size_t smem_v[3] = {0, 0, 0};  // dynamic shared memory per block-size variant
+  int grid_v[3] = {0, 0, 0};     // resident blocks per variant (0: does not fit)
+  int variant = 1;               // 256 threads unless the autotuner picks another
+  float tune_ms[3] = {-1.f, -1.f, -1.f};
+  long state_words = 0;          // states (+ carried errors) of all instances
+  bool params_set = false;
+  // the persistent launch as a CUDA graph: reset the work counter, launch
+  cudaGraphExec_t gexec = nullptr;
+  int gexec_variant = -1;
+  cudaStream_t cap = nullptr;
 
   ~Batch2D() override {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (cap) cudaStreamDestroy(cap);
     if (pool) cudaFree(pool);
     if (d_insts) cudaFree(d_insts);
     if (d_next) cudaFree(d_next);
@@ -117,6 +135,7 @@ struct Batch2D final : Batch2DBase {
       total += (std::is_same<T, float>::value ? 6L : 5L) * nkt2(n);
       maxk = std::max<long>(maxk, nkt2(n));
     }
+    state_words = total;
     for (int i = 0; i < ninst; ++i) {
       woffs.push_back(total + work);
       work += 3L * sizes[i] * (sizes[i] / 3 + 1);
@@ -156,12 +175,75 @@ struct Batch2D final : Batch2DBase {
         case 128: gg = LineFFT<128, 1, T>::G; ss = LineFFT<128, 1, T>::SMEM; break;
         default: gg = LineFFT<256, 1, T>::G; ss = LineFFT<256, 1, T>::SMEM; break;
       }
-      worst = std::max(worst, (size_t)(2 * n + (256 / gg) * ss));
+      for (int v = 0; v < 3; ++v)
+        smem_v[v] = std::max(smem_v[v], sizeof(cpx<T>) * (size_t)(2 * n + (kBlock2D[v] / gg) * ss));
     }
     (void)g; (void)sm;
-    smem = sizeof(cpx<T>) * worst;
-    PSG_CUDA_TRY(cudaFuncSetAttribute(ns2d_persistent<T>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148, big = 0;
+    PSG_CUDA_TRY(cudaGetDevice(&dev));
+    PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    for (int v = 0; v < 3; ++v) {
+      const void* k = kernel(v);
+      grid_v[v] = 0;
+      if (smem_v[v] + 1024 > (size_t)big) continue;
+      PSG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_v[v]));
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kBlock2D[v], smem_v[v]);
+      grid_v[v] = std::max(0, std::min(ninst, nsm * per_sm));
+    }
+    if (!grid_v[variant]) {
+      variant = -1;
+      for (int v = 0; v < 3 && variant < 0; ++v)
+        if (grid_v[v]) variant = v;
+      if (variant < 0) {
+        psg_set_error("2D batch: no block size fits this device");
+        return PSG_ERR_UNSUPPORTED;
+      }
+    }
+    PSG_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    return PSG_OK;
+  }
+
+  static const void* kernel(int v) {
+    switch (v) {
+      case 0: return (const void*)ns2d_persistent<T, 128>;
+      case 1: return (const void*)ns2d_persistent<T, 256>;
+      default: return (const void*)ns2d_persistent<T, 512>;
+    }
+  }
+
+  Twiddles2D<T> twiddles() const {
+    Twiddles2D<T> tws;
+    long o = 0;
+    for (int q = 0, n = 16; q < 5; ++q, n *= 2) { tws.t[q] = twp + o; o += 2 * n; }
+    return tws;
+  }
+
+  void launch_kernel(int v, cudaStream_t st) {
+    const Twiddles2D<T> tws = twiddles();
+    switch (v) {
+      case 0: ns2d_persistent<T, 128><<<grid_v[0], 128, smem_v[0], st>>>(d_insts, ninst, d_next, tws); break;
+      case 1: ns2d_persistent<T, 256><<<grid_v[1], 256, smem_v[1], st>>>(d_insts, ninst, d_next, tws); break;
+      default: ns2d_persistent<T, 512><<<grid_v[2], 512, smem_v[2], st>>>(d_insts, ninst, d_next, tws); break;
+    }
+  }
+
+  // (re)build the graph of one persistent launch for the current variant
+  int build_graph() {
+    if (gexec && gexec_variant == variant) return PSG_OK;
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+    cudaGraph_t graph = nullptr;
+    PSG_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(d_next, 0, sizeof(int), cap);
+    launch_kernel(variant, cap);
+    cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    if (e != cudaSuccess) { psg_set_error("graph capture: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { psg_set_error("graph instantiate: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
+    gexec_variant = variant;
     return PSG_OK;
   }
 
@@ -192,6 +274,70 @@ struct Batch2D final : Batch2DBase {
   }
 
   int run(const double* nu, const double* dt, const int* nsteps) override {
+    int rc = set_params(nu, dt, nsteps);
+    return rc ? rc : launch();
+  }
+
+  int launch() override {
+    if (!params_set) { psg_set_error("2D batch: parameters not set"); return PSG_ERR_STATE; }
+    if (int rc = build_graph()) return rc;
+    PSG_CUDA_TRY(cudaGraphLaunch(gexec, stream));
+    ++launches;
+    return PSG_OK;
+  }
+
+  // time every block size on the current parameters (3 timed launches of a
+  // 2-step copy of the run after one warm-up), restoring the states after
+  // each, and keep the fastest
+  int autotune(int* v_out, float* ms) override {
+    if (!params_set) { psg_set_error("2D batch: parameters not set"); return PSG_ERR_STATE; }
+    std::vector<Inst2D<T>> h(hparams), shortp(hparams);
+    for (auto& I : shortp) I.nsteps = std::min(I.nsteps, 2);
+    cpx<T>* save = nullptr;
+    PSG_CUDA_TRY(cudaMalloc(&save, sizeof(cpx<T>) * state_words));
+    PSG_CUDA_TRY(cudaMemcpyAsync(save, pool, sizeof(cpx<T>) * state_words, cudaMemcpyDeviceToDevice, stream));
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_insts, shortp.data(), sizeof(Inst2D<T>) * ninst,
+                                 cudaMemcpyHostToDevice, stream));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    int pick = variant;
+    for (int v = 0; v < 3; ++v) {
+      tune_ms[v] = -1.f;
+      if (!grid_v[v]) continue;
+      cudaMemsetAsync(d_next, 0, sizeof(int), stream);
+      launch_kernel(v, stream);
+      cudaEventRecord(a, stream);
+      for (int r = 0; r < 3; ++r) {
+        cudaMemsetAsync(d_next, 0, sizeof(int), stream);
+        launch_kernel(v, stream);
+      }
+      cudaEventRecord(b, stream);
+      cudaError_t e = cudaEventSynchronize(b);
+      if (e != cudaSuccess) { cudaFree(save); psg_set_error("autotune: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
+      float t = 0.f;
+      cudaEventElapsedTime(&t, a, b);
+      tune_ms[v] = t / 3.f;
+      if (tune_ms[v] < best) { best = tune_ms[v]; pick = v; }
+    }
+    launches += 4 * 3;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    PSG_CUDA_TRY(cudaMemcpyAsync(pool, save, sizeof(cpx<T>) * state_words, cudaMemcpyDeviceToDevice, stream));
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst2D<T>) * ninst,
+                                 cudaMemcpyHostToDevice, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    cudaFree(save);
+    variant = pick;
+    if (v_out) *v_out = variant;
+    if (ms) for (int v = 0; v < 3; ++v) ms[v] = tune_ms[v];
+    return PSG_OK;
+  }
+
+  std::vector<Inst2D<T>> hparams;
+
+  int set_params(const double* nu, const double* dt, const int* nsteps) override {
     std::vector<Inst2D<T>> h(ninst);
     for (int j = 0; j < ninst; ++j) {
       const int i = order[j];
@@ -205,19 +351,16 @@ struct Batch2D final : Batch2DBase {
     }
     PSG_CUDA_TRY(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst2D<T>) * ninst,
                                  cudaMemcpyHostToDevice, stream));
-    PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
-    Twiddles2D<T> tws;
-    long o = 0;
-    for (int q = 0, n = 16; q < 5; ++q, n *= 2) { tws.t[q] = twp + o; o += 2 * n; }
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ns2d_persistent<T>, 256, smem);
-    const int grid = std::max(1, std::min(ninst, nsm * std::max(per_sm, 1)));
-    ns2d_persistent<T><<<grid, 256, smem, stream>>>(d_insts, ninst, d_next, tws);
-    ++launches;
-    PSG_CUDA_TRY(cudaGetLastError());
+    // the copy reads pageable host memory: finish it before h goes away
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    hparams = h;
+    params_set = true;
+    return PSG_OK;
+  }
+
+  int tuning(int* v_out, float* ms) const override {
+    if (v_out) *v_out = variant;
+    if (ms) for (int v = 0; v < 3; ++v) ms[v] = tune_ms[v];
     return PSG_OK;
   }
 
@@ -280,6 +423,24 @@ extern "C" int psg_batch2d_run(psg_batch2d* h, const double* nu, const double* d
   PSG_B2(h);
   if (!nu || !dt || !nsteps) { psg_set_error("null parameter arrays"); return PSG_ERR_ARG; }
   return h->b->run(nu, dt, nsteps);
+}
+extern "C" int psg_batch2d_set_params(psg_batch2d* h, const double* nu, const double* dt,
+                                      const int* nsteps) {
+  PSG_B2(h);
+  if (!nu || !dt || !nsteps) { psg_set_error("null parameter arrays"); return PSG_ERR_ARG; }
+  return h->b->set_params(nu, dt, nsteps);
+}
+extern "C" int psg_batch2d_launch(psg_batch2d* h) {
+  PSG_B2(h);
+  return h->b->launch();
+}
+extern "C" int psg_batch2d_autotune(psg_batch2d* h, int* variant, float* ms) {
+  PSG_B2(h);
+  return h->b->autotune(variant, ms);
+}
+extern "C" int psg_batch2d_tuning(psg_batch2d* h, int* variant, float* ms) {
+  PSG_B2(h);
+  return h->b->tuning(variant, ms);
 }
 extern "C" int psg_batch2d_sync(psg_batch2d* h) {
   PSG_B2(h);
