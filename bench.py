@@ -224,7 +224,7 @@ def run_ours(args, rank, world, dist):
     eng.close()
 
     upo = run_upo(args) if (world == 1 and not args.no_upo) else None
-    ens = run_ensemble2d(args) if (world == 1 and not args.no_ensemble) else None
+    ens = None if args.no_ensemble else run_ensemble2d(args, rank, world, dist, dev)
 
     out = None
     if rank == 0:
@@ -376,7 +376,7 @@ def run_upo(args):
 
 
 # ------------------------------------------------------------ 2D ensemble
-def run_ensemble2d(args):
+def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
     """512 independent 2D Kolmogorov runs in one persistent launch replayed as a
     CUDA graph: sizes uniform over {64^2, 128^2, 256^2}, Re uniform in [20, 100],
     forcing wavenumber 4, seeded initial vorticity (modes 1 <= |k| <= 8, phases
@@ -384,18 +384,25 @@ def run_ensemble2d(args):
     block size picked by the autotuner.  Instance-steps per second on the device
     and end to end (initial states uploaded from the host and final states
     downloaded inside the timed region), beside the reference's 2D step run one
-    instance at a time (its ms/step per size measured on a 200-step call)."""
+    instance at a time (its ms/step per size measured on a 200-step call).
+    With N ranks the 512 instances are split by cost (psgpu_b200.replicas) and
+    the time is the slowest rank's (strong scaling: the total work is fixed)."""
     import torch
     import psgpu_b200 as P
     from psgpu_b200.fields import kolmogorov_ic2d
+    from psgpu_b200.replicas import cost2d, max_over_ranks, shard
 
     M, steps = 512, 1000
     rng = np.random.default_rng(2048)
-    sizes = rng.choice([64, 128, 256], M)
-    nu = 1.0 / rng.uniform(20.0, 100.0, M)
-    ics = [kolmogorov_ic2d(int(n), 9000 + i) for i, n in enumerate(sizes)]
+    sizes_all = rng.choice([64, 128, 256], M)
+    nu_all = 1.0 / rng.uniform(20.0, 100.0, M)
+    mine = shard([cost2d(int(n)) for n in sizes_all], world)[rank]
+    sizes = [int(sizes_all[i]) for i in mine]
+    nu = nu_all[mine]
+    ics = [kolmogorov_ic2d(int(sizes_all[i]), 9000 + i) for i in mine]
+    m = len(mine)
     b = P.Batch2D(sizes, precision=32)
-    for i in range(M):
+    for i in range(m):
         b.upload(i, ics[i])
     b.set_params(nu, 0.005, steps)
     tune = b.autotune()
@@ -403,8 +410,11 @@ def run_ensemble2d(args):
     b.set_stream(stream.cuda_stream)
     b.launch()  # warm-up: captures the graph
     b.sync()
-    for i in range(M):
+    for i in range(m):
         b.upload(i, ics[i])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     l0 = b.launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -412,28 +422,32 @@ def run_ensemble2d(args):
     b.launch()
     e1.record(stream)
     torch.cuda.synchronize()
-    dev_s = e0.elapsed_time(e1) / 1e3
+    dev_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
     launches = b.launches - l0
     # end to end: upload every initial state, integrate, download every result
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
-    for i in range(M):
+    for i in range(m):
         b.upload(i, ics[i])
     b.launch()
-    outs = [b.download(i) for i in range(M)]
-    e2e_s = time.perf_counter() - t0
+    outs = [b.download(i) for i in range(m)]
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
     finite = all(np.isfinite(o).all() for o in outs)
     b.close()
+    if rank != 0:
+        return None
     out = {"workload": "512 x 2D Kolmogorov, sizes U{64,128,256}^2, Re U[20,100], kf=4, "
-                       "dt=0.005, 1000 steps, FP32, one persistent launch (CUDA graph)",
+                       "dt=0.005, 1000 steps, FP32, one persistent launch (CUDA graph) per GPU",
            "instance_steps_per_s": round(M * steps / dev_s, 1), "seconds": round(dev_s, 4),
            "e2e_instance_steps_per_s": round(M * steps / e2e_s, 1), "e2e_seconds": round(e2e_s, 3),
-           "gpu_launches": launches, "finite": bool(finite),
+           "scaling": "strong", "ranks": world, "gpu_launches": launches, "finite": bool(finite),
            "block_autotune": {"variant": tune[0], "ms_per_2_steps": [round(x, 4) for x in tune[1]],
                               "threads": [128, 256, 512]}}
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
-    if os.path.exists(path):
+    if os.path.exists(path) and world == 1:
         ms = {int(n): ref2d_step_ms(200, int(n)) for n in (64, 128, 256)}
-        ref_s = sum(steps * ms[int(n)] / 1e3 for n in sizes)
+        ref_s = sum(steps * ms[int(n)] / 1e3 for n in sizes_all)
         out["plain_reference"] = {"instance_steps_per_s": round(M * steps / ref_s, 2),
                                   "ms_per_step": {str(k): round(v, 4) for k, v in ms.items()},
                                   "how": "one reference timestep_cuda_ call per instance, costed "
