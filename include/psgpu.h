@@ -51,6 +51,13 @@ int psg_ns3d_create(psg_ns3d** h, int n, double alpha, int scheme, int precision
 void psg_ns3d_destroy(psg_ns3d* h);
 /* nu = 1/Re; ampfor/kf: forcing as the reference's d_AMPFOR/d_KFY; ri, sc,
  * theta (radians): Boussinesq parameters (ignored by the other schemes). */
+/* Heun/CN forcing of the 3D Navier-Stokes scheme: PSG_FORCING_DNS adds
+ * +-ampfor to Re xi at (0, kf, +-kf) (3D_NavierStokes/src/kernels.h:342-343);
+ * PSG_FORCING_NEWTON adds to Im eta and Im zeta at (0, kf, +-kf) as the
+ * Newton-solver build does (3D_NavierStokes/src_gmres/kernels.h:234-238) */
+#define PSG_FORCING_DNS 0
+#define PSG_FORCING_NEWTON 1
+int psg_ns3d_set_forcing_form(psg_ns3d* h, int form);
 int psg_ns3d_set_params(psg_ns3d* h, double nu, double ampfor, double kf, double ri,
                         double sc, double theta);
 int psg_ns3d_set_stream(psg_ns3d* h, void* cuda_stream);

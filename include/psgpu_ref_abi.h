@@ -1,6 +1,7 @@
 /*
  * psgpu_ref_abi.h -- the reference-compatible entry points of the drop-in
- * libraries libpsg_ns2d.so, libpsg_ns3d.so, libpsg_euler3d.so, libpsg_bous3d.so.
+ * libraries libpsg_ns2d.so, libpsg_ns3d.so, libpsg_ns3d_newton.so,
+ * libpsg_euler3d.so, libpsg_bous3d.so.
  *
  * psgpu's Fortran drivers call one C-ABI function per flavour with every
  * argument by pointer (Fortran by-reference ABI, no hidden lengths).  Each
@@ -8,7 +9,8 @@
  * lists, so a driver links against it unchanged.  Every flavour exports
  * timestep_cuda_, hence one library per flavour; define exactly one of
  * PSG_ABI_NS2D, PSG_ABI_NS3D, PSG_ABI_EULER3D, PSG_ABI_BOUS3D before including
- * this header to get that flavour's prototypes.
+ * this header to get that flavour's prototypes (PSG_ABI_NS3D_NEWTON for the
+ * Newton-solver build's 3D step).
  *
  * double2 is CUDA's vector type (two doubles: real, imaginary).
  */
@@ -49,6 +51,18 @@ void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* xir, doubl
                     int* ikN, int* LC, int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT,
                     int* NX, int* NY, int* NZ, int* NSTOP, int* NOUT, int* NOUTV,
                     int* statsFLAG, int* RecFLAG, int* RANK);
+#endif
+
+#if defined(PSG_ABI_NS3D_NEWTON) || defined(PSG_FLAVOUR_NS3D_NEWTON)
+/* 3D Navier-Stokes Heun / Crank-Nicolson as the Newton-solver build steps it
+ * (its own forcing form, no outputs besides the state); replaces
+ * 3D_NavierStokes/src_gmres/cuda.cu:10-28.  The reference fixes the grid in
+ * its kernels.h (128^3); libpsg_ns3d_newton.so uses 128 unless PSG_NEWTON_N is
+ * set in the environment. */
+void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* nuzn, double* nu1,
+                    double* kx, double* ky, double* kz, double* Time, double* TSTART,
+                    double* AMPFOR, double* DELT, int* KFY, double* V2, int* ikF, int* ikN,
+                    int* LC, int* NSTOP);
 #endif
 
 #if defined(PSG_ABI_EULER3D) || defined(PSG_FLAVOUR_EULER3D)

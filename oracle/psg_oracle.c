@@ -581,7 +581,21 @@ static inline void curl3d(double kx, double ky, double kz, cplx U, cplx V, cplx 
 /* 3D Navier-Stokes (DNS build) and Euler: Heun with/without CN             */
 /* ------------------------------------------------------------------------ */
 
-static int heun3d(int euler, double *xid, double *etd, double *ztd, double *phys,
+/* forcing of the Heun/CN flavours: form 0 as the DNS build applies it
+ * (3D_NavierStokes/src/kernels.h:342-343, 419-420), form 1 as the
+ * Newton-solver build does (3D_NavierStokes/src_gmres/kernels.h:234-238, 320-324) */
+static void heun_force(int form, double kx, double ky, double kz, double kfy, double ampfor,
+                       cplx *nx, cplx *ny, cplx *nz) {
+  if (form == 0) {
+    if (kx == 0.0 && kz == kfy && ky == kfy) *nx += ampfor;
+    if (kx == 0.0 && kz == -kfy && ky == kfy) *nx -= ampfor;
+  } else {
+    if (kx == 0.0 && kz == kfy && ky == kfy) { *ny += I * ampfor; *nz -= I * ampfor; }
+    if (kx == 0.0 && kz == -kfy && ky == kfy) { *ny += I * ampfor; *nz += I * ampfor; }
+  }
+}
+
+static int heun3d(int euler, int fform, double *xid, double *etd, double *ztd, double *phys,
                   const double *nuzn, const double *nu1, int n, double alpha,
                   double ampfor, double kfy, double dt, int nstop, double tstart,
                   double *time) {
@@ -616,8 +630,7 @@ static int heun3d(int euler, double *xid, double *etd, double *ztd, double *phys
       cplx nx, ny, nz;
       curl3d(kx, ky, kz, U[ik], V[ik], W[ik], &nx, &ny, &nz);
       if (!euler) {
-        if (kx == 0.0 && kz == kfy && ky == kfy) nx += ampfor;
-        if (kx == 0.0 && kz == -kfy && ky == kfy) nx -= ampfor;
+        heun_force(fform, kx, ky, kz, kfy, ampfor, &nx, &ny, &nz);
         double NUZN = nuzn[ik], NU1 = g->LL[ik] * nu1[ik];
         RX[ik] = nx; RY[ik] = ny; RZ[ik] = nz;
         nx = NU1 * (creal(xi[ik]) * NUZN + creal(nx)) + I * (NU1 * (NUZN * cimag(xi[ik]) + cimag(nx)));
@@ -651,8 +664,7 @@ static int heun3d(int euler, double *xid, double *etd, double *ztd, double *phys
       double NU2;
       if (!euler) {
         NU2 = 0.5 * nu1[ik];
-        if (kx == 0.0 && kz == kfy && ky == kfy) nx += ampfor;
-        if (kx == 0.0 && kz == -kfy && ky == kfy) nx -= ampfor;
+        heun_force(fform, kx, ky, kz, kfy, ampfor, &nx, &ny, &nz);
       } else {
         NU2 = 0.5 * dt;
       }
@@ -676,14 +688,23 @@ int orc_ns3d_timestep(double *xii, double *eta, double *zet, double *phys,
                       const double *nuzn, const double *nu1, int n, double alpha,
                       double ampfor, double kfy, double dt, int nstop,
                       double tstart, double *time) {
-  return heun3d(0, xii, eta, zet, phys, nuzn, nu1, n, alpha, ampfor, kfy, dt,
+  return heun3d(0, 0, xii, eta, zet, phys, nuzn, nu1, n, alpha, ampfor, kfy, dt,
                 nstop, tstart, time);
+}
+
+/* the Newton-solver build's step (3D_NavierStokes/src_gmres/cuda.cu:10-176):
+ * the same Heun/CN scheme with its own forcing form */
+int orc_ns3d_newton_timestep(double *xii, double *eta, double *zet, const double *nuzn,
+                             const double *nu1, int n, double alpha, double ampfor, double kfy,
+                             double dt, int nstop, double tstart, double *time) {
+  return heun3d(0, 1, xii, eta, zet, NULL, nuzn, nu1, n, alpha, ampfor, kfy, dt, nstop,
+                tstart, time);
 }
 
 int orc_euler3d_timestep(double *xii, double *eta, double *zet, double *phys,
                          int n, double alpha, double dt, int nstop,
                          double tstart, double *time) {
-  return heun3d(1, xii, eta, zet, phys, NULL, NULL, n, alpha, 0.0, 0.0, dt,
+  return heun3d(1, 0, xii, eta, zet, phys, NULL, NULL, n, alpha, 0.0, 0.0, dt,
                 nstop, tstart, time);
 }
 

@@ -49,6 +49,9 @@ int orc_ns2d_timederiv(const double *Z, double *dZ, int n, double alpha, double 
  *      (3D_NavierStokes/src/cuda.cu:18-151, kernels.h:113-464).  State xii,eta,zet
  *      complex128 [IKTZ][IKTY][IKTX] overwritten; phys (may be NULL) receives the
  *      three physical vorticity fields of the last predictor transform, n^3 each. */
+int orc_ns3d_newton_timestep(double *xii, double *eta, double *zet, const double *nuzn,
+                             const double *nu1, int n, double alpha, double ampfor, double kfy,
+                             double dt, int nstop, double tstart, double *time);
 int orc_ns3d_timestep(double *xii, double *eta, double *zet, double *phys,
                       const double *nuzn, const double *nu1,
                       int n, double alpha, double ampfor, double kfy,

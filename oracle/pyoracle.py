@@ -46,6 +46,8 @@ def lib():
         L.orc_ns2d_timederiv.restype = i
         L.orc_ns3d_timestep.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, i, d, d, d, d, i, d, _dp]
         L.orc_ns3d_timestep.restype = i
+        L.orc_ns3d_newton_timestep.argtypes = [_dp, _dp, _dp, _dp, _dp, i, d, d, d, d, i, d, _dp]
+        L.orc_ns3d_newton_timestep.restype = i
         L.orc_euler3d_timestep.argtypes = [_dp, _dp, _dp, _dp, i, d, d, i, d, _dp]
         L.orc_euler3d_timestep.restype = i
         L.orc_bous3d_timestep.argtypes = [_dp, _dp, _dp, _dp, i, d, d, d, d, d, d, d, d, d, d, _dp]
@@ -143,6 +145,19 @@ def ns3d_timestep(xii, eta, zet, n, nu, dt, nstop, ampfor=0.0, kfy=4.0, tstart=0
     if want_phys:
         out = out + (phys.reshape(3, n, n, n),)
     return out
+
+
+def ns3d_newton_timestep(xii, eta, zet, n, nu, dt, nstop, ampfor=0.0, kfy=4.0, tstart=0.0,
+                         alpha=1.0):
+    """the Newton-solver build's Heun/CN step (its own forcing form)"""
+    xii, eta, zet = _c(xii), _c(eta), _c(zet)
+    nuzn, nu1 = cn_coeffs3d(n, nu, dt, alpha)
+    t = np.zeros(1)
+    rc = lib().orc_ns3d_newton_timestep(_p(xii.view(np.float64)), _p(eta.view(np.float64)),
+                                        _p(zet.view(np.float64)), _p(nuzn), _p(nu1), n, alpha,
+                                        ampfor, kfy, dt, nstop, tstart, _p(t))
+    assert rc == 0
+    return xii, eta, zet, float(t[0])
 
 
 def euler3d_timestep(xii, eta, zet, n, dt, nstop, tstart=0.0, alpha=1.0, want_phys=False):

@@ -54,7 +54,7 @@ class TimestepLibrary:
     """One flavour's shared object exporting ``timestep_cuda_`` (and for the
     Boussinesq flavour ``timederiv_cuda_``)."""
 
-    FLAVOURS = ("ns2d", "ns3d", "euler3d", "bous3d")
+    FLAVOURS = ("ns2d", "ns3d", "ns3d_newton", "euler3d", "bous3d")
 
     def __init__(self, path: str, flavour: str):
         if flavour not in self.FLAVOURS:
@@ -120,6 +120,20 @@ class TimestepLibrary:
                     _i(g.kt), _i(g.nkt), _i(n), _i(n), _i(n), _i(nstop), _i(1),
                     _i(nstop + 1), _i(0), _i(0), _i(0))
         return xii, eta, zet, float(t[0]), phys.reshape(3, n, n, n)
+
+    def ns3d_newton(self, xii, eta, zet, n, nu, dt, nstop, ampfor=0.0, kf=4, tstart=0.0,
+                    alpha=1.0):
+        """3D NS Heun/CN as the Newton-solver build steps it (18 arguments; the grid
+        is the library's: 128 for the reference build, PSG_NEWTON_N for ours).
+        Returns (xii, eta, zet, time)."""
+        g, kx, ky, kz, LC, ikF, ikN = self._grid3(n, alpha)
+        xii, eta, zet = (_cplx(a, g.shape) for a in (xii, eta, zet))
+        nuzn, nu1 = g.cn_coeffs(nu, dt)
+        t = np.zeros(1)
+        self.fn(_pd(xii.view(np.float64)), _pd(eta.view(np.float64)), _pd(zet.view(np.float64)),
+                _pd(nuzn), _pd(nu1), _pd(kx), _pd(ky), _pd(kz), _pd(t), _d(tstart), _d(ampfor),
+                _d(dt), _i(int(kf)), _d(nu), _pi(ikF), _pi(ikN), _pi(LC), _i(nstop))
+        return xii, eta, zet, float(t[0])
 
     def euler3d(self, xii, eta, zet, n, dt, nstop, tstart=0.0, alpha=1.0, workdir=None):
         g, kx, ky, kz, LC, ikF, ikN = self._grid3(n, alpha)

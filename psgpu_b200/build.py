@@ -33,6 +33,7 @@ CORE = ["psg_api.cu", "psg_ns3d_api.cu", "psg_ns3d_f32.cu", "psg_ns3d_f64.cu",
 # drop-in libraries: name -> (source, macro)
 DROPINS = {
     "ns3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D"),
+    "ns3d_newton": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D_NEWTON"),
     "euler3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_EULER3D"),
     "bous3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_BOUS3D"),
     "ns2d": ("psg_dropin2d.cu", "PSG_FLAVOUR_NS2D"),

@@ -1,6 +1,7 @@
 // psg_dropin3d.cu -- reference-compatible timestep_cuda_ entry points (3D).
 //
-// Compiled once per flavour (-DPSG_FLAVOUR_NS3D / _EULER3D / _BOUS3D) into
+// Compiled once per flavour (-DPSG_FLAVOUR_NS3D / _NS3D_NEWTON / _EULER3D /
+// _BOUS3D) into
 // libpsg_<flavour>.so, because every flavour exports the same Fortran-mangled
 // symbol.  The argument lists are the reference's, all by pointer; the state
 // arrays are overwritten in place exactly as the reference does.  Unlike the
@@ -88,6 +89,32 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double*
   if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, 0.0, 1.0, 0.0) ||
       psg_ns3d_upload(h, in) || psg_ns3d_step(h, *DELT, *NSTOP, 1) || psg_ns3d_download(h, out) ||
       (*NSTOP > 0 && psg_ns3d_download_phys(h, phys))) {
+    report("timestep_cuda_");
+    return;
+  }
+  if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
+}
+
+#elif defined(PSG_FLAVOUR_NS3D_NEWTON)
+
+// The Newton-solver build's step (3D_NavierStokes/src_gmres/cuda.cu:10-176):
+// 18 arguments and no sizes -- the reference fixes the grid at compile time
+// in its kernels.h (128^3 as shipped).  The grid here is 128 unless
+// PSG_NEWTON_N in the environment names another supported size.
+extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* nuzn, double* nu1,
+                               double* kx, double* ky, double* kz, double* Time, double* TSTART,
+                               double* AMPFOR, double* DELT, int* KFY, double* V2, int* ikF,
+                               int* ikN, int* LC, int* NSTOP) {
+  (void)nuzn; (void)nu1; (void)kx; (void)ky; (void)kz; (void)ikF; (void)ikN; (void)LC;
+  int n = 128;
+  if (const char* e = getenv("PSG_NEWTON_N")) n = atoi(e);
+  psg_ns3d* h = engine(n, PSG_SCHEME_NS_HEUN);
+  if (!h) { report("timestep_cuda_"); return; }
+  const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
+  double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
+  if (psg_ns3d_set_forcing_form(h, PSG_FORCING_NEWTON) ||
+      psg_ns3d_set_params(h, *V2, *AMPFOR, (double)*KFY, 0.0, 1.0, 0.0) ||
+      psg_ns3d_upload(h, in) || psg_ns3d_step(h, *DELT, *NSTOP, 0) || psg_ns3d_download(h, out)) {
     report("timestep_cuda_");
     return;
   }

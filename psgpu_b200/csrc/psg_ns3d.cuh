@@ -54,6 +54,7 @@ struct StepParams {
   T nu;      // viscosity (1/Re)
   T ampfor;  // forcing amplitude (the reference's d_AMPFOR)
   T kf;      // forcing wavenumber
+  int fform; // Heun/CN forcing: 0 as the DNS build applies it, 1 as the Newton-solver build
   T ri, sc, sinth, costh;  // Boussinesq parameters
 };
 
@@ -75,6 +76,7 @@ struct Engine3DBase {
   virtual int upload_device(const void* const* comps) = 0;
   virtual int download_device(void* const* comps) = 0;
   virtual int energetics(double* out) = 0;
+  virtual int set_forcing_form(int form) = 0;
   virtual int linear(int mode, double dt, const void* const* in, void* const* out) = 0;
   virtual int steps(double dt, int nsteps, int dump_last) = 0;
   virtual int timederiv(double* const* out) = 0;

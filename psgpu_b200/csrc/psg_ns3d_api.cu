@@ -146,3 +146,8 @@ extern "C" int psg_ns3d_linear(psg_ns3d* h, int mode, double dt, void* const* in
   if (!in || !out) { psg_set_error("null vector"); return PSG_ERR_ARG; }
   return h->e->linear(mode, dt, (const void* const*)in, out);
 }
+
+extern "C" int psg_ns3d_set_forcing_form(psg_ns3d* h, int form) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->set_forcing_form(form);
+}

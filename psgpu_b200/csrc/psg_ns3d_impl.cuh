@@ -561,8 +561,13 @@ __device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R
     cpx<T>* H0 = R.K1.c[0]; cpx<T>* H1 = R.K1.c[1]; cpx<T>* H2 = R.K1.c[2];
     const cpx<T> s0 = S0[ik], s1 = S1[ik], s2 = S2[ik];
     if (SCHEME == SCHEME_NS_HEUN) {
-      if (kx == (T)0 && kz == p.kf && ky == p.kf) xiX += p.ampfor;
-      if (kx == (T)0 && kz == -p.kf && ky == p.kf) xiX -= p.ampfor;
+      if (p.fform == 0) {  // 3D_NavierStokes/src/kernels.h:342-343, 419-420
+        if (kx == (T)0 && kz == p.kf && ky == p.kf) xiX += p.ampfor;
+        if (kx == (T)0 && kz == -p.kf && ky == p.kf) xiX -= p.ampfor;
+      } else if (kx == (T)0 && ky == p.kf) {  // 3D_NavierStokes/src_gmres/kernels.h:234-238, 320-324
+        if (kz == p.kf) { etY += p.ampfor; ztY -= p.ampfor; }
+        if (kz == -p.kf) { etY += p.ampfor; ztY += p.ampfor; }
+      }
       // nuzn = (1 - nu k^2 dt/2)/dt, nu1 = dt/(1 + nu k^2 dt/2) (3D_NavierStokes/src/init.F90:194-198)
       const T NU = p.nu * wk;
       const T nuzn = LL * (((T)1 - (T)0.5 * NU * p.dt) / p.dt);
@@ -1764,6 +1769,12 @@ struct Engine3D final : Engine3DBase {
       box_to_ref<T><<<592, 256, 0, stream>>>(g, res.c[q], (double2*)out[q], nullptr);
     launches += 3;
     PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  int set_forcing_form(int form) override {
+    if (form != 0 && form != 1) { psg_set_error("forcing form %d unknown", form); return PSG_ERR_ARG; }
+    prm.fform = form;
     return PSG_OK;
   }
 
