@@ -6,6 +6,7 @@ Produces (git-ignored, shipped with the tree):
   psgpu_b200/lib/libpsgpu.so          engines + re-entrant C API (include/psgpu.h)
   psgpu_b200/lib/libpsg_<flavour>.so  reference-compatible timestep_cuda_ drop-ins
                                       (include/psgpu_ref_abi.h), linked to libpsgpu.so
+  psgpu_b200/bin/psg_dns3             3D Navier-Stokes DNS driver (include/psgpu_host.h)
 Objects are rebuilt only when a source or header is newer.
 """
 from __future__ import annotations
@@ -18,6 +19,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+HOST = os.path.join(HERE, "host")
+BIN = os.path.join(HERE, "bin")
+CC = os.environ.get("CC", "gcc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
@@ -30,6 +34,10 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 # translation units of libpsgpu.so
 CORE = ["psg_api.cu", "psg_ns3d_api.cu", "psg_ns3d_f32.cu", "psg_ns3d_f64.cu",
         "psg_ns2d.cu", "psg_newton2d.cu"]
+# host-side C of libpsgpu.so (parameter files, random starts, record I/O)
+HOST_SRC = ["psg_host.c"]
+# driver programs: name -> source (linked to libpsgpu.so)
+DRIVERS = {"psg_dns3": "psg_dns3.c"}
 # drop-in libraries: name -> (source, macro)
 DROPINS = {
     "ns3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D"),
@@ -42,6 +50,7 @@ DROPINS = {
 
 def _headers():
     hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    hs += glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "host", "*.h"))
     hs += glob.glob(os.path.join(INCLUDE, "*.h"))
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
@@ -69,9 +78,19 @@ def _compile(src, obj, defines=()):
     return obj
 
 
+def _compile_c(src, obj):
+    srcp = os.path.join(HOST, src)
+    if not _stale(obj, [srcp]):
+        return obj
+    _run([CC, "-std=c11", "-O2", "-fPIC", "-Wall", "-D_POSIX_C_SOURCE=200809L", f"-I{INCLUDE}",
+          "-c", srcp, "-o", obj])
+    return obj
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB, exist_ok=True)
+    os.makedirs(BIN, exist_ok=True)
     jobs = []
     core = [s for s in CORE if os.path.exists(os.path.join(CSRC, s))]
     dropins = {k: v for k, v in DROPINS.items() if os.path.exists(os.path.join(CSRC, v[0]))}
@@ -80,9 +99,12 @@ def build(verbose: bool = False) -> str:
             jobs.append(ex.submit(_compile, s, os.path.join(OBJ, s.replace(".cu", ".o"))))
         for name, (s, macro) in dropins.items():
             jobs.append(ex.submit(_compile, s, os.path.join(OBJ, f"dropin_{name}.o"), (macro,)))
+        for s in HOST_SRC:
+            jobs.append(ex.submit(_compile_c, s, os.path.join(OBJ, s.replace(".c", ".o"))))
         for j in jobs:
             j.result()
     core_objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in core]
+    core_objs += [os.path.join(OBJ, s.replace(".c", ".o")) for s in HOST_SRC]
     libcore = os.path.join(LIB, "libpsgpu.so")
     if _stale(libcore, core_objs):
         _run([NVCC, *ARCH, "-shared", "-o", libcore, *core_objs, "-lcudart"])
@@ -92,6 +114,12 @@ def build(verbose: bool = False) -> str:
         if _stale(out, [obj, libcore]):
             _run([NVCC, *ARCH, "-shared", "-o", out, obj, f"-L{LIB}", "-lpsgpu", "-lcudart",
                   "-Xlinker", "-rpath,$ORIGIN"])
+    for name, src in DRIVERS.items():
+        srcp = os.path.join(HOST, src)
+        out = os.path.join(BIN, name)
+        if _stale(out, [srcp, libcore]):
+            _run([CC, "-std=c11", "-O2", "-Wall", "-D_POSIX_C_SOURCE=200809L", f"-I{INCLUDE}", srcp,
+                  "-o", out, f"-L{LIB}", "-lpsgpu", "-Wl,-rpath,$ORIGIN/../lib", "-lm"])
     if verbose:
         print("built", libcore)
     return libcore

@@ -1,0 +1,121 @@
+/* psg_dns3 -- 3D Navier-Stokes DNS driver on psgpu_b200, in place of the
+ * reference's Fortran front end (3D_NavierStokes/src/main.F90).
+ *
+ *   psg_dns3 [-n N] [-d JOBDIR] [-p 32|64]
+ *
+ * Reads JOBDIR/params.txt (JOBDIR defaults to JOB<rank>, the rank taken from
+ * the MPI launcher's environment, as main.F90:38 names it), builds the random
+ * start (or reads the restart file named there), integrates NSTOP Heun /
+ * Crank-Nicolson steps with the DNS forcing, writes JOBDIR/stats.dat and
+ * JOBDIR/engy.dat every NOUT steps as the reference's statistics do
+ * (3D_NavierStokes/src/cuda.cu:116-140), and JOBDIR/Zk.out: main.F90's header
+ * record (1, IKTX, IKTY, IKTZ) followed by the final state as a type "D"
+ * restart record.  The grid is compile-time in the reference
+ * (global_params.F90, 128^3); here it is -n (default 128). */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "psgpu.h"
+#include "psgpu_host.h"
+
+static int env_rank(void) {
+  const char* names[] = {"OMPI_COMM_WORLD_RANK", "PMI_RANK", "RANK"};
+  for (int i = 0; i < 3; ++i) {
+    const char* v = getenv(names[i]);
+    if (v) return atoi(v);
+  }
+  return 0;
+}
+
+static double now(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+#define FAIL(...) do { fprintf(stderr, "psg_dns3: " __VA_ARGS__); fprintf(stderr, "\n"); return 1; } while (0)
+
+int main(int argc, char** argv) {
+  int n = 128, prec = 32;
+  char dir[512];
+  snprintf(dir, sizeof dir, "JOB%d", env_rank());
+  for (int i = 1; i < argc; ++i) {
+    if (!strcmp(argv[i], "-n") && i + 1 < argc) n = atoi(argv[++i]);
+    else if (!strcmp(argv[i], "-d") && i + 1 < argc) snprintf(dir, sizeof dir, "%s", argv[++i]);
+    else if (!strcmp(argv[i], "-p") && i + 1 < argc) prec = atoi(argv[++i]);
+    else FAIL("usage: psg_dns3 [-n N] [-d JOBDIR] [-p 32|64]");
+  }
+  char path[1024];
+  psg_params3d P;
+  snprintf(path, sizeof path, "%s/params.txt", dir);
+  if (psg_read_params3d(path, &P)) FAIL("%s", psg_last_error());
+  const int K = n / 3;
+  const long nkt = (long)(K + 1) * (2 * K + 1) * (2 * K + 1);
+  double* st[3];
+  for (int q = 0; q < 3; ++q)
+    if (!(st[q] = (double*)calloc(2 * nkt, sizeof(double)))) FAIL("out of host memory");
+  double meta[7] = {0};
+  if (P.irest == 0) {
+    if (psg_ic_random3d(n, P.iseed, P.ampv, st[0], st[1], st[2])) FAIL("%s", psg_last_error());
+  } else {
+    snprintf(path, sizeof path, "%s/%s", dir, P.infile);
+    if (psg_read_state3d(path, P.infile_type, P.irest, n, meta, st[0], st[1], st[2]))
+      FAIL("%s", psg_last_error());
+    if (P.infile_type[0] == 'A' || P.infile_type[0] == 'D') P.v2 = meta[1];
+  }
+  if (P.upoflag == 1) P.tstep = meta[2];  /* main.F90:68-77 */
+  P.nstop = (int)(P.tstep / P.delt);
+  printf("        Re= %g\n          NSTOP= %d\n          NOUT= %d\n          NOUTV= %d\n",
+         1.0 / P.v2, P.nstop, P.nout, P.noutv);
+
+  psg_ns3d* h = NULL;
+  if (psg_ns3d_create(&h, n, 1.0, PSG_SCHEME_NS_HEUN, prec) ||
+      psg_ns3d_set_params(h, P.v2, P.ampfor, (double)P.kf, 0.0, 1.0, 0.0))
+    FAIL("%s", psg_last_error());
+  const double* in[3] = {st[0], st[1], st[2]};
+  double* out[3] = {st[0], st[1], st[2]};
+  if (psg_ns3d_upload(h, in)) FAIL("%s", psg_last_error());
+
+  FILE *fs = NULL, *fe = NULL;
+  psg_stats3d* S = NULL;
+  if (P.statsflag) {
+    snprintf(path, sizeof path, "%s/stats.dat", dir);
+    fs = fopen(path, "w");
+    snprintf(path, sizeof path, "%s/engy.dat", dir);
+    fe = fopen(path, "w");
+    S = psg_stats3d_create(n, P.v2, P.ampfor, P.kf);
+    if (!fs || !fe || !S) FAIL("cannot open the statistics files in %s", dir);
+  }
+  const double t0 = now();
+  int done = 0;
+  /* statistics after step NT for NT = NOUT, 2 NOUT, ... (NT counted from 0) */
+  for (int nt = P.nout; nt < P.nstop && S; nt += P.nout) {
+    if (psg_ns3d_step(h, P.delt, nt + 1 - done, 0)) FAIL("%s", psg_last_error());
+    done = nt + 1;
+    const double tme = done * P.delt;
+    if (P.statsflag == 2 && tme <= 500.0) continue;
+    if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
+    psg_stats3d_add(S, tme, st[0], st[1], st[2], fs, fe);
+  }
+  if (done < P.nstop && psg_ns3d_step(h, P.delt, P.nstop - done, 0)) FAIL("%s", psg_last_error());
+  if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
+  const double el = now() - t0;
+
+  snprintf(path, sizeof path, "%s/Zk.out", dir);
+  FILE* fz = fopen(path, "wb");
+  if (!fz) FAIL("cannot write %s", path);
+  const double rec[7] = {P.nstop * P.delt, P.v2, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (psg_write_state3d_header(fz, 1, n) || psg_write_state3d_record(fz, n, rec, st[0], st[1], st[2]))
+    FAIL("writing %s failed", path);
+  fclose(fz);
+  if (fs) fclose(fs);
+  if (fe) fclose(fe);
+  psg_stats3d_destroy(S);
+  psg_ns3d_destroy(h);
+  printf("time stepping done: %d steps in %.3f s (%.1f steps/s)\n", P.nstop, el,
+         el > 0 ? P.nstop / el : 0.0);
+  for (int q = 0; q < 3; ++q) free(st[q]);
+  return 0;
+}

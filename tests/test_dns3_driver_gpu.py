@@ -1,0 +1,41 @@
+"""The C DNS driver psg_dns3 (params.txt -> random start -> Heun/CN steps ->
+stats.dat / engy.dat / Zk.out) against the same integration through the
+Python binding of the engine, FP64, 32^3."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import psgpu_b200 as P
+from psgpu_b200 import host as H
+from tests.test_host_cpu import _params_text
+
+pytestmark = pytest.mark.gpu
+
+
+def test_dns3_driver(tmp_path):
+    job = tmp_path / "JOB0"
+    job.mkdir()
+    (job / "params.txt").write_text(_params_text(TSTEP="0.1", outfreq1="0.02", DELT="0.01"))
+    r = subprocess.run([H.driver_path(), "-n", "32", "-d", str(job), "-p", "64"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    n, nu, dt = 32, 1 / 20.0, 0.01
+    # statistics after steps 3, 5, 7, 9 (NT = 2, 4, 6, 8 counted from 0)
+    rows = np.loadtxt(job / "stats.dat", ndmin=2)
+    assert rows.shape == (4, 6)
+    np.testing.assert_allclose(rows[:, 0], [0.03, 0.05, 0.07, 0.09], rtol=1e-6)
+    assert np.loadtxt(job / "engy.dat", ndmin=2).shape == (4, 7)
+    ic = H.ic_random3d(n, 837920, 1.0)
+    eng = P.NS3D(n, P.SCHEME_NS_HEUN, precision=64, nu=nu, ampfor=-4.0, kf=4.0)
+    eng.upload(*ic)
+    eng.step(dt, 3)
+    e, _, _ = eng.energetics()
+    assert rows[0, 1] == pytest.approx(e, rel=1e-6)  # %e keeps 7 digits
+    eng.step(dt, 7)
+    ref = eng.download()
+    meta, *st = H.read_state3d(str(job / "Zk.out"), "D", 1, n)
+    assert meta[0] == pytest.approx(10 * dt) and meta[1] == pytest.approx(nu)
+    for a, b in zip(st, ref):
+        np.testing.assert_array_equal(a, b)
