@@ -113,7 +113,7 @@ __device__ __forceinline__ cpx<T> spec_op(int op, int comp, const cpx<T>* x, T k
 }
 
 template <typename T, int N, int NC, int NF, int MODE = 0>
-__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G)
+__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, 3)
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
        int mask_vel, int* status, Fields4<T> in2 = Fields4<T>{}, int ops = 0) {
   using F = LineFFT<N, +1, T>;
