@@ -697,6 +697,45 @@ def run_adjoint(args):
             errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
             scale = float(g64.abs().pow(2).sum().sqrt() * v.abs().pow(2).sum().sqrt())
             nerrs.append(abs(ad - fd) / scale)
+    # Boussinesq variant: N = 1 (Ri = 1), Pr = 1 (Sc = 1), gravity along z
+    rng = np.random.default_rng(2025)
+    r0 = torch.tensor((rng.standard_normal(sp.grid.shape) + 1j * rng.standard_normal(sp.grid.shape))
+                      * sp.grid.mask() * 1e-3, dtype=torch.complex128, device="cuda")
+    beng = P.NS3D(n, P.SCHEME_BOUS_RK4, precision=64, nu=nu, ri=1.0, sc=1.0, theta=np.pi / 2)
+
+    def bloss(u, r):
+        s0 = torch.cat([sp.curl(u), r[None]], 0)
+        return sp.energy(sp.velocity(trajectory(s0, beng, dt, steps, every)[:3]))
+
+    u = u0.clone().requires_grad_(True)
+    r = r0.clone().requires_grad_(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = bloss(u, r)
+    L.backward()
+    torch.cuda.synchronize()
+    bsec = time.perf_counter() - t0
+    berrs, bnerrs = [], []
+    with torch.no_grad():
+        for d in range(min(4, args.adjoint_dirs)):
+            vu = sp.random_velocity(8000 + d, energy=1.0)
+            vr = torch.tensor(np.random.default_rng(8100 + d).standard_normal(sp.grid.shape) *
+                              sp.grid.mask() * 1e-2, dtype=torch.complex128, device="cuda")
+            fd = (float(bloss(u0 + eps * vu, r0 + eps * vr)) -
+                  float(bloss(u0 - eps * vu, r0 - eps * vr))) / (2 * eps)
+            ad = float((u.grad.real * vu.real + u.grad.imag * vu.imag).sum() +
+                       (r.grad.real * vr.real + r.grad.imag * vr.imag).sum())
+            berrs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+            gn = float((u.grad.abs().pow(2).sum() + r.grad.abs().pow(2).sum()).sqrt())
+            vn = float((vu.abs().pow(2).sum() + vr.abs().pow(2).sum()).sqrt())
+            bnerrs.append(abs(ad - fd) / (gn * vn))
+    out["boussinesq"] = {"workload": "Ri=1, Sc=1, gravity along z, rho0 seeded 1e-3; "
+                                     "L = terminal kinetic energy; gradient w.r.t. (u0, rho0)",
+                         "fp64_gradient_s": round(bsec, 3), "loss": float(L.detach()),
+                         "fd_directions": len(berrs),
+                         "fp64_adjoint_vs_central_fd_max_rel": float(max(berrs)) if berrs else None,
+                         "fp64_adjoint_vs_central_fd_max_normalised":
+                             float(max(bnerrs)) if bnerrs else None}
     out["fd_directions"] = args.adjoint_dirs
     out["fd_eps"] = eps
     out["fp64_adjoint_vs_central_fd_max_rel"] = float(max(errs)) if errs else None

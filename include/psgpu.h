@@ -100,16 +100,19 @@ int psg_ns3d_download_device(psg_ns3d* h, void* const* comps);
  * out[2] = sum |rho|^2 (Boussinesq; 0 otherwise) */
 int psg_ns3d_energetics(psg_ns3d* h, double* out);
 
-/* Tangent-linear and adjoint of the RK4/CN step (PSG_SCHEME_NS_RK4), exact to
+/* Tangent-linear and adjoint of the RK4/CN step (PSG_SCHEME_NS_RK4, and
+ * PSG_SCHEME_BOUS_RK4 with the density as a fourth component), exact to
  * round-off for the discrete step (one RK4/CN step with the stage state
- * reset to the state, as after an upload).  in / out: 3 device arrays each,
- * FP64 complex boxes in the reference layout; in == out is allowed.
+ * reset to the state, as after an upload).  in / out: 3 (4) device arrays
+ * each, FP64 complex boxes in the reference layout; in == out is allowed.
  *   PSG_LIN_TANGENT_STEP   out = dPhi_dt(S) in,     then S = Phi_dt(S)
  *   PSG_LIN_ADJOINT_STEP   out = dPhi_dt(S)^T in,   then S = Phi_dt(S)
  *   PSG_LIN_TANGENT_RHS    out = N'(S) in           (S unchanged, dt unused)
  *   PSG_LIN_ADJOINT_RHS    out = N'(S)^T in
- * where N(w) = curl F(u x w) is the nonlinear term and the transpose is
- * taken in the real inner product of the stored coefficients. */
+ * where N is the right-hand side without viscosity (N(w) = curl F(u x w);
+ * Boussinesq: also buoyancy, -F(u.grad rho) and the stratification term) and
+ * the transpose is taken in the real inner product of the stored
+ * coefficients. */
 #define PSG_LIN_TANGENT_STEP 0
 #define PSG_LIN_ADJOINT_STEP 1
 #define PSG_LIN_TANGENT_RHS 2

@@ -214,17 +214,19 @@ class NS3D:
 
     def linear(self, mode: int, x, dt: float = 0.0, out=None):
         """Tangent / adjoint step or right-hand side (see psg_ns3d_linear) applied to
-        x, a torch CUDA complex128 tensor of shape (3, IKTZ, IKTY, IKTX) in the
-        reference layout; returns `out` (a new tensor unless given).  Ordered on
-        the engine's stream (set_stream) -- the caller synchronises."""
+        x, a torch CUDA complex128 tensor of shape (ncomp, IKTZ, IKTY, IKTX) in the
+        reference layout (ncomp = 3, or 4 with the density); returns `out` (a new
+        tensor unless given).  Ordered on the engine's stream (set_stream) -- the
+        caller synchronises."""
         import torch
-        if x.dtype != torch.complex128 or not x.is_cuda or x.shape[0] != 3:
-            raise ValueError("x must be a CUDA complex128 tensor of 3 components")
+        nc = self.ncomp
+        if x.dtype != torch.complex128 or not x.is_cuda or x.shape[0] != nc:
+            raise ValueError(f"x must be a CUDA complex128 tensor of {nc} components")
         x = x.contiguous()
         if out is None:
             out = torch.empty_like(x)
-        ip = (C.c_void_p * 3)(*[x[q].data_ptr() for q in range(3)])
-        op = (C.c_void_p * 3)(*[out[q].data_ptr() for q in range(3)])
+        ip = (C.c_void_p * nc)(*[x[q].data_ptr() for q in range(nc)])
+        op = (C.c_void_p * nc)(*[out[q].data_ptr() for q in range(nc)])
         _check(lib().psg_ns3d_linear(self._h, mode, dt, ip, op))
         return out
 

@@ -21,7 +21,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import NS3D, SCHEME_NS_RK4
+from . import NS3D, SCHEME_BOUS_RK4, SCHEME_NS_RK4
 from .fields import Grid3D
 
 
@@ -72,10 +72,13 @@ class _Trajectory(torch.autograd.Function):
 
 
 def trajectory(w0: torch.Tensor, engine: NS3D, dt: float, nsteps: int, every: int = 20):
-    """Vorticity after `nsteps` RK4/CN steps from w0 (CUDA complex128, shape
-    (3, IKTZ, IKTY, IKTX)), differentiable with respect to w0."""
-    if engine.scheme != SCHEME_NS_RK4:
-        raise ValueError("the differentiable trajectory needs the RK4/CN scheme")
+    """State after `nsteps` RK4/CN steps from w0 (CUDA complex128, shape
+    (ncomp, IKTZ, IKTY, IKTX): the vorticity, and the density for the
+    Boussinesq scheme), differentiable with respect to w0."""
+    if engine.scheme not in (SCHEME_NS_RK4, SCHEME_BOUS_RK4):
+        raise ValueError("the differentiable trajectory needs an RK4/CN scheme")
+    if w0.shape[0] != engine.ncomp:
+        raise ValueError(f"the engine's state has {engine.ncomp} components")
     return _Trajectory.apply(w0, engine, float(dt), int(nsteps), int(every))
 
 

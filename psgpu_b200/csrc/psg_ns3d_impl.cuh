@@ -98,6 +98,8 @@ __device__ __forceinline__ bool tile_wait(uint64_t* bar, int* s_ok, int* status)
 // the w slots 0-2 that pass C reads as w) and a = in2 (the u slots 3-5), each
 // passed through the spectral operator of `ops` (bits 0-3 for b, 4-7 for a:
 // OP_ID, OP_CURL = i k x, OP_BS = i k x / k^2) and masked to the kept modes.
+// MODE 2 (scale): the fields of the Boussinesq adjoint's scalar products,
+// [psi, i k rho, B w] from psi = in2.c[0] and (w, rho) = in.c[0..3].
 // ---------------------------------------------------------------------------
 enum SpecOp : int { OP_ID = 0, OP_CURL = 1, OP_BS = 2 };
 
@@ -139,6 +141,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   __syncthreads();
   auto src_comp = [&](int q) -> const cpx<T>* {
     if (MODE == 1 && q >= 3) return in2.c[q - 3];
+    if (MODE == 2 && q == 4) return in2.c[0];
     return in.c[q];
   };
   if (tid == 0) {
@@ -196,6 +199,25 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
           const T kz = (T)(ikz - K);
           const T wki = wkinv(kx * kx + ky * ky + kz * kz);
           r = spec_op<T>((ops >> (4 * sl)) & 15, comp, x, kx, ky, kz, wki);
+        }
+      } else if (MODE == 2) {
+        if (ikz >= 0 && live_col && live_f && s_ll[ikz * W + c]) {
+          auto fetch = [&](int q) -> cpx<T> {
+            if (mcol && !(iky == K && ikz > K)) return cconj(s_mir[q * Y + ikz]);
+            if (mcol) return s_in[q * Y * W + ikz * W];
+            return s_in[q * Y * W + ikz * W + c];
+          };
+          const T kz = (T)(ikz - K);
+          if (f == 0) {
+            r = fetch(4);
+          } else if (f <= 3) {  // i k_j rho
+            const cpx<T> rho = fetch(3);
+            const T kk = (f == 1) ? kx : (f == 2) ? ky : kz;
+            r = cpx<T>{-kk * rho.y, kk * rho.x};
+          } else {
+            const cpx<T> x[3] = {fetch(0), fetch(1), fetch(2)};
+            r = spec_op<T>(OP_BS, f - 4, x, kx, ky, kz, wkinv(kx * kx + ky * ky + kz * kz));
+          }
         }
       } else if (ikz >= 0 && live_col && live_f) {
         cpx<T> xi, et, zt, rho;
@@ -416,6 +438,30 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     const int z = (int)(row / N), y = (int)(row % N);
     const cpx<T>* src = s_buf + b * tile_words + lr * XP;
     const int fs = L * XP;  // field stride in shared memory
+    cpx<T>* dst = out + ((long)z * N + y) * kTileW;
+    const cpx<T>* two = s_tw + N;  // swapped plan for the forward transforms
+    if (NF == 7) {
+      // scalar products of the Boussinesq adjoint: psi * (i k rho), psi * u
+      T ps[E], ga[E], gb[E], p0[E], p1[E], p2[E];
+      R::c2r_pair(src, src + fs, K, gi, s_tw, ex, ps, ga);
+#pragma unroll
+      for (int e = 0; e < E; ++e) p0[e] = ps[e] * ga[e] * scale;
+      R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, ga, gb);
+#pragma unroll
+      for (int e = 0; e < E; ++e) { p1[e] = ps[e] * ga[e] * scale; p2[e] = ps[e] * gb[e] * scale; }
+      R::r2c_pair(p0, p1, K, XP, gi, two, ex, dst, dst + fstride, tstride);
+      R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, ga, gb);
+#pragma unroll
+      for (int e = 0; e < E; ++e) { p0[e] = ps[e] * ga[e] * scale; p1[e] = ps[e] * gb[e] * scale; }
+      R::r2c_pair(p2, p0, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
+      R::c2r_pair(src + 6 * fs, nullptr, K, gi, s_tw, ex, ga, gb);
+#pragma unroll
+      for (int e = 0; e < E; ++e) p2[e] = ps[e] * ga[e] * scale;
+      R::r2c_pair(p1, p2, K, XP, gi, two, ex, dst + 4 * fstride, dst + 5 * fstride, tstride);
+      __syncthreads();  // release buffer b
+      if (ST == 1 && tid == 0 && tn < ntiles) issue(tn, 0);
+      continue;
+    }
     T xi[E], et[E], zt[E], u[E], v[E], w[E];
     R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
     R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
@@ -439,8 +485,6 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
       n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
       n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
     }
-    cpx<T>* dst = out + ((long)z * N + y) * kTileW;
-    const cpx<T>* two = s_tw + N;  // swapped plan for the forward transforms
     if (!BOUS) {
       R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
       R::r2c_pair(n3, nullptr, K, XP, gi, two, ex, dst + 2 * fstride, nullptr, tstride);
@@ -795,11 +839,14 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
     const cpx<T> V = s_in[(1 * N + ikz) * W + cc];
     const cpx<T> Wv = s_in[(2 * N + ikz) * W + cc];
     const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + ikz) * W + cc] : czero<T>();
-    if (SCHEME == SCHEME_RAW) {
+    if (SCHEME == SCHEME_RAW) {  // outputs 0-3 to K1, 4-5 to K2
       const T LL = keep_mode<T>(ikx, iy, iz, g.K, g.alpha) ? (T)1 : (T)0;
-      R.K1.c[0][ik] = cpx<T>{LL * U.x, LL * U.y};
-      R.K1.c[1][ik] = cpx<T>{LL * V.x, LL * V.y};
-      R.K1.c[2][ik] = cpx<T>{LL * Wv.x, LL * Wv.y};
+#pragma unroll
+      for (int q = 0; q < NO; ++q) {
+        const cpx<T> a = s_in[(q * N + ikz) * W + cc];
+        cpx<T>* o = (q < 4) ? R.K1.c[q] : R.K2.c[q - 4];
+        o[ik] = cpx<T>{LL * a.x, LL * a.y};
+      }
       continue;
     }
     // curl of F(-(u x w)) as preStep/corStep form it (3D_NavierStokes/src/kernels.h:327-334)
@@ -1002,16 +1049,20 @@ __global__ void lin_combine(Geom3<T> g, int adjoint, Fields4<T> Pa, Fields4<T> P
 template <typename T>
 __device__ __forceinline__ T stage_e(T q, T nk) { return (T)2 * q * nk / ((T)1 + q * nk); }
 
+// component c's viscous factor nu k^2 dt (the density's divided by Sc)
+template <typename T>
+__device__ __forceinline__ T comp_nk(T nk, int c, T sc) { return c == 3 ? nk / sc : nk; }
+
 // tangent stage: K = dt LL n, Z = (1 - e)(D + fr K)
 template <typename T>
 __global__ void tan_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> n, Fields4<T> D,
-                          Fields4<T> Kout, Fields4<T> Zout, long len) {
+                          Fields4<T> Kout, Fields4<T> Zout, long len, int nc, T sc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x) {
     const TileMode<T> m = tile_mode(g, i);
     const T LL = m.keep ? (T)1 : (T)0;
-    const T e = stage_e(q, dt * nu * m.wk);
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < nc; ++c) {
+      const T e = stage_e(q, comp_nk(dt * nu * m.wk, c, sc));
       const cpx<T> nn = n.c[c][i], d = D.c[c][i];
       const cpx<T> k = cpx<T>{dt * LL * nn.x, dt * LL * nn.y};
       const cpx<T> v = cpx<T>{d.x + fr * k.x, d.y + fr * k.y};
@@ -1022,8 +1073,8 @@ __global__ void tan_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> n, Field
 }
 
 // divergence removal of scheme_point's final stage, o - k (k.o) / k^2
-template <typename T>
-__device__ __forceinline__ void remove_div(const TileMode<T>& m, cpx<T> (&o)[3]) {
+template <typename T, int M>
+__device__ __forceinline__ void remove_div(const TileMode<T>& m, cpx<T> (&o)[M]) {
   const T wki = wkinv(m.wk);
   const T pr = (m.kx * o[0].x + m.ky * o[1].x + m.kz * o[2].x) * wki;
   const T pi = (m.kx * o[0].y + m.ky * o[1].y + m.kz * o[2].y) * wki;
@@ -1036,23 +1087,23 @@ __device__ __forceinline__ void remove_div(const TileMode<T>& m, cpx<T> (&o)[3])
 // D' = Pdiv LL [(1 - eS) D + (1 - eI)(K1/6 + dt n/6 + (K2 + K3)/3)]
 template <typename T>
 __global__ void tan_final(Geom3<T> g, T dt, T nu, Fields4<T> n, Fields4<T> K1, Fields4<T> K2,
-                          Fields4<T> K3, Fields4<T> D, long len) {
+                          Fields4<T> K3, Fields4<T> D, long len, int nc, T sc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x) {
     const TileMode<T> m = tile_mode(g, i);
     const T LL = m.keep ? (T)1 : (T)0;
-    const T nk = dt * nu * m.wk, hn = (T)0.5 * nk;
-    const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
     const T sixth = (T)(1.0 / 6.0), third = (T)(1.0 / 3.0);
-    cpx<T> o[3];
-    for (int c = 0; c < 3; ++c) {
+    cpx<T> o[4];
+    for (int c = 0; c < nc; ++c) {
+      const T nk = comp_nk(dt * nu * m.wk, c, sc), hn = (T)0.5 * nk;
+      const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
       const cpx<T> d = D.c[c][i], a = K1.c[c][i], b = K2.c[c][i], k3 = K3.c[c][i], nn = n.c[c][i];
       const T ix = sixth * (a.x + dt * nn.x) + third * (b.x + k3.x);
       const T iy = sixth * (a.y + dt * nn.y) + third * (b.y + k3.y);
       o[c] = cpx<T>{LL * ((d.x - eS * d.x) + (ix - eI * ix)), LL * ((d.y - eS * d.y) + (iy - eI * iy))};
     }
     remove_div(m, o);
-    for (int c = 0; c < 3; ++c) D.c[c][i] = o[c];
+    for (int c = 0; c < nc; ++c) D.c[c][i] = o[c];
   }
 }
 
@@ -1060,17 +1111,17 @@ __global__ void tan_final(Geom3<T> g, T dt, T nu, Fields4<T> n, Fields4<T> K1, F
 // Lk1 = b/6, Lk2 = Lk3 = b/3, Ln = dt b/6
 template <typename T>
 __global__ void adj_final(Geom3<T> g, T dt, T nu, Fields4<T> Lin, Fields4<T> Lz, Fields4<T> Lk1,
-                          Fields4<T> Lk2, Fields4<T> Lk3, Fields4<T> Ln, long len) {
+                          Fields4<T> Lk2, Fields4<T> Lk3, Fields4<T> Ln, long len, int nc, T sc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x) {
     const TileMode<T> m = tile_mode(g, i);
     const T LL = m.keep ? (T)1 : (T)0;
-    const T nk = dt * nu * m.wk, hn = (T)0.5 * nk;
-    const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
-    cpx<T> a[3];
-    load3(Lin, i, a);
+    cpx<T> a[4];
+    for (int c = 0; c < nc; ++c) a[c] = Lin.c[c][i];
     remove_div(m, a);
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < nc; ++c) {
+      const T nk = comp_nk(dt * nu * m.wk, c, sc), hn = (T)0.5 * nk;
+      const T eS = nk / ((T)1 + hn), eI = hn / ((T)1 + hn);
       const cpx<T> x = cpx<T>{LL * a[c].x, LL * a[c].y};
       const cpx<T> b = cpx<T>{x.x - eI * x.x, x.y - eI * x.y};
       Lz.c[c][i] = cpx<T>{x.x - eS * x.x, x.y - eS * x.y};
@@ -1087,13 +1138,13 @@ __global__ void adj_final(Geom3<T> g, T dt, T nu, Fields4<T> Lin, Fields4<T> Lz,
 // adjoint right-hand side of the stage that produced K
 template <typename T>
 __global__ void adj_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> Ls, Fields4<T> Lz,
-                          Fields4<T> Lk, Fields4<T> Ln, long len) {
+                          Fields4<T> Lk, Fields4<T> Ln, long len, int nc, T sc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x) {
     const TileMode<T> m = tile_mode(g, i);
     const T LL = m.keep ? (T)1 : (T)0;
-    const T e = stage_e(q, dt * nu * m.wk);
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < nc; ++c) {
+      const T e = stage_e(q, comp_nk(dt * nu * m.wk, c, sc));
       const cpx<T> l = Ls.c[c][i];
       const cpx<T> dl = cpx<T>{l.x - e * l.x, l.y - e * l.y};
       const cpx<T> z = Lz.c[c][i], k = Lk.c[c][i];
@@ -1105,15 +1156,86 @@ __global__ void adj_stage(Geom3<T> g, T dt, T nu, T q, T fr, Fields4<T> Ls, Fiel
   }
 }
 
-// y += a x
+// y = b y + a x  (nc components)
 template <typename T>
-__global__ void lin_axpy(Fields4<T> y, T a, Fields4<T> x, long len) {
+__global__ void lin_axpby(Fields4<T> y, T b, T a, Fields4<T> x, long len, int nc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x)
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < nc; ++c) {
       const cpx<T> u = y.c[c][i], v = x.c[c][i];
-      y.c[c][i] = cpx<T>{u.x + a * v.x, u.y + a * v.y};
+      y.c[c][i] = cpx<T>{b * u.x + a * v.x, b * u.y + a * v.y};
     }
+}
+
+// out = z + a x  (nc components)
+template <typename T>
+__global__ void lin_shift(Fields4<T> out, Fields4<T> z, T a, Fields4<T> x, long len, int nc) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x)
+    for (int c = 0; c < nc; ++c) {
+      const cpx<T> u = z.c[c][i], v = x.c[c][i];
+      out.c[c][i] = cpx<T>{u.x + a * v.x, u.y + a * v.y};
+    }
+}
+
+// partial sums of |x|^2 (nc components), one per block
+template <typename T>
+__global__ void __launch_bounds__(256) lin_norm2(Fields4<T> x, long len, int nc, double* part) {
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x)
+    for (int c = 0; c < nc; ++c) {
+      const cpx<T> v = x.c[c][i];
+      s += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+    }
+  __shared__ double r[256];
+  r[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) r[threadIdx.x] += r[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = r[0];
+}
+
+// Boussinesq adjoint right-hand side from the products
+//   PA = F(-(E(w) x E(C lw))), PB = F(-(E(C lw) x E(B w))),
+//   SA = [F(psi i k rho) (3), F(psi u_x)], SB = [F(psi u_y), F(psi u_z)], psi = E(l_rho):
+// l_w' = -B (PA + F(psi grad rho) - e l_rho) - PB,    e = (0, cos th, sin th)
+// l_rho' = conj(b) . l_w + i k . F(psi u),            b = Ri i (-(ky sin th - kz cos th), kx sin th, -kx cos th)
+// (buoyancy and stratification of scheme_point's Boussinesq branch, transposed)
+template <typename T>
+__global__ void bous_adj_combine(Geom3<T> g, T ri, T sinth, T costh, Fields4<T> PA, Fields4<T> PB,
+                                 Fields4<T> SA, Fields4<T> SB, Fields4<T> X, Fields4<T> out, long len) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+       i += (long)gridDim.x * blockDim.x) {
+    const TileMode<T> m = tile_mode(g, i);
+    const T LL = m.keep ? (T)1 : (T)0;
+    const T wki = wkinv(m.wk);
+    const cpx<T> lr = X.c[3][i];
+    cpx<T> v[3];
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> a = PA.c[c][i], sg = SA.c[c][i];
+      v[c] = cpx<T>{a.x + sg.x, a.y + sg.y};
+    }
+    v[1] = cpx<T>{v[1].x - costh * lr.x, v[1].y - costh * lr.y};
+    v[2] = cpx<T>{v[2].x - sinth * lr.x, v[2].y - sinth * lr.y};
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> bw = spec_op<T>(OP_BS, c, v, m.kx, m.ky, m.kz, wki), pb = PB.c[c][i];
+      out.c[c][i] = cpx<T>{-LL * (bw.x + pb.x), -LL * (bw.y + pb.y)};
+    }
+    // conj(i beta) l = beta (l.y, -l.x);  i k u = (-k u.y, k u.x)
+    const T beta[3] = {-ri * (m.ky * sinth - m.kz * costh), ri * m.kx * sinth, -ri * m.kx * costh};
+    const cpx<T> su[3] = {SA.c[3][i], SB.c[0][i], SB.c[1][i]};
+    const T kk[3] = {m.kx, m.ky, m.kz};
+    T rx = 0, ry = 0;
+    for (int c = 0; c < 3; ++c) {
+      const cpx<T> l = X.c[c][i];
+      rx += beta[c] * l.y - kk[c] * su[c].y;
+      ry += -beta[c] * l.x + kk[c] * su[c].x;
+    }
+    out.c[3][i] = cpx<T>{LL * rx, LL * ry};
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1142,7 +1264,8 @@ struct Engine3D final : Engine3DBase {
   // linearised step (tangent / adjoint), allocated on first use
   cpx<T>* lin = nullptr;
   Fields4<T> Zb[4]{};          // base stage states z, z1, z2, z3
-  Fields4<T> LA{}, LN{}, LS{}, LZ{}, LK1{}, LK2{}, LK3{}, PA{}, PB{}, LD{};
+  Fields4<T> LA{}, LN{}, LS{}, LZ{}, LK1{}, LK2{}, LK3{}, PA{}, PB{}, LD{}, LT{};
+  Fields4<T> SA{}, SB{};       // Boussinesq adjoint products: psi (i k rho) | psi u
   int c_variant = 0;           // x-pass variant chosen by the autotuner
   int c_resident[4] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
   float c_ms[4] = {0, 0, 0, 0};      // autotuner timings (ms per launch)
@@ -1258,7 +1381,11 @@ struct Engine3D final : Engine3DBase {
     const long b1 = (long)nfi * n * g.Y * g.XP;
     const long b3 = (long)nfo * n * n * g.XP;
     const long b2 = (long)nfi * n * n * g.XP;
-    const long nb1 = b1 > b3 ? b1 : b3;
+    // B1 also holds the x-pass output of the linearised Boussinesq step's
+    // scalar products (6 fields)
+    const long b3lin = (bous ? 6L : 3L) * n * n * g.XP;
+    long nb1 = b1 > b3 ? b1 : b3;
+    if (b3lin > nb1) nb1 = b3lin;
     // the FP32 engine carries the rounding error of its state updates
     const int ncomp_regs = std::is_same<T, float>::value ? 1 : 0;
     const long total = (long)(nregs + ncomp_regs) * nc * box + nb1 + b2 + 2 * n;
@@ -1370,16 +1497,19 @@ struct Engine3D final : Engine3DBase {
     }
   }
   template <int N>
-  int launch_c(int v, T scale, T* dp) {
+  // nf: fields the x-pass reads (6: -(u x w); 9: + u.grad rho; 7: the
+  // Boussinesq adjoint's scalar products); 0: the engine's own
+  int launch_c(int v, T scale, T* dp, int nf = 0) {
     constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
     const int rows = L1 * c_rows_mult(v);
     const int ntiles = (N * N) / rows;
     const int grid = ntiles < c_resident[v] ? ntiles : c_resident[v];
     const size_t sm = smem_c_v(v);
     const int th = c_threads<N>(v);
-    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    if (!nf) nf = (scheme == SCHEME_BOUS_RK4) ? 9 : 6;
 #define PSG_LC(LL, STG)                                                                          \
-  if (bous) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
+  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
+  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
   else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles);
     switch (v) {
       case 0: PSG_LC(L1, 1); break;
@@ -1593,6 +1723,13 @@ struct Engine3D final : Engine3DBase {
   }
 
   // ---------------------------------------------------------------- linearised step
+  size_t smem_a_nc(int ncin) const {
+    return sizeof(cpx<T>) * ((size_t)ncin * g.Y * kTileW + (size_t)ncin * g.Y + g.n +
+                             2 * kTileW * col_stride()) + g.Y * kTileW;
+  }
+  size_t smem_e_no(int no) const {
+    return sizeof(cpx<T>) * ((size_t)no * g.n * kTileW + g.n + kTileW * col_stride());
+  }
   size_t smem_pair() const {
     return sizeof(cpx<T>) * ((size_t)6 * g.Y * kTileW + (size_t)6 * g.Y + g.n +
                              2 * kTileW * col_stride()) + g.Y * kTileW;
@@ -1604,22 +1741,35 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaGetDevice(&dev));
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     big -= 1024;
-    if (smem_pair() > (size_t)big) {
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    const size_t need = std::max(smem_pair(), bous ? std::max(smem_a_nc(5), smem_e_no(6)) : 0);
+    if (need > (size_t)big) {
       psg_set_error("linearised step at grid %d needs %zu bytes of shared memory per block", g.n,
-                    smem_pair());
+                    need);
       return PSG_ERR_UNSUPPORTED;
     }
     PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, 6, 6, 1>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, 3, SCHEME_RAW>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    if (bous) {
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_a<T, N, 5, 7, 2>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, 6, SCHEME_RAW>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, L1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, 2 * L1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, L1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, 2 * L1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    }
     return PSG_OK;
   }
 
   int lin_init() {
     if (lin) return PSG_OK;
-    if (scheme != SCHEME_NS_RK4) {
-      psg_set_error("tangent and adjoint steps are defined for the Navier-Stokes RK4/CN scheme");
+    if (scheme != SCHEME_NS_RK4 && scheme != SCHEME_BOUS_RK4) {
+      psg_set_error("tangent and adjoint steps are defined for the RK4/CN schemes");
       return PSG_ERR_UNSUPPORTED;
     }
     int rc;
@@ -1631,16 +1781,22 @@ struct Engine3D final : Engine3DBase {
       default: rc = lin_attrs<256>(); break;
     }
     if (rc) return rc;
-    constexpr int kFields = 14;
-    PSG_CUDA_TRY(cudaMalloc(&lin, sizeof(cpx<T>) * kFields * 3 * box));
-    PSG_CUDA_TRY(cudaMemsetAsync(lin, 0, sizeof(cpx<T>) * kFields * 3 * box, stream));
+    // state-shaped registers (nc components) and product outputs (3, or 4 + 2)
+    constexpr int kState = 13;
+    Fields4<T>* st[kState] = {&Zb[0], &Zb[1], &Zb[2], &Zb[3], &LA, &LN, &LS,
+                              &LZ, &LK1, &LK2, &LK3, &LD, &LT};
+    const long words = ((long)kState * nc + 3 + 3 + (nc > 3 ? 6 : 0)) * box;
+    PSG_CUDA_TRY(cudaMalloc(&lin, sizeof(cpx<T>) * words));
+    PSG_CUDA_TRY(cudaMemsetAsync(lin, 0, sizeof(cpx<T>) * words, stream));
     cpx<T>* p = lin;
-    Fields4<T>* all[kFields] = {&Zb[0], &Zb[1], &Zb[2], &Zb[3], &LA, &LN, &LS,
-                                &LZ, &LK1, &LK2, &LK3, &PA, &PB, &LD};
-    for (Fields4<T>* f : all) {
-      for (int q = 0; q < 4; ++q) f->c[q] = nullptr;
-      for (int q = 0; q < 3; ++q) { f->c[q] = p; p += box; }
-    }
+    auto carve = [&](Fields4<T>& f, int k) {
+      for (int q = 0; q < 4; ++q) f.c[q] = nullptr;
+      for (int q = 0; q < k; ++q) { f.c[q] = p; p += box; }
+    };
+    for (Fields4<T>* f : st) carve(*f, nc);
+    carve(PA, 3);
+    carve(PB, 3);
+    if (nc > 3) { carve(SA, 4); carve(SB, 2); }
     return PSG_OK;
   }
 
@@ -1653,7 +1809,7 @@ struct Engine3D final : Engine3DBase {
     pass_a<T, N, 6, 6, 1><<<dim3(XT, g.Y), blk2, smem_pair(), stream>>>(
         g, b, B1, tw, 0, d_status, a, op_b | (op_a << 4));
     pass_b<T, N><<<dim3(XT, N, 6), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
-    launch_c<N>(c_variant, (T)1 / ((T)N * (T)N * (T)N), nullptr);
+    launch_c<N>(c_variant, (T)1 / ((T)N * (T)N * (T)N), nullptr, 6);
     pass_d<T, N><<<dim3(XT, N, 3), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     Regs<T> Rr{};
     Rr.K1 = out;
@@ -1663,6 +1819,53 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
+  // SA, SB <- the Boussinesq adjoint's scalar products of psi = E(x_rho) with
+  // E(i k z_rho) and E(B z_w)
+  template <int N>
+  int scale_products_n(Fields4<T> z, Fields4<T> x) {
+    using FG = LineFFT<N, 1, T>;
+    const dim3 blk(kTileW * FG::G), blk2(2 * kTileW * FG::G);
+    const int XT = g.XP / kTileW;
+    Fields4<T> psi{};
+    psi.c[0] = x.c[3];
+    pass_a<T, N, 5, 7, 2><<<dim3(XT, g.Y), blk2, smem_a_nc(5), stream>>>(g, z, B1, tw, 0, d_status,
+                                                                         psi, 0);
+    pass_b<T, N><<<dim3(XT, N, 7), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
+    launch_c<N>(c_variant, (T)1 / ((T)N * (T)N * (T)N), nullptr, 7);
+    pass_d<T, N><<<dim3(XT, N, 6), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
+    Regs<T> Rr{};
+    Rr.K1 = SA;
+    Rr.K2 = SB;
+    pass_e<T, N, 6, SCHEME_RAW><<<dim3(XT, g.Y), blk, smem_e_no(6), stream>>>(g, B2, tw, Rr, prm, 0,
+                                                                              d_status);
+    launches += 5;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+  int scale_products(Fields4<T> z, Fields4<T> x) {
+    switch (g.n) {
+      case 16: return scale_products_n<16>(z, x);
+      case 32: return scale_products_n<32>(z, x);
+      case 64: return scale_products_n<64>(z, x);
+      case 128: return scale_products_n<128>(z, x);
+      default: return scale_products_n<256>(z, x);
+    }
+  }
+
+  double norm2(Fields4<T> x) {
+    constexpr int kBlk = 296;
+    if (!d_energ && cudaMalloc(&d_energ, sizeof(double) * (3 * kBlk + 3)) != cudaSuccess) return -1.0;
+    lin_norm2<T><<<kBlk, 256, 0, stream>>>(x, box, nc, d_energ);
+    ++launches;
+    double h[kBlk];
+    if (cudaMemcpyAsync(h, d_energ, sizeof(double) * kBlk, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return -1.0;
+    double t = 0.0;
+    for (int b = 0; b < kBlk; ++b) t += h[b];
+    return t;
+  }
+
   int bilinear(Fields4<T> b, int op_b, Fields4<T> a, int op_a, Fields4<T> out) {
     switch (g.n) {
       case 16: return bilinear_n<16>(b, op_b, a, op_a, out);
@@ -1676,6 +1879,7 @@ struct Engine3D final : Engine3DBase {
   // out = N'(z) x (tangent) or N'(z)^T x (adjoint)
   int lin_rhs(int adjoint, Fields4<T> z, Fields4<T> x, Fields4<T> out) {
     int rc;
+    if (scheme == SCHEME_BOUS_RK4) return lin_rhs_bous(adjoint, z, x, out);
     if (!adjoint) {
       if ((rc = bilinear(z, OP_ID, x, OP_BS, PA))) return rc;  // F(-(E(B x) x E(z)))
       if ((rc = bilinear(x, OP_ID, z, OP_BS, PB))) return rc;  // F(-(E(B z) x E(x)))
@@ -1689,19 +1893,67 @@ struct Engine3D final : Engine3DBase {
     return PSG_OK;
   }
 
+  // Boussinesq: the tangent as the central difference of the engine's own
+  // right-hand side (exact up to round-off: the terms are quadratic and
+  // linear), D(z + s x) - D(z - s x) over 2 s with s = |z| / |x|; the adjoint
+  // from the cross products and the scalar products, transposed by hand
+  int lin_rhs_bous(int adjoint, Fields4<T> z, Fields4<T> x, Fields4<T> out) {
+    int rc;
+    if (!adjoint) {
+      const double nx = norm2(x), nz = norm2(z);
+      if (nx < 0.0 || nz < 0.0) { psg_set_error("norm reduction failed"); return PSG_ERR_CUDA; }
+      if (nx == 0.0) {
+        lin_axpby<T><<<592, 256, 0, stream>>>(out, (T)0, (T)0, x, box, nc);
+        ++launches;
+        return PSG_OK;
+      }
+      const T sc = (T)(nz > 0.0 ? sqrt(nz / nx) : 1.0);
+      const int saved_first = first_rhs;
+      first_rhs = 0;
+      lin_shift<T><<<592, 256, 0, stream>>>(R.X0, z, sc, x, box, nc);
+      ++launches;
+      if ((rc = rhs(STAGE_DERIV))) return rc;
+      copy_fields<T><<<592, 256, 0, stream>>>(R.K1, LT, nc, box);
+      lin_shift<T><<<592, 256, 0, stream>>>(R.X0, z, -sc, x, box, nc);
+      launches += 2;
+      if ((rc = rhs(STAGE_DERIV))) return rc;
+      first_rhs = saved_first;
+      copy_fields<T><<<592, 256, 0, stream>>>(LT, out, nc, box);
+      lin_axpby<T><<<592, 256, 0, stream>>>(out, (T)(0.5) / sc, (T)(-0.5) / sc, R.K1, box, nc);
+      launches += 2;
+      PSG_CUDA_TRY(cudaGetLastError());
+      return PSG_OK;
+    }
+    if ((rc = bilinear(x, OP_CURL, z, OP_ID, PA))) return rc;  // F(-(E(z) x E(C x)))
+    if ((rc = bilinear(z, OP_BS, x, OP_CURL, PB))) return rc;  // F(-(E(C x) x E(B z)))
+    if ((rc = scale_products(z, x))) return rc;
+    bous_adj_combine<T><<<592, 256, 0, stream>>>(g, prm.ri, prm.sinth, prm.costh, PA, PB, SA, SB,
+                                                 x, out, box);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
   // one forward step from S with X0 = S, keeping the four stage states
   int base_stages(T dt) {
     prm.dt = dt;
-    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, 3, box);
-    copy_fields<T><<<592, 256, 0, stream>>>(R.S, Zb[0], 3, box);
+    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
+    copy_fields<T><<<592, 256, 0, stream>>>(R.S, Zb[0], nc, box);
     launches += 2;
     const int stg[3] = {STAGE_RK1, STAGE_RK2, STAGE_RK3};
     for (int s = 0; s < 3; ++s) {
       if (int rc = rhs(stg[s])) return rc;
-      copy_fields<T><<<592, 256, 0, stream>>>(R.X0, Zb[s + 1], 3, box);
+      copy_fields<T><<<592, 256, 0, stream>>>(R.X0, Zb[s + 1], nc, box);
       ++launches;
     }
     return rhs(STAGE_RK4);
+  }
+
+  // after a linearised step: the stage state of the advanced state is the
+  // state itself, as after an upload (the Boussinesq tangent reuses X0, K1)
+  void reset_stage_state() {
+    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
+    ++launches;
   }
 
   // D <- dPhi(S) D, S <- Phi(S)
@@ -1712,15 +1964,17 @@ struct Engine3D final : Engine3DBase {
     const T qs[3] = {(T)0.25, (T)0.25, (T)0.5}, frs[3] = {(T)0.5, (T)0.5, (T)1};
     Fields4<T> Ks[3] = {LK1, LK2, LK3};
     Fields4<T> in = D;
+    const T sc = prm.sc;
     for (int s = 0; s < 3; ++s) {
       if ((rc = lin_rhs(0, Zb[s], in, LN))) return rc;
-      tan_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LN, D, Ks[s], LA, box);
+      tan_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LN, D, Ks[s], LA, box, nc, sc);
       ++launches;
       in = LA;
     }
     if ((rc = lin_rhs(0, Zb[3], LA, LN))) return rc;
-    tan_final<T><<<592, 256, 0, stream>>>(g, dt, nu, LN, LK1, LK2, LK3, D, box);
+    tan_final<T><<<592, 256, 0, stream>>>(g, dt, nu, LN, LK1, LK2, LK3, D, box, nc, sc);
     ++launches;
+    reset_stage_state();
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -1730,19 +1984,21 @@ struct Engine3D final : Engine3DBase {
     int rc;
     if ((rc = base_stages(dt))) return rc;
     const T nu = prm.nu;
-    adj_final<T><<<592, 256, 0, stream>>>(g, dt, nu, L, LZ, LK1, LK2, LK3, LN, box);
+    const T sc = prm.sc;
+    adj_final<T><<<592, 256, 0, stream>>>(g, dt, nu, L, LZ, LK1, LK2, LK3, LN, box, nc, sc);
     ++launches;
     const T qs[3] = {(T)0.5, (T)0.25, (T)0.25}, frs[3] = {(T)1, (T)0.5, (T)0.5};
     Fields4<T> Ks[3] = {LK3, LK2, LK1};
     for (int s = 0; s < 3; ++s) {
       if ((rc = lin_rhs(1, Zb[3 - s], LN, LS))) return rc;
-      adj_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LS, LZ, Ks[s], LN, box);
+      adj_stage<T><<<592, 256, 0, stream>>>(g, dt, nu, qs[s], frs[s], LS, LZ, Ks[s], LN, box, nc, sc);
       ++launches;
     }
     if ((rc = lin_rhs(1, Zb[0], LN, LS))) return rc;
-    lin_axpy<T><<<592, 256, 0, stream>>>(LZ, (T)1, LS, box);
-    copy_fields<T><<<592, 256, 0, stream>>>(LZ, L, 3, box);
+    lin_axpby<T><<<592, 256, 0, stream>>>(LZ, (T)1, (T)1, LS, box, nc);
+    copy_fields<T><<<592, 256, 0, stream>>>(LZ, L, nc, box);
     launches += 2;
+    reset_stage_state();
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -1753,9 +2009,9 @@ struct Engine3D final : Engine3DBase {
   int linear(int mode, double dt, const void* const* in, void* const* out) override {
     int rc;
     if ((rc = lin_init())) return rc;
-    for (int q = 0; q < 3; ++q)
+    for (int q = 0; q < nc; ++q)
       box_from_ref<T><<<592, 256, 0, stream>>>(g, (const double2*)in[q], LD.c[q], nullptr);
-    launches += 3;
+    launches += nc;
     Fields4<T> res = LD;
     switch (mode) {
       case 0: rc = tangent_step_t((T)dt, LD); break;
@@ -1765,9 +2021,9 @@ struct Engine3D final : Engine3DBase {
       default: psg_set_error("linear mode %d unknown", mode); return PSG_ERR_ARG;
     }
     if (rc) return rc;
-    for (int q = 0; q < 3; ++q)
+    for (int q = 0; q < nc; ++q)
       box_to_ref<T><<<592, 256, 0, stream>>>(g, res.c[q], (double2*)out[q], nullptr);
-    launches += 3;
+    launches += nc;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }

@@ -116,3 +116,90 @@ def test_fp32_linear_step_matches_fp64(mode):
         e = _engine(z, prec)
         r[prec] = e.linear(mode, _cuda(d), DT).cpu().numpy()
     assert _rel(r[32], r[64]) < 2e-5
+
+
+# ---------------------------------------------------------------- Boussinesq
+# Ri = 1 (N = 1), Sc = 1 (Pr = 1), gravity along z (theta = 90 degrees)
+RI, SC, THETA = 1.0, 1.0, np.pi / 2
+
+
+def _bous_engine(z, precision=64):
+    e = P.NS3D(N, P.SCHEME_BOUS_RK4, precision=precision, nu=NU, ri=RI, sc=SC, theta=THETA)
+    e.upload(*z)
+    return e
+
+
+def _bous_base():
+    w = _base()
+    g = Grid3D(N)
+    rho = random_vorticity3d(N, 33)[0] * g.mask()
+    return np.concatenate([w, rho[None]], axis=0)
+
+
+def _bous_masked(seed, amp=1.0):
+    g = Grid3D(N)
+    rng = np.random.default_rng(seed)
+    v = np.stack([(rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * g.mask()
+                  for _ in range(4)])
+    return amp * v / np.sqrt(np.sum(np.abs(v) ** 2))
+
+
+@pytest.mark.parametrize("mode", [P.NS3D.LIN_ADJOINT_RHS, P.NS3D.LIN_ADJOINT_STEP])
+def test_bous_adjoint_dot_product(mode):
+    z = _bous_base()
+    d, lam = _bous_masked(12), _bous_masked(13)
+    tmode = P.NS3D.LIN_TANGENT_RHS if mode == P.NS3D.LIN_ADJOINT_RHS else P.NS3D.LIN_TANGENT_STEP
+    e = _bous_engine(z)
+    jd = e.linear(tmode, _cuda(d), DT)
+    e.upload(*z)
+    jtl = e.linear(mode, _cuda(lam), DT)
+    torch.cuda.synchronize()
+    lhs, rhs = _dot(lam, jd), _dot(jtl, d)
+    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), 1e-300) + 1e-13 * np.linalg.norm(jd.cpu().numpy())
+
+
+def test_bous_tangent_step_matches_central_difference():
+    z = _bous_base()
+    d = _bous_masked(14, amp=np.sqrt(np.sum(np.abs(z) ** 2)))
+    e = _bous_engine(z)
+    jd = e.linear(P.NS3D.LIN_TANGENT_STEP, _cuda(d), DT).cpu().numpy()
+    eps = 1e-5
+    outs = []
+    for s in (+1, -1):
+        f = _bous_engine(z + s * eps * d)
+        f.step(DT, 1)
+        outs.append(np.stack(f.download()))
+    fd = (outs[0] - outs[1]) / (2 * eps)
+    assert _rel(jd, fd) < 1e-7
+
+
+@pytest.mark.parametrize("mode", [P.NS3D.LIN_TANGENT_STEP, P.NS3D.LIN_ADJOINT_STEP])
+def test_bous_fp32_linear_step_matches_fp64(mode):
+    z = _bous_base()
+    d = _bous_masked(15)
+    r = {}
+    for prec in (64, 32):
+        e = _bous_engine(z, prec)
+        r[prec] = e.linear(mode, _cuda(d), DT).cpu().numpy()
+    assert _rel(r[32], r[64]) < 5e-5
+
+
+def test_bous_adjoint_step_dot_product_64():
+    """the whole adjoint step at 64^3 (the scalar products' six x-pass outputs
+    fill the intermediate buffer more than the forward step's do)"""
+    n = 64
+    g = Grid3D(n)
+    rng = np.random.default_rng(41)
+    m = g.mask()
+    def rnd():
+        return np.stack([(rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * m
+                         for _ in range(4)])
+    z, d, lam = rnd() * 0.05, rnd(), rnd()
+    e = P.NS3D(n, P.SCHEME_BOUS_RK4, precision=64, nu=NU, ri=RI, sc=SC, theta=THETA)
+    e.upload(*z)
+    jd = e.linear(P.NS3D.LIN_TANGENT_STEP, _cuda(d), DT)
+    e.upload(*z)
+    jtl = e.linear(P.NS3D.LIN_ADJOINT_STEP, _cuda(lam), DT)
+    torch.cuda.synchronize()
+    lhs, rhs = _dot(lam, jd), _dot(jtl, d)
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
