@@ -37,6 +37,27 @@ struct InstTan2D {
   cpx<T>* work;  // [6][n][K+1]
 };
 
+// The thread blocks that integrate one instance together: one block, or the
+// two blocks of a cluster, each taking every other group of lines in every
+// phase (the row scratch is in global memory, so no shared memory crosses
+// blocks); the phases are separated by a block or a cluster barrier.
+struct Team {
+  int rank, size;
+};
+
+__device__ __forceinline__ void team_sync(const Team& t) {
+  if (t.size == 1) {
+    __syncthreads();
+  } else {
+    // release this block's global writes at cluster scope, then wait for the
+    // other block's (barrier.cluster with release / acquire semantics)
+    asm volatile(
+        "fence.acq_rel.cluster;\n\t"
+        "barrier.cluster.arrive.release.aligned;\n\t"
+        "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
+}
+
 template <typename T, int N>
 struct Tan2D {
   using FI = LineFFT<N, +1, T>;
@@ -46,8 +67,10 @@ struct Tan2D {
   static constexpr int K = N / 3, X = K + 1, Y = 2 * K + 1;
 
   // phase 1: y-inverse of nf fields (0..2 base from Z0, 3..5 perturbation from D0)
-  static __device__ void phase1(const InstTan2D<T>& I, const cpx<T>* tw, cpx<T>* ex, int nf) {
-    const int gid = threadIdx.x / G, gi = threadIdx.x % G, ng = blockDim.x / G;
+  static __device__ void phase1(const InstTan2D<T>& I, const cpx<T>* tw, cpx<T>* ex, int nf,
+                                const Team& t) {
+    const int gid = t.rank * (blockDim.x / G) + threadIdx.x / G, gi = threadIdx.x % G;
+    const int ng = t.size * (blockDim.x / G);
     for (int base = 0; base < nf * X; base += ng) {
       const int col = base + gid;
       const bool live = col < nf * X;
@@ -114,8 +137,10 @@ struct Tan2D {
 
   // phase 2: rows.  Base products (v w, u w) -> work[0], work[1]; with the
   // perturbation, their linearisation -> work[2], work[3].
-  static __device__ void phase2(const InstTan2D<T>& I, const cpx<T>* tw, cpx<T>* ex, bool tan) {
-    const int gid = threadIdx.x / G, gi = threadIdx.x % G, ng = blockDim.x / G;
+  static __device__ void phase2(const InstTan2D<T>& I, const cpx<T>* tw, cpx<T>* ex, bool tan,
+                                const Team& t) {
+    const int gid = t.rank * (blockDim.x / G) + threadIdx.x / G, gi = threadIdx.x % G;
+    const int ng = t.size * (blockDim.x / G);
     const T scale = (T)1 / ((T)N * (T)N);
     const long fs = (long)N * X;
     for (int base = 0; base < N; base += ng) {
@@ -183,8 +208,9 @@ struct Tan2D {
 
   // phase 3: y-forward, spectral finish, stage update (s >= 0) or derivative (s < 0)
   static __device__ void phase3(const InstTan2D<T>& I, const cpx<T>* tw, cpx<T>* ex, int s,
-                                bool tan) {
-    const int gid = threadIdx.x / G, gi = threadIdx.x % G, ng = blockDim.x / G;
+                                bool tan, const Team& t) {
+    const int gid = t.rank * (blockDim.x / G) + threadIdx.x / G, gi = threadIdx.x % G;
+    const int ng = t.size * (blockDim.x / G);
     const long fs = (long)N * X;
     for (int base = 0; base < X; base += ng) {
       const int ikx = base + gid;
@@ -234,35 +260,36 @@ struct Tan2D {
     }
   }
 
-  static __device__ void run(const InstTan2D<T>& I, const cpx<T>* __restrict__ gtw, cpx<T>* smem) {
+  static __device__ void run(const InstTan2D<T>& I, const cpx<T>* __restrict__ gtw, cpx<T>* smem,
+                             Team t = Team{0, 1}) {
     cpx<T>* tw = smem;
     cpx<T>* ex = smem + 2 * N + (threadIdx.x / G) * FI::SMEM;
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = gtw[i];
     const bool tan = (I.mode == 0);
-    for (int ik = threadIdx.x; ik < X * Y; ik += blockDim.x) {
+    for (int ik = t.rank * blockDim.x + threadIdx.x; ik < X * Y; ik += t.size * blockDim.x) {
       const int iky = ik / X, ikx = ik % X;
       const bool keep = keep2(ikx, iky - K, K);
       I.Z0[ik] = keep ? I.Z[ik] : czero<T>();
       if (tan) I.D0[ik] = keep ? I.D[ik] : czero<T>();
     }
-    __syncthreads();
+    team_sync(t);
     if (I.mode == 2) {
-      phase1(I, tw, ex, 3);
-      __syncthreads();
-      phase2(I, tw, ex, false);
-      __syncthreads();
-      phase3(I, tw, ex, -1, false);
-      __syncthreads();
+      phase1(I, tw, ex, 3, t);
+      team_sync(t);
+      phase2(I, tw, ex, false, t);
+      team_sync(t);
+      phase3(I, tw, ex, -1, false, t);
+      team_sync(t);
       return;
     }
     for (int step = 0; step < I.nsteps; ++step) {
       for (int s = 0; s < 4; ++s) {
-        phase1(I, tw, ex, tan ? 6 : 3);
-        __syncthreads();
-        phase2(I, tw, ex, tan);
-        __syncthreads();
-        phase3(I, tw, ex, s, tan);
-        __syncthreads();
+        phase1(I, tw, ex, tan ? 6 : 3, t);
+        team_sync(t);
+        phase2(I, tw, ex, tan, t);
+        team_sync(t);
+        phase3(I, tw, ex, s, tan, t);
+        team_sync(t);
       }
     }
   }
