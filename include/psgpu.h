@@ -156,6 +156,32 @@ long psg_batch2d_launches(psg_batch2d* h);
  * writes Z directly must zero that array too (or use psg_batch2d_upload). */
 int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z);
 
+/* ------------------------------------------------------- recurrence search */
+/* Near-recurrence search for UPO guesses, as the 3D DNS does it
+ * (3D_NavierStokes/src/functions.h:111-389): a ring of store_size states,
+ * each new one compared with the earlier ones under nshift_x * nshift_y *
+ * nshift_z trial translations over the 4 W^3 modes of a low-wavenumber box
+ * (W = norm_width; the reference uses 500, 8, 30, 2, 2).  States are 3 device
+ * FP64 boxes (reference layout).  psg_rec3d_start takes the initial state;
+ * psg_rec3d_add the state after step nt (nt = NOUT, 2 NOUT, ...); *emitted is
+ * 1 when a guess left the residual threshold, whose data psg_rec3d_guess then
+ * returns: meta[7] = start time, v2, period, shift x, y, z, residual, and the
+ * state (host arrays, each may be null). */
+typedef struct psg_rec3d psg_rec3d;
+int psg_rec3d_create(psg_rec3d** h, int n, double alpha, int store_size, int norm_width,
+                     int nshift_x, int nshift_y, int nshift_z, double threshold, int nout,
+                     double dt, double tstart, double v2);
+void psg_rec3d_destroy(psg_rec3d* h);
+int psg_rec3d_set_stream(psg_rec3d* h, void* cuda_stream);
+int psg_rec3d_start(psg_rec3d* h, void* const* state);
+int psg_rec3d_add(psg_rec3d* h, int nt, void* const* state, int* emitted);
+int psg_rec3d_guess(psg_rec3d* h, double* meta, double* xii, double* eta, double* zet);
+/* the same, with the state taken from a 3D engine (its current state) */
+int psg_rec3d_start_engine(psg_rec3d* h, psg_ns3d* engine);
+int psg_rec3d_add_engine(psg_rec3d* h, int nt, psg_ns3d* engine, int* emitted);
+int psg_rec3d_count(psg_rec3d* h);
+long psg_rec3d_launches(psg_rec3d* h);
+
 /* ---------------------------------------------------------------- UPO search */
 /* Batched Newton-GMRES-hookstep search for unstable periodic orbits of 2D
  * Kolmogorov flow (2D_NavierStokes/src_RK4/src_gmres/main.F90:688-1823), all

@@ -101,6 +101,14 @@ def _declare_2d(L):
     L.psg_batch2d_launches.restype = C.c_long
     L.psg_batch2d_device_state.argtypes = [vp, i, C.POINTER(vp)]
     L.psg_ns2d_step_noalloc.argtypes = [i, i, C.c_double, C.c_double, i, vp, vp, vp]
+    d = C.c_double
+    L.psg_rec3d_create.argtypes = [C.POINTER(vp), i, d, i, i, i, i, i, d, i, d, d, d]
+    L.psg_rec3d_destroy.argtypes = [vp]
+    L.psg_rec3d_destroy.restype = None
+    L.psg_rec3d_start.argtypes = [vp, C.POINTER(vp)]
+    L.psg_rec3d_add.argtypes = [vp, i, C.POINTER(vp), C.POINTER(i)]
+    L.psg_rec3d_guess.argtypes = [vp, dp, dp, dp, dp]
+    L.psg_rec3d_count.argtypes = [vp]
     L.psg_upo2d_create.argtypes = [C.POINTER(vp), i, i, i, i]
     L.psg_upo2d_destroy.argtypes = [vp]
     L.psg_upo2d_destroy.restype = None
@@ -345,6 +353,56 @@ class Batch2D:
     @property
     def launches(self) -> int:
         return int(lib().psg_batch2d_launches(self._h))
+
+
+class Recurrence3D:
+    """Near-recurrence search over a ring of stored 3D states (the DNS's UPO guess
+    generator), residuals on the GPU.  States are torch CUDA complex128 tensors
+    of shape (3, IKTZ, IKTY, IKTX) in the reference layout."""
+
+    def __init__(self, n, nout, dt, threshold, store_size=500, norm_width=8, nshift=(30, 2, 2),
+                 alpha=1.0, tstart=0.0, v2=0.0):
+        h = C.c_void_p()
+        _check(lib().psg_rec3d_create(C.byref(h), n, alpha, store_size, norm_width, nshift[0],
+                                      nshift[1], nshift[2], threshold, nout, dt, tstart, v2))
+        self._h = h
+        self.grid = Grid3D(n)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().psg_rec3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptrs(t):
+        return (C.c_void_p * 3)(*[t[q].data_ptr() for q in range(3)])
+
+    def start(self, state):
+        _check(lib().psg_rec3d_start(self._h, self._ptrs(state.contiguous())))
+
+    def add(self, nt, state) -> bool:
+        e = C.c_int()
+        _check(lib().psg_rec3d_add(self._h, int(nt), self._ptrs(state.contiguous()), C.byref(e)))
+        return bool(e.value)
+
+    def guess(self):
+        meta = np.zeros(7)
+        out = [np.zeros(self.grid.shape, np.complex128) for _ in range(3)]
+        dp = C.POINTER(C.c_double)
+        _check(lib().psg_rec3d_guess(self._h, meta.ctypes.data_as(dp),
+                                     *[o.ctypes.data_as(dp) for o in out]))
+        keys = ("time", "v2", "period", "shift_x", "shift_y", "shift_z", "residual")
+        return dict(zip(keys, meta.tolist())), tuple(out)
+
+    @property
+    def count(self) -> int:
+        return int(lib().psg_rec3d_count(self._h))
 
 
 UPO_STATUS = {0: "ACTIVE", 1: "CONVERGED", 2: "GMRES FAILED", 3: "H-STEP FAILED", 4: "NEWTON STALLED",

@@ -8,7 +8,8 @@
  * start (or reads the restart file named there), integrates NSTOP Heun /
  * Crank-Nicolson steps with the DNS forcing, writes JOBDIR/stats.dat and
  * JOBDIR/engy.dat every NOUT steps as the reference's statistics do
- * (3D_NavierStokes/src/cuda.cu:116-140), and JOBDIR/Zk.out: main.F90's header
+ * (3D_NavierStokes/src/cuda.cu:116-140), with RCFLAG = 1 the recurrence
+ * search's UPO_ZK.out / UPOinfo_ts.dat, and JOBDIR/Zk.out: main.F90's header
  * record (1, IKTX, IKTY, IKTZ) followed by the final state as a type "D"
  * restart record.  The grid is compile-time in the reference
  * (global_params.F90, 128^3); here it is -n (default 128). */
@@ -78,8 +79,23 @@ int main(int argc, char** argv) {
   double* out[3] = {st[0], st[1], st[2]};
   if (psg_ns3d_upload(h, in)) FAIL("%s", psg_last_error());
 
-  FILE *fs = NULL, *fe = NULL;
+  FILE *fs = NULL, *fe = NULL, *fu = NULL, *fi = NULL;
   psg_stats3d* S = NULL;
+  psg_rec3d* rec = NULL;
+  if (P.rcflag == 1) {
+    /* recurrence search (init.h:182-213): UPO guesses into UPO_ZK.out (a type A
+     * stream) and UPOinfo_ts.dat */
+    if (psg_rec3d_create(&rec, n, 1.0, 500, 8, 30, 2, 2, P.residual_threshold, P.nout, P.delt,
+                         0.0, P.v2) ||
+        psg_rec3d_start_engine(rec, h))
+      FAIL("%s", psg_last_error());
+    snprintf(path, sizeof path, "%s/UPO_ZK.out", dir);
+    fu = fopen(path, "wb");
+    snprintf(path, sizeof path, "%s/UPOinfo_ts.dat", dir);
+    fi = fopen(path, "w");
+    if (!fu || !fi) FAIL("cannot open the recurrence files in %s", dir);
+    fprintf(fi, "Guess No : Start time : guess Period : guess Shift x: guess Shift y: guess Residual \n");
+  }
   if (P.statsflag) {
     snprintf(path, sizeof path, "%s/stats.dat", dir);
     fs = fopen(path, "w");
@@ -91,11 +107,27 @@ int main(int argc, char** argv) {
   const double t0 = now();
   int done = 0;
   /* statistics after step NT for NT = NOUT, 2 NOUT, ... (NT counted from 0) */
-  for (int nt = P.nout; nt < P.nstop && S; nt += P.nout) {
+  int izkout = 0;
+  for (int nt = P.nout; nt < P.nstop && (S || rec); nt += P.nout) {
     if (psg_ns3d_step(h, P.delt, nt + 1 - done, 0)) FAIL("%s", psg_last_error());
     done = nt + 1;
     const double tme = done * P.delt;
-    if (P.statsflag == 2 && tme <= 500.0) continue;
+    if (rec) {
+      int emitted = 0;
+      if (psg_rec3d_add_engine(rec, nt, h, &emitted)) FAIL("%s", psg_last_error());
+      if (emitted) {
+        double meta[7];
+        if (psg_rec3d_guess(rec, meta, st[0], st[1], st[2])) FAIL("%s", psg_last_error());
+        fwrite(meta, sizeof(double), 7, fu);
+        for (int q = 0; q < 3; ++q) fwrite(st[q], 2 * sizeof(double), nkt, fu);
+        ++izkout;
+        fprintf(fi, "%d %e %e %e %e %e %e \n", izkout, meta[0], meta[2], meta[3], meta[4], meta[5],
+                meta[6]);
+        fflush(fu);
+        fflush(fi);
+      }
+    }
+    if (!S || (P.statsflag == 2 && tme <= 500.0)) continue;
     if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
     psg_stats3d_add(S, tme, st[0], st[1], st[2], fs, fe);
   }
@@ -106,12 +138,15 @@ int main(int argc, char** argv) {
   snprintf(path, sizeof path, "%s/Zk.out", dir);
   FILE* fz = fopen(path, "wb");
   if (!fz) FAIL("cannot write %s", path);
-  const double rec[7] = {P.nstop * P.delt, P.v2, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (psg_write_state3d_header(fz, 1, n) || psg_write_state3d_record(fz, n, rec, st[0], st[1], st[2]))
+  const double fin[7] = {P.nstop * P.delt, P.v2, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (psg_write_state3d_header(fz, 1, n) || psg_write_state3d_record(fz, n, fin, st[0], st[1], st[2]))
     FAIL("writing %s failed", path);
   fclose(fz);
   if (fs) fclose(fs);
   if (fe) fclose(fe);
+  if (fu) fclose(fu);
+  if (fi) fclose(fi);
+  psg_rec3d_destroy(rec);
   psg_stats3d_destroy(S);
   psg_ns3d_destroy(h);
   printf("time stepping done: %d steps in %.3f s (%.1f steps/s)\n", P.nstop, el,

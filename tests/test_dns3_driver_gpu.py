@@ -39,3 +39,19 @@ def test_dns3_driver(tmp_path):
     assert meta[0] == pytest.approx(10 * dt) and meta[1] == pytest.approx(nu)
     for a, b in zip(st, ref):
         np.testing.assert_array_equal(a, b)
+
+
+def test_dns3_driver_recurrence_files(tmp_path):
+    job = tmp_path / "JOB0"
+    job.mkdir()
+    (job / "params.txt").write_text(_params_text(TSTEP="0.2", outfreq1="0.02", DELT="0.01",
+                                                 STATSFLAG="0", RCFLAG="1"))
+    r = subprocess.run([H.driver_path(), "-n", "32", "-d", str(job), "-p", "32"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    info = (job / "UPOinfo_ts.dat").read_text().splitlines()
+    assert info[0].startswith("Guess No")
+    size = (job / "UPO_ZK.out").stat().st_size
+    nkt = 11 * 21 * 21
+    assert size % (56 + 3 * 16 * nkt) == 0 and size // (56 + 3 * 16 * nkt) == len(info) - 1
+    assert not (job / "stats.dat").exists()
