@@ -771,8 +771,19 @@ __device__ __forceinline__ void scheme_point(const Geom3<T>& g, const Regs<T>& R
 
 }
 
+// barrier of the first `count` threads of the block only (hardware barrier 1)
+struct GroupSync {
+  int count;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory");
+  }
+};
+
+// Pass E runs 2 W G threads: the first W G transform the tile (a named
+// barrier of their own), then all of them do the update, whose state loads
+// are what the pass waits on.
 template <typename T, int N, int NO, int SCHEME>
-__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, T>::G)
+__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, 3)
 pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw, Regs<T> R,
        StepParams<T> p, int stage, int* status) {
   using F = LineFFT<N, -1, T>;
@@ -816,16 +827,18 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   }
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
+  if (tid < W * F::G) {
 #pragma unroll 1
-  for (int f = 0; f < NO; ++f) {
-    cpx<T> v[F::E];
+    for (int f = 0; f < NO; ++f) {
+      cpx<T> v[F::E];
 #pragma unroll
-    for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(gi, e)) * W + c];
-    F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+      for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(gi, e)) * W + c];
+      F::run(v, gi, s_tw, s_ex + c * SX, GroupSync{W * F::G});
 #pragma unroll
-    for (int e = 0; e < F::E; ++e) {
-      const int ikz = row_to_box(F::out_index(gi, e), K, N);
-      if (ikz >= 0) s_in[(f * N + ikz) * W + c] = v[e];
+      for (int e = 0; e < F::E; ++e) {
+        const int ikz = row_to_box(F::out_index(gi, e), K, N);
+        if (ikz >= 0) s_in[(f * N + ikz) * W + c] = v[e];
+      }
     }
   }
   __syncthreads();
@@ -1635,16 +1648,16 @@ struct Engine3D final : Engine3DBase {
     const dim3 ge(XT, g.Y);
     switch (scheme) {
       case SCHEME_NS_HEUN:
-        pass_e<T, N, 3, SCHEME_NS_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        pass_e<T, N, 3, SCHEME_NS_HEUN><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       case SCHEME_EULER_HEUN:
-        pass_e<T, N, 3, SCHEME_EULER_HEUN><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        pass_e<T, N, 3, SCHEME_EULER_HEUN><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       case SCHEME_NS_RK4:
-        pass_e<T, N, 3, SCHEME_NS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        pass_e<T, N, 3, SCHEME_NS_RK4><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
         break;
       default:
-        pass_e<T, N, 4, SCHEME_BOUS_RK4><<<ge, blk, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        pass_e<T, N, 4, SCHEME_BOUS_RK4><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
     }
     mark(4);
     launches += 5;
@@ -1813,7 +1826,7 @@ struct Engine3D final : Engine3DBase {
     pass_d<T, N><<<dim3(XT, N, 3), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     Regs<T> Rr{};
     Rr.K1 = out;
-    pass_e<T, N, 3, SCHEME_RAW><<<dim3(XT, g.Y), blk, smem_e(), stream>>>(g, B2, tw, Rr, prm, 0,
+    pass_e<T, N, 3, SCHEME_RAW><<<dim3(XT, g.Y), blk2, smem_e(), stream>>>(g, B2, tw, Rr, prm, 0,
                                                                           d_status);
     launches += 5;
     PSG_CUDA_TRY(cudaGetLastError());
@@ -1836,7 +1849,7 @@ struct Engine3D final : Engine3DBase {
     Regs<T> Rr{};
     Rr.K1 = SA;
     Rr.K2 = SB;
-    pass_e<T, N, 6, SCHEME_RAW><<<dim3(XT, g.Y), blk, smem_e_no(6), stream>>>(g, B2, tw, Rr, prm, 0,
+    pass_e<T, N, 6, SCHEME_RAW><<<dim3(XT, g.Y), blk2, smem_e_no(6), stream>>>(g, B2, tw, Rr, prm, 0,
                                                                               d_status);
     launches += 5;
     PSG_CUDA_TRY(cudaGetLastError());
