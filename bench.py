@@ -225,6 +225,7 @@ def run_ours(args, rank, world, dist):
 
     upo = run_upo(args) if (world == 1 and not args.no_upo) else None
     ens = None if args.no_ensemble else run_ensemble2d(args, rank, world, dist, dev)
+    single2d = run_ns2d_single(args) if (world == 1 and not args.no_ensemble) else None
 
     out = None
     if rank == 0:
@@ -243,7 +244,7 @@ def run_ours(args, rank, world, dist):
                        "grid": N, "replicas": world, "parallelism": f"replicas{world}",
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
             "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu, "upo": upo,
-            "ensemble2d": ens,
+            "ensemble2d": ens, "ns2d_single": single2d,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
                                 "variants": ["L=128/G,1 stage", "L=256/G,1 stage",
@@ -372,6 +373,41 @@ def run_upo(args):
                    "included"}
         out["exact_vs_plain"] = round(out["exact_jv"]["newton_iters_per_s"] /
                                       out["plain_reference"]["newton_iters_per_s"], 2)
+    return out
+
+
+# --------------------------------------------- 2D Kolmogorov flow, one instance
+def run_ns2d_single(args):
+    """2D Kolmogorov flow, 128^2, nu = 1/40, dt = 0.005, 2000 RK4/CN steps, FP64,
+    seeded initial vorticity (modes 1 <= |k| <= 8, amplitude ~ 1/|k|, enstrophy
+    1): through the 2D drop-in timestep_cuda_ (host arrays in and out inside the
+    timed region), beside the reference's own 2D step (timed on a 200-step call
+    in a separate process) and the oracle's host step on a 50-step sample."""
+    import psgpu_b200 as P
+    from oracle import pyoracle as O
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import kolmogorov_ic2d
+
+    n, nu, dt, steps = 128, 1.0 / 40.0, 0.005, 2000
+    Z0 = kolmogorov_ic2d(n, 77)
+    os.environ["PSG_PRECISION"] = "64"
+    lib = TimestepLibrary(P.dropin_path("ns2d"), "ns2d")
+    lib.ns2d(Z0.copy(), n, nu, dt, 10)
+    t0 = time.perf_counter()
+    Z, _ = lib.ns2d(Z0.copy(), n, nu, dt, steps)
+    ours = time.perf_counter() - t0
+    os.environ["PSG_PRECISION"] = "32"
+    out = {"workload": "2D Kolmogorov 128^2, nu=1/40, dt=0.005, 2000 RK4/CN steps, FP64",
+           "steps_per_s": round(steps / ours, 1), "api": "timestep_cuda_ (2D ABI), e2e",
+           "finite": bool(np.isfinite(Z).all())}
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
+    if os.path.exists(path):
+        ms = ref2d_step_ms(200, n)
+        out["reference_steps_per_s"] = round(1e3 / ms, 1)
+    t0 = time.perf_counter()
+    O.ns2d_timestep(Z0.copy(), n, nu, dt, 50)
+    out["cpu_port_steps_per_s"] = round(50 / (time.perf_counter() - t0), 1)
+    out["cpu_cores"] = O.num_threads()
     return out
 
 
