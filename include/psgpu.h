@@ -40,6 +40,12 @@ int psg_version(void);
 /* building-block check: the library's line FFT on nlines contiguous lines of n
  * complex doubles (in -> out), unnormalised, sign -1 forward / +1 inverse;
  * swap selects the transposed factorisation used after another transform */
+/* Runs one block whose bounded mbarrier wait cannot succeed (a transfer that
+ * is never issued), `polls` polls long (1..2^20); *status is the status word
+ * the kernel leaves: PSG_DEVICE_TIMEOUT when the wait ran out.  The engines'
+ * waits end the same way (2^22 polls) and their sync calls report it. */
+#define PSG_DEVICE_TIMEOUT 0x7e01
+int psg_debug_wait_timeout(int polls, int* status);
 int psg_debug_linefft(int n, int sign, int swap, const double* in, double* out, int nlines);
 
 /* ---------------------------------------------------------------- 3D */

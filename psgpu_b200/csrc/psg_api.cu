@@ -28,6 +28,7 @@ extern "C" int psg_version(void) { return PSG_VERSION; }
 // line).  Used by the unit tests; unnormalised, sign -1 forward / +1 inverse.
 // ---------------------------------------------------------------------------
 #include "psg_fft.cuh"
+#include "psg_tma.cuh"
 
 namespace {
 template <int N, int SIGN, bool SWAP>
@@ -105,4 +106,39 @@ extern "C" int psg_debug_linefft(int n, int sign, int swap, const double* in, do
       return PSG_ERR_UNSUPPORTED;
   }
 #undef PSG_LF
+}
+
+// ---------------------------------------------------------------------------
+// The bounded-wait path, exercised: a block arms an mbarrier for a transfer
+// that is never issued and waits `polls` times; the wait runs out, the kernel
+// records PSG_DEV_TIMEOUT in the status word and returns (no copy is in flight,
+// so nothing outlives the block).  The host reads the status as the engines do.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void wait_nothing(int polls, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    psg::mbar_init(&bar, 1);
+    psg::mbar_expect_tx(&bar, 16);  // 16 bytes that never arrive
+    psg::mbar_wait_polls(&bar, 0, polls, status);
+  }
+}
+}  // namespace
+
+extern "C" int psg_debug_wait_timeout(int polls, int* status_out) {
+  if (polls < 1 || polls > (1 << 20) || !status_out) {
+    psg_set_error("bad arguments");
+    return PSG_ERR_ARG;
+  }
+  int* d = nullptr;
+  PSG_CUDA_TRY(cudaMalloc(&d, sizeof(int)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    wait_nothing<<<1, 32>>>(polls, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(status_out, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  PSG_CUDA_TRY(e);
+  return PSG_OK;
 }

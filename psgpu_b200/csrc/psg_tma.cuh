@@ -66,6 +66,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// the same with a caller-chosen number of polls
+__device__ __forceinline__ bool mbar_wait_polls(uint64_t* bar, uint32_t parity, int polls,
+                                                int* status) {
+  for (int i = 0; i < polls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (status) atomicExch(status, PSG_DEV_TIMEOUT);
+  return false;
+}
+
 // Block-wide load of `nchunks` contiguous chunks into shared memory through one
 // mbarrier: thread 0 arms the barrier and issues the copies, every thread waits.
 // Returns false (uniformly) when the wait timed out.
