@@ -1,0 +1,45 @@
+"""Every x-pass schedule the autotuner can pick (PSG_XPASS_VARIANT pins one;
+a variant that does not fit the device at that size is skipped) gives the
+same step as variant 1, for the RK4/CN and the Heun/CN (with the physical
+vorticity it keeps) schemes: 1e-12 in FP64, 2e-6 in FP32 (max-norm
+relative)."""
+import numpy as np
+import pytest
+
+import psgpu_b200 as P
+from psgpu_b200.fields import random_vorticity3d
+
+pytestmark = pytest.mark.gpu
+
+TOL = {64: 1e-12, 32: 2e-6}
+
+
+def _run(monkeypatch, v, n, scheme, prec):
+    monkeypatch.setenv("PSG_XPASS_VARIANT", str(v))
+    e = P.NS3D(n, scheme, precision=prec, nu=0.01, ampfor=-1.0, kf=4.0)
+    if e.autotune(rerun=False)[0] != v:
+        return None, None  # the variant does not fit: the pin is not taken
+    e.upload(*random_vorticity3d(n, 12))
+    e.step(2e-3, 3, dump_last=(scheme == P.SCHEME_NS_HEUN))
+    st = np.stack(e.download())
+    ph = e.physical() if scheme == P.SCHEME_NS_HEUN else None
+    return st, ph
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("scheme", [P.SCHEME_NS_RK4, P.SCHEME_NS_HEUN])
+@pytest.mark.parametrize("n", [32, 64])
+def test_xpass_variants_agree(monkeypatch, prec, scheme, n):
+    ref, ref_ph = _run(monkeypatch, 1, n, scheme, prec)
+    assert ref is not None
+    for v in (0, 2, 3):
+        st, ph = _run(monkeypatch, v, n, scheme, prec)
+        if st is None:
+            continue
+        assert _rel(st, ref) < TOL[prec], v
+        if ph is not None:
+            assert _rel(ph, ref_ph) < TOL[prec], v
