@@ -389,8 +389,11 @@ struct RowOps {
 // Template knobs picked by the engine's autotuner: L rows per tile (one group
 // of G lanes per row, so L*G threads) and ST pipeline stages (1: load then
 // compute; 2: the next tile's bulk copy overlaps this tile's transforms).
+// The nine-field (Boussinesq) build at 128 threads asks for three blocks per
+// SM, which caps it at 168 registers (it spills 8 bytes instead of holding
+// 255); every other build leaves the block count to the compiler (0).
 template <typename T, int N, int NF, int L, int ST>
-__global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G)
+__global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G, (NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
        const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int ntiles) {
   using R = RowOps<T, N>;
