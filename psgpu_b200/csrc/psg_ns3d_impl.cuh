@@ -114,8 +114,8 @@ __device__ __forceinline__ cpx<T> spec_op(int op, int comp, const cpx<T>* x, T k
   return r;
 }
 
-template <typename T, int N, int NC, int NF, int MODE = 0>
-__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, 3)
+template <typename T, int N, int NC, int NF, int MODE = 0, int NG = 2>
+__global__ void __launch_bounds__(NG * kTileW * LineFFT<N, 1, T>::G, NG == 2 ? 3 : 2)
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
        int mask_vel, int* status, Fields4<T> in2 = Fields4<T>{}, int ops = 0) {
   using F = LineFFT<N, +1, T>;
@@ -128,12 +128,12 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);   // [NC][Y][W]
   cpx<T>* s_mir = s_in + NC * Y * W;                      // [NC][Y] mirror column
   cpx<T>* s_tw = s_mir + NC * Y;                          // [N]
-  cpx<T>* s_ex = s_tw + N;                                // [2][W][SX]
-  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + 2 * W * SX);  // [Y][W]
+  cpx<T>* s_ex = s_tw + N;                                // [NG][W][SX]
+  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + NG * W * SX);  // [Y][W]
 
-  // two groups of W x G threads transform two output fields at a time
+  // NG groups of W x G threads transform NG output fields at a time
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int half = tid / (W * F::G), ht = tid % (W * F::G);
+  const int grp = tid / (W * F::G), ht = tid % (W * F::G);
   const int c = ht % W, gi = ht / W;
   const int xt = blockIdx.x, iky = blockIdx.y;
   const long tile = ((long)xt * Y + iky) * Y * W;
@@ -177,8 +177,8 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   const bool live_col = ikx < g.X;
   const bool mcol = mirror && c == 0;
 #pragma unroll 1
-  for (int f0 = 0; f0 < NF; f0 += 2) {
-    const int f = f0 + half;
+  for (int f0 = 0; f0 < NF; f0 += NG) {
+    const int f = f0 + grp;
     const bool live_f = f < NF;
     cpx<T> v[F::E];
 #pragma unroll
@@ -256,7 +256,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
       }
       v[e] = r;
     }
-    F::run(v, gi, s_tw, s_ex + (half * W + c) * SX, BlockSync());
+    F::run(v, gi, s_tw, s_ex + (grp * W + c) * SX, BlockSync());
     if (live_f) {
       cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
 #pragma unroll
@@ -1324,9 +1324,12 @@ struct Engine3D final : Engine3DBase {
   }
 
   // dynamic shared memory of each pass (must match the kernels' carve-up)
+  // pass A runs three groups of W x G threads for the nine Boussinesq fields
+  // (three rounds, none idle) and two for the six Navier-Stokes fields
+  int groups_a() const { return nc == 4 ? 3 : 2; }
   size_t smem_a() const {
     return sizeof(cpx<T>) * ((size_t)nc * g.Y * kTileW + (size_t)nc * g.Y + g.n +
-                             2 * kTileW * col_stride()) + g.Y * kTileW;
+                             (size_t)groups_a() * kTileW * col_stride()) + g.Y * kTileW;
   }
   size_t smem_b() const { return sizeof(cpx<T>) * ((size_t)g.Y * kTileW + g.n + kTileW * col_stride()); }
   // x-pass variants (rows per tile in units of 128/G, pipeline stages)
@@ -1470,7 +1473,7 @@ struct Engine3D final : Engine3DBase {
       }
 #define PSG_SMEM(kern) PSG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, big))
     PSG_SMEM((pass_a<T, N, 3, 6>));
-    PSG_SMEM((pass_a<T, N, 4, 9>));
+    PSG_SMEM((pass_a<T, N, 4, 9, 0, 3>));
     PSG_SMEM((pass_b<T, N>));
     PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 1>));
     PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 1>));
@@ -1636,7 +1639,8 @@ struct Engine3D final : Engine3DBase {
     mark(-1);
     const dim3 blk2(2 * kTileW * G);
     if (bous)
-      pass_a<T, N, 4, 9><<<dim3(XT, g.Y), blk2, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
+      pass_a<T, N, 4, 9, 0, 3><<<dim3(XT, g.Y), dim3(3 * kTileW * G), smem_a(), stream>>>(g, in, B1, tw,
+                                                                                       mv, d_status);
     else
       pass_a<T, N, 3, 6><<<dim3(XT, g.Y), blk2, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
     mark(0);
