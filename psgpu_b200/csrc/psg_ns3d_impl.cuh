@@ -31,6 +31,15 @@ namespace psg {
 
 constexpr int kTileW = 8;
 
+// The truncated box of an N^3 grid as compile-time constants (the engine sets
+// Geom3 to the same values: K = N/3, X = K+1, Y = 2K+1, XP = X rounded up to
+// kTileW), so that the row <-> box index arithmetic of the passes folds.
+template <int N>
+struct Box {
+  static constexpr int K = N / 3, X = K + 1, Y = 2 * K + 1;
+  static constexpr int XP = (X + kTileW - 1) / kTileW * kTileW, XT = XP / kTileW;
+};
+
 // FFT row (0..n-1) -> box index (0..2K) or -1 when the row is truncated
 __device__ __forceinline__ int row_to_box(int r, int K, int n) {
   if (r <= K) return r + K;
@@ -124,7 +133,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
-  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);   // [NC][Y][W]
   cpx<T>* s_mir = s_in + NC * Y * W;                      // [NC][Y] mirror column
   cpx<T>* s_tw = s_mir + NC * Y;                          // [N]
@@ -162,7 +171,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   for (int idx = tid; idx < Y * W; idx += nth) {
     const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
     unsigned char ll;
-    if (ikx >= g.X) ll = 0;
+    if (ikx >= Box<N>::X) ll = 0;
     else if (ikx == 0 && mirror && !(iky == K && ikz > K))  // value taken from the mirror mode
       ll = (iky == K && ikz == K) ? 0
                                   : (unsigned char)keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
@@ -174,7 +183,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   const int ikx = xt * W + c;
   const T kx = (T)ikx * g.alpha;
   const T ky = (T)(iky - K);
-  const bool live_col = ikx < g.X;
+  const bool live_col = ikx < Box<N>::X;
   const bool mcol = mirror && c == 0;
 #pragma unroll 1
   for (int f0 = 0; f0 < NF; f0 += NG) {
@@ -278,7 +287,7 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
-  const int Y = g.Y, K = g.K, XP = g.XP, XT = XP / W;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XP = Box<N>::XP, XT = Box<N>::XT;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [Y][W]
   cpx<T>* s_tw = s_in + Y * W;
   cpx<T>* s_ex = s_tw + N;
@@ -402,7 +411,7 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar[2];
   __shared__ int s_ok;
-  const int K = g.K, XP = g.XP, XT = XP / kTileW;
+  constexpr int K = Box<N>::K, XP = Box<N>::XP, XT = Box<N>::XT;
   const int tile_words = NF * L * XP;
   cpx<T>* s_buf = reinterpret_cast<cpx<T>*>(smem_raw);  // [ST][NF][L][XP]
   cpx<T>* s_tw = s_buf + ST * tile_words;                // [2N]: plain | swapped plan
@@ -520,7 +529,7 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
-  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [N][W]
   cpx<T>* s_tw = s_in + N * W;
   cpx<T>* s_ex = s_tw + N;
@@ -795,7 +804,7 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
-  const int Y = g.Y, K = g.K, XT = g.XP / W;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
   // field f's transformed rows overwrite the start of its own input tile
   // (every thread has read its inputs before the barrier inside F::run)
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NO][N][W]
@@ -847,7 +856,7 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   __syncthreads();
   for (int idx = tid; idx < Y * W; idx += nth) {
     const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
-    if (ikx >= g.X) continue;
+    if (ikx >= Box<N>::X) continue;
     const long ik = tile + idx;
     const int iy = iky - K, iz = ikz - K;
     const T kx = (T)ikx * g.alpha, ky = (T)iy, kz = (T)iz;
@@ -856,7 +865,7 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
     const cpx<T> Wv = s_in[(2 * N + ikz) * W + cc];
     const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + ikz) * W + cc] : czero<T>();
     if (SCHEME == SCHEME_RAW) {  // outputs 0-3 to K1, 4-5 to K2
-      const T LL = keep_mode<T>(ikx, iy, iz, g.K, g.alpha) ? (T)1 : (T)0;
+      const T LL = keep_mode<T>(ikx, iy, iz, Box<N>::K, g.alpha) ? (T)1 : (T)0;
 #pragma unroll
       for (int q = 0; q < NO; ++q) {
         const cpx<T> a = s_in[(q * N + ikz) * W + cc];
