@@ -130,15 +130,15 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   using F = LineFFT<N, +1, T>;
   constexpr int W = kTileW;
   constexpr int SX = ColStride<F::SMEM>::value;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
-  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);   // [NC][Y][W]
-  cpx<T>* s_mir = s_in + NC * Y * W;                      // [NC][Y] mirror column
-  cpx<T>* s_tw = s_mir + NC * Y;                          // [N]
+  cpx<T>* s_tw = s_in + NC * Y * W;                       // [N]
   cpx<T>* s_ex = s_tw + N;                                // [NG][W][SX]
-  unsigned char* s_ll = reinterpret_cast<unsigned char*>(s_ex + NG * W * SX);  // [Y][W]
+  // 1/k^2 of every mode of the tile, negated where the 2/3 rule drops the mode
+  T* s_wk = reinterpret_cast<T*>(s_ex + NG * W * SX);     // [Y][W]
 
   // NG groups of W x G threads transform NG output fields at a time
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -159,106 +159,81 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
       bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), &s_bar);
   }
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
-  // mirror column for the Hermitian completion of kx = 0 (only tile 0, ky <= 0)
   const bool mirror = (xt == 0) && (iky <= K);
-  if (mirror) {
-    const long mt = ((long)0 * Y + (2 * K - iky)) * Y * W;
-    for (int i = tid; i < NC * Y; i += nth) {
-      const int q = i / Y, ikz = i % Y;
-      s_mir[i] = src_comp(q)[mt + (long)(2 * K - ikz) * W];
-    }
-  }
   for (int idx = tid; idx < Y * W; idx += nth) {
     const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
-    unsigned char ll;
-    if (ikx >= Box<N>::X) ll = 0;
+    bool ll;
+    if (ikx >= Box<N>::X) ll = false;
     else if (ikx == 0 && mirror && !(iky == K && ikz > K))  // value taken from the mirror mode
-      ll = (iky == K && ikz == K) ? 0
-                                  : (unsigned char)keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
-    else ll = (unsigned char)keep_mode<T>(ikx, iky - K, ikz - K, K, g.alpha);
-    s_ll[idx] = ll;
+      ll = (iky == K && ikz == K) ? false : keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
+    else ll = keep_mode<T>(ikx, iky - K, ikz - K, K, g.alpha);
+    const T kx = (T)ikx * g.alpha, ky = (T)(iky - K), kz = (T)(ikz - K);
+    const T wki = wkinv(kx * kx + ky * ky + kz * kz);
+    s_wk[idx] = ll ? wki : -wki;
   }
   if (!tile_wait(&s_bar, &s_ok, status)) return;
+  // the kx = 0 column of tile 0 for ky <= 0 is the conjugate of the stored
+  // mode at (-ky, -kz) (Hermitian completion): patched into the staged tile
+  if (mirror) {
+    const long mt = (long)(2 * K - iky) * Y * W;
+    for (int i = tid; i < NC * Y; i += nth) {
+      const int q = i / Y, ikz = i % Y;
+      cpx<T>* d = s_in + q * Y * W + ikz * W;
+      if (iky == K && ikz == K) *d = czero<T>();
+      else if (!(iky == K && ikz > K)) *d = cconj(src_comp(q)[mt + (long)(2 * K - ikz) * W]);
+    }
+    __syncthreads();
+  }
 
   const int ikx = xt * W + c;
   const T kx = (T)ikx * g.alpha;
   const T ky = (T)(iky - K);
   const bool live_col = ikx < Box<N>::X;
-  const bool mcol = mirror && c == 0;
 #pragma unroll 1
   for (int f0 = 0; f0 < NF; f0 += NG) {
     const int f = f0 + grp;
-    const bool live_f = f < NF;
+    const bool live = live_col && f < NF;
     cpx<T> v[F::E];
 #pragma unroll
     for (int e = 0; e < F::E; ++e) {
       const int ikz = row_to_box(F::in_index(gi, e), K, N);
+      const int o = ikz * W + c;
       cpx<T> r = czero<T>();
-      if (MODE == 1) {
-        if (ikz >= 0 && live_col && live_f && s_ll[ikz * W + c]) {
-          const int sl = f / 3, comp = f % 3;
-          cpx<T> x[3];
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            const int q = 3 * sl + j;
-            if (mcol && !(iky == K && ikz > K)) x[j] = cconj(s_mir[q * Y + ikz]);
-            else if (mcol) x[j] = s_in[q * Y * W + ikz * W];
-            else x[j] = s_in[q * Y * W + ikz * W + c];
-          }
-          const T kz = (T)(ikz - K);
-          const T wki = wkinv(kx * kx + ky * ky + kz * kz);
-          r = spec_op<T>((ops >> (4 * sl)) & 15, comp, x, kx, ky, kz, wki);
-        }
-      } else if (MODE == 2) {
-        if (ikz >= 0 && live_col && live_f && s_ll[ikz * W + c]) {
-          auto fetch = [&](int q) -> cpx<T> {
-            if (mcol && !(iky == K && ikz > K)) return cconj(s_mir[q * Y + ikz]);
-            if (mcol) return s_in[q * Y * W + ikz * W];
-            return s_in[q * Y * W + ikz * W + c];
-          };
-          const T kz = (T)(ikz - K);
-          if (f == 0) {
-            r = fetch(4);
-          } else if (f <= 3) {  // i k_j rho
-            const cpx<T> rho = fetch(3);
-            const T kk = (f == 1) ? kx : (f == 2) ? ky : kz;
-            r = cpx<T>{-kk * rho.y, kk * rho.x};
-          } else {
-            const cpx<T> x[3] = {fetch(0), fetch(1), fetch(2)};
-            r = spec_op<T>(OP_BS, f - 4, x, kx, ky, kz, wkinv(kx * kx + ky * ky + kz * kz));
-          }
-        }
-      } else if (ikz >= 0 && live_col && live_f) {
-        cpx<T> xi, et, zt, rho;
-        if (mcol) {
-          if (iky == K && ikz == K) {
-            xi = et = zt = rho = czero<T>();
-          } else if (iky == K && ikz > K) {
-            xi = s_in[ikz * W]; et = s_in[Y * W + ikz * W]; zt = s_in[2 * Y * W + ikz * W];
-            rho = (NC > 3) ? s_in[3 * Y * W + ikz * W] : czero<T>();
-          } else {
-            xi = cconj(s_mir[ikz]); et = cconj(s_mir[Y + ikz]); zt = cconj(s_mir[2 * Y + ikz]);
-            rho = (NC > 3) ? cconj(s_mir[3 * Y + ikz]) : czero<T>();
-          }
-        } else {
-          const int o = ikz * W + c;
-          xi = s_in[o]; et = s_in[Y * W + o]; zt = s_in[2 * Y * W + o];
-          rho = (NC > 3) ? s_in[3 * Y * W + o] : czero<T>();
-        }
+      if (ikz >= 0 && live) {
         const T kz = (T)(ikz - K);
-        if (f == 0) r = xi;
-        else if (f == 1) r = et;
-        else if (f == 2) r = zt;
-        else if (f < 6) {
-          const T wk = kx * kx + ky * ky + kz * kz;
-          T wki = wkinv(wk);
-          if (mask_vel && !s_ll[ikz * W + c]) wki = (T)0;
+        const T tk = s_wk[o];
+        if (MODE == 1) {
+          if (tk > (T)0) {
+            const int sl = f / 3, comp = f % 3;
+            const cpx<T> x[3] = {s_in[(3 * sl) * Y * W + o], s_in[(3 * sl + 1) * Y * W + o],
+                                 s_in[(3 * sl + 2) * Y * W + o]};
+            r = spec_op<T>((ops >> (4 * sl)) & 15, comp, x, kx, ky, kz, tk);
+          }
+        } else if (MODE == 2) {
+          if (tk > (T)0) {
+            if (f == 0) {
+              r = s_in[4 * Y * W + o];
+            } else if (f <= 3) {  // i k_j rho
+              const cpx<T> rho = s_in[3 * Y * W + o];
+              const T kk = (f == 1) ? kx : (f == 2) ? ky : kz;
+              r = cpx<T>{-kk * rho.y, kk * rho.x};
+            } else {
+              const cpx<T> x[3] = {s_in[o], s_in[Y * W + o], s_in[2 * Y * W + o]};
+              r = spec_op<T>(OP_BS, f - 4, x, kx, ky, kz, tk);
+            }
+          }
+        } else if (f < 3) {
+          r = s_in[f * Y * W + o];
+        } else if (f < 6) {
           // u = i k x w / k^2 (3D_NavierStokes/src/kernels.h:194-201)
+          const T wki = (mask_vel && tk < (T)0) ? (T)0 : fabs(tk);
+          const cpx<T> xi = s_in[o], et = s_in[Y * W + o], zt = s_in[2 * Y * W + o];
           if (f == 3) r = cpx<T>{-(ky * zt.y - kz * et.y) * wki, -(kz * et.x - ky * zt.x) * wki};
           else if (f == 4) r = cpx<T>{-(kz * xi.y - kx * zt.y) * wki, -(kx * zt.x - kz * xi.x) * wki};
           else r = cpx<T>{-(kx * et.y - ky * xi.y) * wki, -(ky * xi.x - kx * et.x) * wki};
-        } else {
+        } else if (NC > 3) {
           // i k_j rho (setFFK, 3D_Boussinesq/src/kernels.h:75-93)
+          const cpx<T> rho = s_in[3 * Y * W + o];
           const T kk = (f == 6) ? kx : (f == 7) ? ky : kz;
           r = cpx<T>{-kk * rho.y, kk * rho.x};
         }
@@ -266,7 +241,7 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
       v[e] = r;
     }
     F::run(v, gi, s_tw, s_ex + (grp * W + c) * SX, BlockSync());
-    if (live_f) {
+    if (live) {
       cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
 #pragma unroll
       for (int e = 0; e < F::E; ++e) o[(long)F::out_index(gi, e) * Y * W] = v[e];
@@ -1336,10 +1311,7 @@ struct Engine3D final : Engine3DBase {
   // pass A runs three groups of W x G threads for the nine Boussinesq fields
   // (three rounds, none idle) and two for the six Navier-Stokes fields
   int groups_a() const { return nc == 4 ? 3 : 2; }
-  size_t smem_a() const {
-    return sizeof(cpx<T>) * ((size_t)nc * g.Y * kTileW + (size_t)nc * g.Y + g.n +
-                             (size_t)groups_a() * kTileW * col_stride()) + g.Y * kTileW;
-  }
+  size_t smem_a() const { return smem_a_nc(nc, groups_a()); }
   size_t smem_b() const { return sizeof(cpx<T>) * ((size_t)g.Y * kTileW + g.n + kTileW * col_stride()); }
   // x-pass variants (rows per tile in units of 128/G, pipeline stages)
   static constexpr int kCVariants = 4;
@@ -1752,17 +1724,15 @@ struct Engine3D final : Engine3DBase {
   }
 
   // ---------------------------------------------------------------- linearised step
-  size_t smem_a_nc(int ncin) const {
-    return sizeof(cpx<T>) * ((size_t)ncin * g.Y * kTileW + (size_t)ncin * g.Y + g.n +
-                             2 * kTileW * col_stride()) + g.Y * kTileW;
+  // pass A: staged tile [ncin][Y][W], twiddles, ng exchange groups, 1/k^2 table
+  size_t smem_a_nc(int ncin, int ng = 2) const {
+    return sizeof(cpx<T>) * ((size_t)ncin * g.Y * kTileW + g.n + (size_t)ng * kTileW * col_stride()) +
+           sizeof(T) * g.Y * kTileW;
   }
   size_t smem_e_no(int no) const {
     return sizeof(cpx<T>) * ((size_t)no * g.n * kTileW + g.n + kTileW * col_stride());
   }
-  size_t smem_pair() const {
-    return sizeof(cpx<T>) * ((size_t)6 * g.Y * kTileW + (size_t)6 * g.Y + g.n +
-                             2 * kTileW * col_stride()) + g.Y * kTileW;
-  }
+  size_t smem_pair() const { return smem_a_nc(6); }
 
   template <int N>
   int lin_attrs() {
