@@ -780,11 +780,17 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
   constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
-  // field f's transformed rows overwrite the start of its own input tile
-  // (every thread has read its inputs before the barrier inside F::run)
-  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NO][N][W]
-  cpx<T>* s_tw = s_in + NO * N * W;
-  cpx<T>* s_ex = s_tw + N;
+  // Fields are transformed last to first.  Field f's kept rows go to the last
+  // Y rows of its own input tile.  With ALIAS its exchange space is the start
+  // of that tile (its inputs are in registers by then), running on into the
+  // first rows of field f+1 (dead: already transformed, outputs further on)
+  // or, for the last field, into a pad after the tiles.
+  constexpr int EXW = W * SX, OVER = EXW > N * W ? EXW - N * W : 0;
+  constexpr bool ALIAS = OVER <= (N - Y) * W;
+  constexpr int R0 = N - Y;  // first output row
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NO][N][W] (+ pad)
+  cpx<T>* s_tw = s_in + NO * N * W + (ALIAS ? OVER : 0);
+  cpx<T>* s_ex = s_tw + N;                              // without ALIAS only
   const int tid = threadIdx.x, nth = blockDim.x, c = tid % W, gi = tid / W;
   const int xt = blockIdx.x, iky = blockIdx.y;
   if (tid == 0) mbar_init(&s_bar, 1);
@@ -816,15 +822,16 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   if (tid < W * F::G) {
 #pragma unroll 1
-    for (int f = 0; f < NO; ++f) {
+    for (int f = NO - 1; f >= 0; --f) {
       cpx<T> v[F::E];
 #pragma unroll
       for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(gi, e)) * W + c];
-      F::run(v, gi, s_tw, s_ex + c * SX, GroupSync{W * F::G});
+      if (ALIAS) GroupSync{W * F::G}();  // every input read before the exchange reuses them
+      F::run(v, gi, s_tw, (ALIAS ? s_in + f * N * W : s_ex) + c * SX, GroupSync{W * F::G});
 #pragma unroll
       for (int e = 0; e < F::E; ++e) {
         const int ikz = row_to_box(F::out_index(gi, e), K, N);
-        if (ikz >= 0) s_in[(f * N + ikz) * W + c] = v[e];
+        if (ikz >= 0) s_in[(f * N + R0 + ikz) * W + c] = v[e];
       }
     }
   }
@@ -835,15 +842,15 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
     const long ik = tile + idx;
     const int iy = iky - K, iz = ikz - K;
     const T kx = (T)ikx * g.alpha, ky = (T)iy, kz = (T)iz;
-    const cpx<T> U = s_in[(0 * N + ikz) * W + cc];
-    const cpx<T> V = s_in[(1 * N + ikz) * W + cc];
-    const cpx<T> Wv = s_in[(2 * N + ikz) * W + cc];
-    const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + ikz) * W + cc] : czero<T>();
+    const cpx<T> U = s_in[(0 * N + R0 + ikz) * W + cc];
+    const cpx<T> V = s_in[(1 * N + R0 + ikz) * W + cc];
+    const cpx<T> Wv = s_in[(2 * N + R0 + ikz) * W + cc];
+    const cpx<T> RKv = (NO > 3) ? s_in[(3 * N + R0 + ikz) * W + cc] : czero<T>();
     if (SCHEME == SCHEME_RAW) {  // outputs 0-3 to K1, 4-5 to K2
       const T LL = keep_mode<T>(ikx, iy, iz, Box<N>::K, g.alpha) ? (T)1 : (T)0;
 #pragma unroll
       for (int q = 0; q < NO; ++q) {
-        const cpx<T> a = s_in[(q * N + ikz) * W + cc];
+        const cpx<T> a = s_in[(q * N + R0 + ikz) * W + cc];
         cpx<T>* o = (q < 4) ? R.K1.c[q] : R.K2.c[q - 4];
         o[ik] = cpx<T>{LL * a.x, LL * a.y};
       }
@@ -1323,9 +1330,7 @@ struct Engine3D final : Engine3DBase {
   }
   size_t smem_c() const { return smem_c_v(c_variant); }
   size_t smem_d() const { return sizeof(cpx<T>) * ((size_t)g.n * kTileW + g.n + kTileW * col_stride()); }
-  size_t smem_e() const {
-    return sizeof(cpx<T>) * ((size_t)nfo * g.n * kTileW + g.n + kTileW * col_stride());
-  }
+  size_t smem_e() const { return smem_e_no(nfo); }
   int col_stride() const {
     switch (g.n) {
       case 16: return ColStride<LineFFT<16, 1, T>::SMEM>::value;
@@ -1729,8 +1734,13 @@ struct Engine3D final : Engine3DBase {
     return sizeof(cpx<T>) * ((size_t)ncin * g.Y * kTileW + g.n + (size_t)ng * kTileW * col_stride()) +
            sizeof(T) * g.Y * kTileW;
   }
+  // pass E: the NO input tiles, then (exchange inside the tiles) the overrun
+  // of the last field's exchange, or a separate exchange area; twiddles
   size_t smem_e_no(int no) const {
-    return sizeof(cpx<T>) * ((size_t)no * g.n * kTileW + g.n + kTileW * col_stride());
+    const long exw = (long)kTileW * col_stride(), tilew = (long)g.n * kTileW;
+    const long over = exw > tilew ? exw - tilew : 0;
+    const bool alias = over <= (long)(g.n - g.Y) * kTileW;
+    return sizeof(cpx<T>) * ((size_t)no * tilew + g.n + (alias ? over : exw));
   }
   size_t smem_pair() const { return smem_a_nc(6); }
 
