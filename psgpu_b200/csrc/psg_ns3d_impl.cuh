@@ -370,61 +370,80 @@ struct RowOps {
   }
 };
 
-// Template knobs picked by the engine's autotuner: L rows per tile (one group
-// of G lanes per row, so L*G threads) and ST pipeline stages (1: load then
-// compute; 2: the next tile's bulk copy overlaps this tile's transforms).
+// Template knobs picked by the engine's autotuner: L rows per block (one group
+// of G lanes per row, so L*G threads) and ST buffers per warp.  Every warp
+// runs its own pipeline over "warp tiles" of 32/G rows (RPW): its lane 0
+// fetches the tile's rows of every field by bulk copies into the warp's own
+// buffer and all lanes wait on the warp's mbarrier, so no warp ever waits for
+// another.  ST = 1: the next tile's copy is issued as soon as the last C2R has
+// gathered its inputs, overlapping the forward transforms and stores; ST = 2:
+// it is issued at the top of the iteration into the other buffer.
 // The nine-field (Boussinesq) build at 128 threads asks for three blocks per
 // SM, which caps it at 168 registers (it spills 8 bytes instead of holding
 // 255); every other build leaves the block count to the compiler (0).
 template <typename T, int N, int NF, int L, int ST>
 __global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G, (NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int ntiles) {
+       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt) {
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
+  constexpr int RPW = 32 / G, WPB = L / RPW;  // rows per warp tile, warps per block
+  static_assert(L % RPW == 0, "whole warps per block");
   constexpr bool BOUS = (NF == 9);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ uint64_t s_bar[2];
-  __shared__ int s_ok;
+  __shared__ uint64_t s_bar[WPB][2];
   constexpr int K = Box<N>::K, XP = Box<N>::XP, XT = Box<N>::XT;
-  const int tile_words = NF * L * XP;
-  cpx<T>* s_buf = reinterpret_cast<cpx<T>*>(smem_raw);  // [ST][NF][L][XP]
-  cpx<T>* s_tw = s_buf + ST * tile_words;                // [2N]: plain | swapped plan
+  constexpr int wtile_words = NF * RPW * XP;
+  cpx<T>* s_buf = reinterpret_cast<cpx<T>*>(smem_raw);  // [WPB][ST][NF][RPW][XP]
+  cpx<T>* s_tw = s_buf + WPB * ST * wtile_words;         // [2N]: plain | swapped plan
   cpx<T>* s_ex = s_tw + 2 * N;                           // [L][SX]
-  const int tid = threadIdx.x, lr = tid / G, gi = tid % G;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int j = lane / G, gi = lane % G;
+  cpx<T>* s_w = s_buf + warp * ST * wtile_words;  // this warp's buffers
+  uint64_t* bar = s_bar[warp];
   const long plane = (long)N * N * XP;
-  const uint32_t bytes = (uint32_t)(L * XP * sizeof(cpx<T>));
-  if (tid == 0) { mbar_init(&s_bar[0], 1); mbar_init(&s_bar[1], 1); }
+  const uint32_t bytes = (uint32_t)(RPW * XP * sizeof(cpx<T>));
+  if (lane == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); }
   for (int i = tid; i < 2 * N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
-  // tile t = rows [t*L, t*L + L) of every field, one bulk copy per field
+  // warp tile t = rows [t*RPW, t*RPW + RPW) of every field, one bulk copy per
+  // field; the buffer's earlier contents were read by this warp's lanes before
+  // the __syncwarp that precedes every call
   auto issue = [&](int t, int b) {
-    mbar_expect_tx(&s_bar[b], NF * bytes);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[b], NF * bytes);
     for (int f = 0; f < NF; ++f)
-      bulk_g2s(s_buf + b * tile_words + f * L * XP, in + f * plane + (long)t * L * XP, bytes, &s_bar[b]);
+      bulk_g2s(s_w + b * wtile_words + f * RPW * XP, in + f * plane + (long)t * RPW * XP, bytes,
+               &bar[b]);
   };
-  int t = blockIdx.x;
-  if (tid == 0 && t < ntiles) issue(t, 0);
+  const int wstride = gridDim.x * WPB;
+  int t = blockIdx.x * WPB + warp;
+  if (lane == 0 && t < nwt) issue(t, 0);
   const long tstride = (long)N * N * kTileW;  // B3: successive xt tiles
   const long fstride = (long)XT * tstride;
-  cpx<T>* ex = s_ex + lr * R::SX;
-  for (int i = 0; t < ntiles; ++i, t += gridDim.x) {
+  cpx<T>* ex = s_ex + (warp * RPW + j) * R::SX;
+  for (int i = 0; t < nwt; ++i, t += wstride) {
     const int b = (ST == 2) ? (i & 1) : 0;
     const uint32_t parity = (ST == 2) ? ((i >> 1) & 1) : (i & 1);
-    const int tn = t + gridDim.x;
-    // two stages: buffer b^1 was released at the end of iteration i-1
-    if (ST == 2 && tid == 0 && tn < ntiles) issue(tn, b ^ 1);
-    if (tid == 0) s_ok = mbar_wait_bounded(&s_bar[b], parity, status) ? 1 : 0;
-    __syncthreads();
-    if (!s_ok) {
-      if (ST == 2 && tid == 0 && tn < ntiles)
-        mbar_wait_bounded(&s_bar[b ^ 1], ((i + 1) >> 1) & 1, nullptr);
+    const int tn = t + wstride;
+    // two buffers: buffer b^1 was released by the __syncwarp ending iteration i-1
+    if (ST == 2 && lane == 0 && tn < nwt) issue(tn, b ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[b], parity, status);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (ST == 2 && lane == 0 && tn < nwt) mbar_wait_bounded(&bar[b ^ 1], ((i + 1) >> 1) & 1, nullptr);
       return;
     }
-    const long row = (long)t * L + lr;
+    // one buffer: free once the last C2R has gathered its rows
+    auto release = [&]() {
+      if (ST == 1) {
+        __syncwarp();
+        if (lane == 0 && tn < nwt) issue(tn, 0);
+      }
+    };
+    const long row = (long)t * RPW + j;
     const int z = (int)(row / N), y = (int)(row % N);
-    const cpx<T>* src = s_buf + b * tile_words + lr * XP;
-    const int fs = L * XP;  // field stride in shared memory
+    const cpx<T>* src = s_w + b * wtile_words + j * XP;
+    constexpr int fs = RPW * XP;  // field stride in shared memory
     cpx<T>* dst = out + ((long)z * N + y) * kTileW;
     const cpx<T>* two = s_tw + N;  // swapped plan for the forward transforms
     if (NF == 7) {
@@ -442,17 +461,18 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
       for (int e = 0; e < E; ++e) { p0[e] = ps[e] * ga[e] * scale; p1[e] = ps[e] * gb[e] * scale; }
       R::r2c_pair(p2, p0, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
       R::c2r_pair(src + 6 * fs, nullptr, K, gi, s_tw, ex, ga, gb);
+      release();
 #pragma unroll
       for (int e = 0; e < E; ++e) p2[e] = ps[e] * ga[e] * scale;
       R::r2c_pair(p1, p2, K, XP, gi, two, ex, dst + 4 * fstride, dst + 5 * fstride, tstride);
-      __syncthreads();  // release buffer b
-      if (ST == 1 && tid == 0 && tn < ntiles) issue(tn, 0);
+      __syncwarp();
       continue;
     }
     T xi[E], et[E], zt[E], u[E], v[E], w[E];
     R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
     R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
     R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
+    if (!BOUS) release();
     if (dump) {
       const long base = row * N;
       const long nr = (long)N * N * N;
@@ -481,13 +501,13 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
 #pragma unroll
       for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
       R::c2r_pair(src + 8 * fs, nullptr, K, gi, s_tw, ex, rx, ry);
+      release();
 #pragma unroll
       for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
       R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
       R::r2c_pair(n3, n4, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
     }
-    __syncthreads();  // release buffer b
-    if (ST == 1 && tid == 0 && tn < ntiles) issue(tn, 0);
+    __syncwarp();
   }
 }
 
@@ -1506,16 +1526,18 @@ struct Engine3D final : Engine3DBase {
   // Boussinesq adjoint's scalar products); 0: the engine's own
   int launch_c(int v, T scale, T* dp, int nf = 0) {
     constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
-    const int rows = L1 * c_rows_mult(v);
-    const int ntiles = (N * N) / rows;
-    const int grid = ntiles < c_resident[v] ? ntiles : c_resident[v];
+    constexpr int RPW = 32 / LineFFT<N, 1, T>::G;  // rows per warp tile
+    const int wpb = L1 * c_rows_mult(v) / RPW;     // warps per block
+    const int nwt = (N * N) / RPW;
+    const int nblk = (nwt + wpb - 1) / wpb;
+    const int grid = nblk < c_resident[v] ? nblk : c_resident[v];
     const size_t sm = smem_c_v(v);
     const int th = c_threads<N>(v);
     if (!nf) nf = (scheme == SCHEME_BOUS_RK4) ? 9 : 6;
 #define PSG_LC(LL, STG)                                                                          \
-  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
-  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles); \
-  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, ntiles);
+  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt); \
+  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt); \
+  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt);
     switch (v) {
       case 0: PSG_LC(L1, 1); break;
       case 1: PSG_LC(2 * L1, 1); break;
