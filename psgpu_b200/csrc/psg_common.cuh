@@ -33,6 +33,14 @@ struct BlockSync {
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
+// barrier of `count` threads (whole warps) on hardware barrier `id` (1..15;
+// 0 is the one __syncthreads uses)
+struct NamedSync {
+  int id, count;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+  }
+};
 
 }  // namespace psg
 

@@ -240,7 +240,8 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
       }
       v[e] = r;
     }
-    F::run(v, gi, s_tw, s_ex + (grp * W + c) * SX, BlockSync());
+    // each group syncs only its own threads (barrier 1 + grp)
+    F::run(v, gi, s_tw, s_ex + (grp * W + c) * SX, NamedSync{1 + grp, W * F::G});
     if (live) {
       cpx<T>* o = out + ((((long)f * XT + xt) * N) * Y + iky) * W + c;
 #pragma unroll
@@ -786,9 +787,9 @@ struct GroupSync {
   }
 };
 
-// Pass E runs 2 W G threads: the first W G transform the tile (a named
-// barrier of their own), then all of them do the update, whose state loads
-// are what the pass waits on.
+// Pass E runs 2 W G threads: for three fields both halves transform the tile,
+// for more the first half alone (named barriers of their own), then all of
+// them do the update, whose state loads are what the pass waits on.
 template <typename T, int N, int NO, int SCHEME>
 __global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, 3)
 pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw, Regs<T> R,
@@ -810,8 +811,9 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   constexpr int R0 = N - Y;  // first output row
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NO][N][W] (+ pad)
   cpx<T>* s_tw = s_in + NO * N * W + (ALIAS ? OVER : 0);
-  cpx<T>* s_ex = s_tw + N;                              // without ALIAS only
-  const int tid = threadIdx.x, nth = blockDim.x, c = tid % W, gi = tid / W;
+  constexpr int TG = (NO == 3) ? 2 : 1;                // transform groups
+  cpx<T>* s_ex = s_tw + N;  // without ALIAS: the first group's; then the second's
+  const int tid = threadIdx.x, nth = blockDim.x, c = tid % W;
   const int xt = blockIdx.x, iky = blockIdx.y;
   if (tid == 0) mbar_init(&s_bar, 1);
   __syncthreads();
@@ -840,19 +842,29 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   }
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
-  if (tid < W * F::G) {
+  // three fields: both halves transform (fields 2 and 1, then 0), the second
+  // half in an exchange area of its own; more fields: the first half alone
+  const int tg = tid / (W * F::G), tl = (tid % (W * F::G)) / W;  // group, lane group in it
+  if (tg < TG) {
 #pragma unroll 1
-    for (int f = NO - 1; f >= 0; --f) {
-      cpx<T> v[F::E];
+    for (int r = 0; r < (NO + TG - 1) / TG; ++r) {
+      const int f = NO - 1 - r * TG - tg;
+      if (f >= 0) {
+        cpx<T> v[F::E];
 #pragma unroll
-      for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(gi, e)) * W + c];
-      if (ALIAS) GroupSync{W * F::G}();  // every input read before the exchange reuses them
-      F::run(v, gi, s_tw, (ALIAS ? s_in + f * N * W : s_ex) + c * SX, GroupSync{W * F::G});
+        for (int e = 0; e < F::E; ++e) v[e] = s_in[(f * N + F::in_index(tl, e)) * W + c];
+        const NamedSync gs{1 + tg, W * F::G};
+        cpx<T>* exb = (tg == 0) ? (ALIAS ? s_in + f * N * W : s_ex) : s_ex + (ALIAS ? 0 : W * SX);
+        if (ALIAS && tg == 0) gs();  // every input read before the exchange reuses them
+        F::run(v, tl, s_tw, exb + c * SX, gs);
 #pragma unroll
-      for (int e = 0; e < F::E; ++e) {
-        const int ikz = row_to_box(F::out_index(gi, e), K, N);
-        if (ikz >= 0) s_in[(f * N + R0 + ikz) * W + c] = v[e];
+        for (int e = 0; e < F::E; ++e) {
+          const int ikz = row_to_box(F::out_index(tl, e), K, N);
+          if (ikz >= 0) s_in[(f * N + R0 + ikz) * W + c] = v[e];
+        }
       }
+      // a round's exchange runs into the previous round's tile
+      if (TG > 1) NamedSync{1 + TG, TG * W * F::G}();
     }
   }
   __syncthreads();
@@ -1757,12 +1769,14 @@ struct Engine3D final : Engine3DBase {
            sizeof(T) * g.Y * kTileW;
   }
   // pass E: the NO input tiles, then (exchange inside the tiles) the overrun
-  // of the last field's exchange, or a separate exchange area; twiddles
+  // of the last field's exchange, or a separate exchange area; twiddles; the
+  // second transform group's exchange area
   size_t smem_e_no(int no) const {
     const long exw = (long)kTileW * col_stride(), tilew = (long)g.n * kTileW;
     const long over = exw > tilew ? exw - tilew : 0;
     const bool alias = over <= (long)(g.n - g.Y) * kTileW;
-    return sizeof(cpx<T>) * ((size_t)no * tilew + g.n + (alias ? over : exw));
+    const int tg = (no == 3) ? 2 : 1;  // transform groups (one exchange area each)
+    return sizeof(cpx<T>) * ((size_t)no * tilew + g.n + (alias ? over + (tg - 1) * exw : tg * exw));
   }
   size_t smem_pair() const { return smem_a_nc(6); }
 
@@ -1773,7 +1787,8 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&big, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     big -= 1024;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
-    const size_t need = std::max(smem_pair(), bous ? std::max(smem_a_nc(5), smem_e_no(6)) : 0);
+    const size_t need = std::max(std::max(smem_pair(), smem_e_no(3)),
+                                 bous ? std::max(smem_a_nc(5), smem_e_no(6)) : (size_t)0);
     if (need > (size_t)big) {
       psg_set_error("linearised step at grid %d needs %zu bytes of shared memory per block", g.n,
                     need);
@@ -1844,7 +1859,7 @@ struct Engine3D final : Engine3DBase {
     pass_d<T, N><<<dim3(XT, N, 3), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     Regs<T> Rr{};
     Rr.K1 = out;
-    pass_e<T, N, 3, SCHEME_RAW><<<dim3(XT, g.Y), blk2, smem_e(), stream>>>(g, B2, tw, Rr, prm, 0,
+    pass_e<T, N, 3, SCHEME_RAW><<<dim3(XT, g.Y), blk2, smem_e_no(3), stream>>>(g, B2, tw, Rr, prm, 0,
                                                                           d_status);
     launches += 5;
     PSG_CUDA_TRY(cudaGetLastError());
