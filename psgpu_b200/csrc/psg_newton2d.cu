@@ -32,20 +32,20 @@ using C2 = cpx<double>;
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-// the same integrations with two blocks per instance (a cluster of two),
-// for batches too small to fill the device one block per instance; cluster c
+// the same integrations with CS blocks per instance (a cluster of CS), for
+// batches too small to fill the device one block per instance; cluster c
 // takes instances c, c + C, ... (all blocks run the same instance sequence)
-template <int N>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256)
+template <int N, int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(256)
     tan2d_cluster(const InstTan2D<double>* __restrict__ insts, int ninst,
                   const C2* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2* smem = reinterpret_cast<C2*>(smem_raw);
   unsigned rank;
   asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  const Team t{(int)rank, 2};
-  const int ncl = gridDim.x / 2;
-  for (int i = blockIdx.x / 2; i < ninst; i += ncl) Tan2D<double, N>::run(insts[i], tw, smem, t);
+  const Team t{(int)rank, CS};
+  const int ncl = gridDim.x / CS;
+  for (int i = blockIdx.x / CS; i < ninst; i += ncl) Tan2D<double, N>::run(insts[i], tw, smem, t);
 }
 
 template <int N>
@@ -326,8 +326,8 @@ struct Upo2D {
   size_t smem = 0;
   long launches = 0, integrations = 0;
   int grid_cap = 148;
-  // two blocks per instance when the batch leaves room (PSG_UPO_PAIRS=0: one)
-  int cluster_pairs = 1;
+  // blocks per instance (a cluster) when the batch leaves room: at most this many
+  int cluster_max = 4;
 
   ~Upo2D() {
     if (pool) cudaFree(pool);
@@ -407,25 +407,32 @@ struct Upo2D {
     }
     smem = sizeof(C2) * (2 * n + (256 / gg) * sm);
     PSG_CUDA_TRY(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(cluster_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PSG_CUDA_TRY(cudaFuncSetAttribute(cluster_kernel(2), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    PSG_CUDA_TRY(cudaFuncSetAttribute(cluster_kernel(4), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     int dev = 0, nsm = 148, occ = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(), 256, smem);
     grid_cap = nsm * std::max(occ, 1);
-    if (const char* e = getenv("PSG_UPO_PAIRS")) cluster_pairs = atoi(e) != 0;
+    // PSG_UPO_CLUSTER: the largest cluster an integration may use (1, 2 or 4)
+    if (const char* e = getenv("PSG_UPO_CLUSTER")) cluster_max = atoi(e);
     return PSG_OK;
   }
 
-  const void* cluster_kernel() const {
+  template <int CS>
+  const void* cluster_kernel_cs() const {
     switch (n) {
-      case 16: return (const void*)tan2d_cluster<16>;
-      case 32: return (const void*)tan2d_cluster<32>;
-      case 64: return (const void*)tan2d_cluster<64>;
-      case 128: return (const void*)tan2d_cluster<128>;
-      default: return (const void*)tan2d_cluster<256>;
+      case 16: return (const void*)tan2d_cluster<16, CS>;
+      case 32: return (const void*)tan2d_cluster<32, CS>;
+      case 64: return (const void*)tan2d_cluster<64, CS>;
+      case 128: return (const void*)tan2d_cluster<128, CS>;
+      default: return (const void*)tan2d_cluster<256, CS>;
     }
+  }
+  const void* cluster_kernel(int cs) const {
+    return cs == 4 ? cluster_kernel_cs<4>() : cluster_kernel_cs<2>();
   }
 
   const void* kernel() const {
@@ -478,15 +485,26 @@ struct Upo2D {
                                  cudaMemcpyHostToDevice, stream));
     PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
     const int ni = (int)h.size();
-    if (cluster_pairs && 2 * ni <= grid_cap) {
-      // room for two blocks per instance
-      const int cgrid = 2 * ni;
-      switch (n) {
-        case 16: tan2d_cluster<16><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-        case 32: tan2d_cluster<32><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-        case 64: tan2d_cluster<64><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-        case 128: tan2d_cluster<128><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-        default: tan2d_cluster<256><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+    if (cluster_max >= 2 && 2 * ni <= grid_cap) {
+      // room for four (else two) blocks per instance
+      const int cs = (cluster_max >= 4 && 4 * ni <= grid_cap) ? 4 : 2;
+      const int cgrid = cs * ni;
+      if (cs == 4) {
+        switch (n) {
+          case 16: tan2d_cluster<16, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 32: tan2d_cluster<32, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 64: tan2d_cluster<64, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 128: tan2d_cluster<128, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          default: tan2d_cluster<256, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+        }
+      } else {
+        switch (n) {
+          case 16: tan2d_cluster<16, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 32: tan2d_cluster<32, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 64: tan2d_cluster<64, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 128: tan2d_cluster<128, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          default: tan2d_cluster<256, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+        }
       }
       ++launches;
       integrations += (long)ni;

@@ -80,3 +80,23 @@ def test_newton_converges_to_laminar_state(exact):
         assert r["status"] == "CONVERGED", r
         assert r["residual"] <= 1e-10
         assert relerr(r["Z"], lam) < 1e-8
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_cluster_sizes_give_the_same_integration(n, monkeypatch):
+    """One, two or four blocks per guess (PSG_UPO_CLUSTER) split the same
+    per-column and per-row work differently: Phi_T(z) and the exact tangent
+    must come out bit for bit the same."""
+    nu, dt, T = 1 / 40, 0.005, 0.1
+    Z = kolmogorov_ic2d(n, 7) * 2.0
+    q = _masked_random(n, 8)
+    out = {}
+    for cs in ("1", "2", "4"):
+        monkeypatch.setenv("PSG_UPO_CLUSTER", cs)
+        u = P.UPO2D(2, n, kmax=4)
+        u.set_guess(0, Z, T=T, nu=nu, dt=dt)
+        u.set_guess(1, Z, T=T, nu=nu, dt=dt)
+        out[cs] = u.apply(1, 0, q)
+    for cs in ("2", "4"):
+        np.testing.assert_array_equal(out[cs][0], out["1"][0])
+        np.testing.assert_array_equal(out[cs][1], out["1"][1])
