@@ -331,7 +331,8 @@ struct RowOps {
   }
 
   // forward transform of two real signals p, q (q == nullptr: p alone); writes
-  // P_k, Q_k for k < XP into the [xt][..][W] layout (zero beyond K)
+  // P_k, Q_k for k < XP into the [xt][..][W] layout (zero beyond K).  With q,
+  // p and q come pre-scaled by 1/2 (exact), which is the 1/2 of the split.
   static __device__ __forceinline__ void r2c_pair(const T (&p)[E], const T* q, int K, int XP,
                                                   int gi, const cpx<T>* tw, cpx<T>* ex,
                                                   cpx<T>* __restrict__ P, cpx<T>* __restrict__ Q,
@@ -352,8 +353,8 @@ struct RowOps {
           if (k <= K) {
             const cpx<T> a = v[e], b = ex[(N - k) & (N - 1)];
             // P = (Z_k + conj Z_{N-k}) / 2,  Q = -i (Z_k - conj Z_{N-k}) / 2
-            pk = cpx<T>{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
-            qk = cpx<T>{(T)0.5 * (a.y + b.y), (T)(-0.5) * (a.x - b.x)};
+            pk = cpx<T>{a.x + b.x, a.y - b.y};
+            qk = cpx<T>{a.y + b.y, b.x - a.x};
           }
           const long o = (long)(k / kTileW) * tstride + (k % kTileW);
           P[o] = pk;
@@ -447,24 +448,25 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     constexpr int fs = RPW * XP;  // field stride in shared memory
     cpx<T>* dst = out + ((long)z * N + y) * kTileW;
     const cpx<T>* two = s_tw + N;  // swapped plan for the forward transforms
+    const T hscale = (T)0.5 * scale;  // products of a paired forward transform
     if (NF == 7) {
       // scalar products of the Boussinesq adjoint: psi * (i k rho), psi * u
       T ps[E], ga[E], gb[E], p0[E], p1[E], p2[E];
       R::c2r_pair(src, src + fs, K, gi, s_tw, ex, ps, ga);
 #pragma unroll
-      for (int e = 0; e < E; ++e) p0[e] = ps[e] * ga[e] * scale;
+      for (int e = 0; e < E; ++e) p0[e] = ps[e] * ga[e] * hscale;
       R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, ga, gb);
 #pragma unroll
-      for (int e = 0; e < E; ++e) { p1[e] = ps[e] * ga[e] * scale; p2[e] = ps[e] * gb[e] * scale; }
+      for (int e = 0; e < E; ++e) { p1[e] = ps[e] * ga[e] * hscale; p2[e] = ps[e] * gb[e] * hscale; }
       R::r2c_pair(p0, p1, K, XP, gi, two, ex, dst, dst + fstride, tstride);
       R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, ga, gb);
 #pragma unroll
-      for (int e = 0; e < E; ++e) { p0[e] = ps[e] * ga[e] * scale; p1[e] = ps[e] * gb[e] * scale; }
+      for (int e = 0; e < E; ++e) { p0[e] = ps[e] * ga[e] * hscale; p1[e] = ps[e] * gb[e] * hscale; }
       R::r2c_pair(p2, p0, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
       R::c2r_pair(src + 6 * fs, nullptr, K, gi, s_tw, ex, ga, gb);
       release();
 #pragma unroll
-      for (int e = 0; e < E; ++e) p2[e] = ps[e] * ga[e] * scale;
+      for (int e = 0; e < E; ++e) p2[e] = ps[e] * ga[e] * hscale;
       R::r2c_pair(p1, p2, K, XP, gi, two, ex, dst + 4 * fstride, dst + 5 * fstride, tstride);
       __syncwarp();
       continue;
@@ -489,9 +491,9 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       // U,V,W <- -(u x w)  (multReal)
-      n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * scale;
-      n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * scale;
-      n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * scale;
+      n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * hscale;
+      n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * hscale;
+      n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * (BOUS ? hscale : scale);
     }
     if (!BOUS) {
       R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
@@ -504,7 +506,7 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
       R::c2r_pair(src + 8 * fs, nullptr, K, gi, s_tw, ex, rx, ry);
       release();
 #pragma unroll
-      for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * scale;
+      for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * hscale;
       R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
       R::r2c_pair(n3, n4, K, XP, gi, two, ex, dst + 2 * fstride, dst + 3 * fstride, tstride);
     }
