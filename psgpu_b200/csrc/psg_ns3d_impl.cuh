@@ -124,7 +124,8 @@ __device__ __forceinline__ cpx<T> spec_op(int op, int comp, const cpx<T>* x, T k
 }
 
 template <typename T, int N, int NC, int NF, int MODE = 0, int NG = 2>
-__global__ void __launch_bounds__(NG * kTileW * LineFFT<N, 1, T>::G, NG == 2 ? 3 : 2)
+__global__ void __launch_bounds__(NG * kTileW * LineFFT<N, 1, T>::G,
+                                  sizeof(T) > 4 ? (N >= 256 ? 1 : 2) : (NG == 2 ? 3 : 2))
 pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __restrict__ tw,
        int mask_vel, int* status, Fields4<T> in2 = Fields4<T>{}, int ops = 0) {
   using F = LineFFT<N, +1, T>;
@@ -380,11 +381,15 @@ struct RowOps {
 // another.  ST = 1: the next tile's copy is issued as soon as the last C2R has
 // gathered its inputs, overlapping the forward transforms and stores; ST = 2:
 // it is issued at the top of the iteration into the other buffer.
-// The nine-field (Boussinesq) build at 128 threads asks for three blocks per
-// SM, which caps it at 168 registers (it spills 8 bytes instead of holding
-// 255); every other build leaves the block count to the compiler (0).
+// The nine-field (Boussinesq) FP32 build at 128 threads asks for three blocks
+// per SM, which caps it at 168 registers (it spills 8 bytes instead of holding
+// 255); every other build, FP64 included (one block per SM by its shared
+// memory), leaves the block count to the compiler (0).  Passes A and E in
+// FP64 at 256^3 likewise ask for one block per SM: their shared memory allows
+// no more, and the register cap of three would only make them spill.
 template <typename T, int N, int NF, int L, int ST>
-__global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G, (NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
+__global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G,
+                                  (sizeof(T) == 4 && NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
        const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt) {
   using R = RowOps<T, N>;
@@ -793,7 +798,7 @@ struct GroupSync {
 // for more the first half alone (named barriers of their own), then all of
 // them do the update, whose state loads are what the pass waits on.
 template <typename T, int N, int NO, int SCHEME>
-__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, 3)
+__global__ void __launch_bounds__(2 * kTileW * LineFFT<N, 1, T>::G, sizeof(T) > 4 ? (N >= 256 ? 1 : 2) : 3)
 pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw, Regs<T> R,
        StepParams<T> p, int stage, int* status) {
   using F = LineFFT<N, -1, T>;
