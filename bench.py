@@ -22,6 +22,8 @@ scheme, 3D_Boussinesq/src/kernels.h:331-621, at Ri = 0).  Data are synthetic
 * ``roofline``: the dominant pass (largest share of the step's device time),
   its algorithmic HBM bytes per launch over its average CUDA-event duration,
   against the measured copy bandwidth in MEASURED_PEAKS.json.
+* ``fp64_engine``: device steps/s of the same workload on the FP64 engine (the
+  reference's precision), Navier-Stokes RK4/CN and Boussinesq at Ri = 0.
 
 The device working set (state, stage registers, transform buffers: ~0.8 GB)
 is far larger than the 126 MB L2, so every pass streams from HBM; no L2 flush
@@ -223,6 +225,7 @@ def run_ours(args, rank, world, dist):
     e2e = None if args.no_e2e else run_e2e(args, dev, dist, world, rank)
     eng.close()
 
+    same_prec = run_fp64(args, dev, stream) if world == 1 and not args.no_fp64 else None
     upo = run_upo(args) if (world == 1 and not args.no_upo) else None
     ens = None if args.no_ensemble else run_ensemble2d(args, rank, world, dist, dev)
     single2d = run_ns2d_single(args) if (world == 1 and not args.no_ensemble) else None
@@ -244,14 +247,45 @@ def run_ours(args, rank, world, dist):
                        "grid": N, "replicas": world, "parallelism": f"replicas{world}",
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
             "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu, "upo": upo,
-            "ensemble2d": ens, "ns2d_single": single2d,
+            "ensemble2d": ens, "ns2d_single": single2d, "fp64_engine": same_prec,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
-                                "variants": ["L=128/G,1 stage", "L=256/G,1 stage",
-                                             "L=128/G,2 stages", "L=256/G,2 stages"]},
+                                "variants": ["L=128/G,1 buffer per warp", "L=256/G,1 buffer per warp",
+                                             "L=128/G,2 buffers per warp",
+                                             "L=256/G,2 buffers per warp"]},
         }
         if out_note:
             out["note"] = out_note
+    return out
+
+
+def run_fp64(args, dev, stream, nsteps=20):
+    """The same workload on the FP64 engine (the reference's precision), device
+    steps/s for the Navier-Stokes RK4/CN scheme and the Boussinesq scheme at
+    Ri = 0 that the reference arm runs."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.fields import taylor_green3d
+
+    xi, et, zt = taylor_green3d(N, 1234, amp=1e-3)
+    out = {}
+    for name, scheme, comps in (("ns_rk4", P.SCHEME_NS_RK4, (xi, et, zt)),
+                                ("boussinesq_ri0", P.SCHEME_BOUS_RK4,
+                                 (xi, et, zt, np.zeros_like(xi)))):
+        eng = P.NS3D(N, scheme, precision=64, nu=NU)
+        eng.set_stream(stream.cuda_stream)
+        eng.upload(*comps)
+        eng.step(DT, 3)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.step(DT, nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        eng.close()
+        out[name + "_steps_per_s"] = round(nsteps / (e0.elapsed_time(e1) / 1e3), 2)
+    out["steps"] = nsteps
     return out
 
 
@@ -803,6 +837,7 @@ def main():
     ap.add_argument("--ref2d-probe", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--grid2d", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 2D ensemble leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-engine leg")
     ap.add_argument("--no-ref", action="store_true",
                     help="accuracy study without the reference FP64 run")
     args = ap.parse_args()
