@@ -265,9 +265,10 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
   constexpr int Y = Box<N>::Y, K = Box<N>::K, XP = Box<N>::XP, XT = Box<N>::XT;
+  // the staged tile, then (every input in registers) the exchange space
+  constexpr int AREA = Y * W > W * SX ? Y * W : W * SX;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [Y][W]
-  cpx<T>* s_tw = s_in + Y * W;
-  cpx<T>* s_ex = s_tw + N;
+  cpx<T>* s_tw = s_in + AREA;
   const int tid = threadIdx.x, c = tid % W, gi = tid / W;
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
   if (tid == 0) mbar_init(&s_bar, 1);
@@ -285,7 +286,8 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     const int iky = row_to_box(F::in_index(gi, e), K, N);
     v[e] = iky >= 0 ? s_in[iky * W + c] : czero<T>();
   }
-  F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+  __syncthreads();
+  F::run(v, gi, s_tw, s_in + c * SX, BlockSync());
   cpx<T>* dst = out + (((long)f * N + z) * N) * XP + xt * W + c;
 #pragma unroll
   for (int e = 0; e < F::E; ++e) dst[(long)F::out_index(gi, e) * XP] = v[e];
@@ -533,9 +535,10 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   __shared__ uint64_t s_bar;
   __shared__ int s_ok;
   constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
+  // the staged tile, then (every input in registers) the exchange space
+  constexpr int AREA = N * W > W * SX ? N * W : W * SX;
   cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [N][W]
-  cpx<T>* s_tw = s_in + N * W;
-  cpx<T>* s_ex = s_tw + N;
+  cpx<T>* s_tw = s_in + AREA;
   const int tid = threadIdx.x, c = tid % W, gi = tid / W;
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
   if (tid == 0) mbar_init(&s_bar, 1);
@@ -550,7 +553,8 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   cpx<T> v[F::E];
 #pragma unroll
   for (int e = 0; e < F::E; ++e) v[e] = s_in[F::in_index(gi, e) * W + c];
-  F::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+  __syncthreads();
+  F::run(v, gi, s_tw, s_in + c * SX, BlockSync());
   // B4[f][xt][ky][z][W]
   cpx<T>* dst = out + (((long)f * XT + xt) * Y * N + z) * W + c;
 #pragma unroll
@@ -1358,7 +1362,10 @@ struct Engine3D final : Engine3DBase {
   // (three rounds, none idle) and two for the six Navier-Stokes fields
   int groups_a() const { return nc == 4 ? 3 : 2; }
   size_t smem_a() const { return smem_a_nc(nc, groups_a()); }
-  size_t smem_b() const { return sizeof(cpx<T>) * ((size_t)g.Y * kTileW + g.n + kTileW * col_stride()); }
+  // passes B and D: one area for the staged tile and then the exchange; twiddles
+  size_t smem_b() const {
+    return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.Y * kTileW, (size_t)kTileW * col_stride()) + g.n);
+  }
   // x-pass variants (rows per tile in units of 128/G, pipeline stages)
   static constexpr int kCVariants = 4;
   static int c_rows_mult(int v) { return (v & 1) ? 2 : 1; }
@@ -1368,7 +1375,9 @@ struct Engine3D final : Engine3DBase {
     return sizeof(cpx<T>) * ((size_t)c_stages(v) * nfi * L * g.XP + 2 * g.n + L * row_stride());
   }
   size_t smem_c() const { return smem_c_v(c_variant); }
-  size_t smem_d() const { return sizeof(cpx<T>) * ((size_t)g.n * kTileW + g.n + kTileW * col_stride()); }
+  size_t smem_d() const {
+    return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.n * kTileW, (size_t)kTileW * col_stride()) + g.n);
+  }
   size_t smem_e() const { return smem_e_no(nfo); }
   int col_stride() const {
     switch (g.n) {
