@@ -1366,7 +1366,7 @@ struct Engine3D final : Engine3DBase {
   size_t smem_b() const {
     return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.Y * kTileW, (size_t)kTileW * col_stride()) + g.n);
   }
-  // x-pass variants (rows per tile in units of 128/G, pipeline stages)
+  // x-pass variants (rows per block in units of 128/G, buffers per warp)
   static constexpr int kCVariants = 4;
   static int c_rows_mult(int v) { return (v & 1) ? 2 : 1; }
   static int c_stages(int v) { return (v & 2) ? 2 : 1; }
@@ -1374,7 +1374,6 @@ struct Engine3D final : Engine3DBase {
     const size_t L = (size_t)(128 / fft_g()) * c_rows_mult(v);
     return sizeof(cpx<T>) * ((size_t)c_stages(v) * nfi * L * g.XP + 2 * g.n + L * row_stride());
   }
-  size_t smem_c() const { return smem_c_v(c_variant); }
   size_t smem_d() const {
     return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.n * kTileW, (size_t)kTileW * col_stride()) + g.n);
   }
