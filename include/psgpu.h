@@ -88,7 +88,7 @@ int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps);
  * passes A..E (z-inverse, y-inverse, x, y-forward, z-forward + update) */
 int psg_ns3d_profile(psg_ns3d* h, int enable);
 int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts);
-/* re-run the set-up autotuner (x-pass tile height and pipeline depth, timed on
+/* re-run the set-up autotuner (x-pass rows per block and buffers per warp, timed on
  * this device); variant receives the choice, ms[4] the timing of each variant
  * (-1: does not fit) */
 int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
