@@ -328,6 +328,9 @@ struct Upo2D {
   int grid_cap = 148;
   // blocks per instance (a cluster) when the batch leaves room: at most this many
   int cluster_max = 4;
+  // side streams and events of integrations split over several launches
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
 
   ~Upo2D() {
     if (pool) cudaFree(pool);
@@ -340,6 +343,11 @@ struct Upo2D {
     if (d_qn) cudaFree(d_qn);
     if (d_H) cudaFree(d_H);
     if (d_next) cudaFree(d_next);
+    for (int k = 0; k < 3; ++k) {
+      if (side[k]) cudaStreamDestroy(side[k]);
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
   }
 
   int init(int ng_, int n_, int kmax_, int jv_mode_) {
@@ -478,50 +486,97 @@ struct Upo2D {
       h.push_back(I);
     }
     // longest first
-    std::stable_sort(h.begin(), h.end(), [](const InstTan2D<double>& a, const InstTan2D<double>& b) {
-      return a.nsteps * (a.mode == 0 ? 5 : 3) > b.nsteps * (b.mode == 0 ? 5 : 3);
+    // blocks per guess: every guess starts with one; while blocks are left
+    // (one per SM: the integrator's registers), the guess that would finish
+    // last moves to a cluster of two, then four.  Relative speeds of one, two
+    // and four blocks on one guess (FP64 tangent at 128^2): 1, 1.67, 2.34.
+    const int ni = (int)h.size();
+    std::vector<int> cs(ni, 1);
+    auto speed = [](int c) { return c == 4 ? 2.34 : c == 2 ? 1.67 : 1.0; };
+    auto work = [&](int i) { return (double)h[i].nsteps * (h[i].mode == 0 ? 5 : 3); };
+    if (cluster_max >= 2 && ni <= grid_cap) {
+      int used = ni;
+      for (;;) {
+        int worst = 0;
+        for (int i = 1; i < ni; ++i)
+          if (work(i) / speed(cs[i]) > work(worst) / speed(cs[worst])) worst = i;
+        const int up = cs[worst] == 1 ? 2 : 4;
+        if (cs[worst] == 4 || up > cluster_max || used + up - cs[worst] > grid_cap) break;
+        used += up - cs[worst];
+        cs[worst] = up;
+      }
+    }
+    // groups of four, two and one block(s), each longest first
+    std::vector<int> idx(ni);
+    for (int i = 0; i < ni; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+      return cs[a] != cs[b] ? cs[a] > cs[b] : work(a) > work(b);
     });
-    PSG_CUDA_TRY(cudaMemcpyAsync(d_inst, h.data(), sizeof(InstTan2D<double>) * h.size(),
+    std::vector<InstTan2D<double>> hs(ni);
+    int cnt[3] = {0, 0, 0};  // four, two, one
+    for (int i = 0; i < ni; ++i) {
+      hs[i] = h[idx[i]];
+      ++cnt[cs[idx[i]] == 4 ? 0 : cs[idx[i]] == 2 ? 1 : 2];
+    }
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_inst, hs.data(), sizeof(InstTan2D<double>) * ni,
                                  cudaMemcpyHostToDevice, stream));
     PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
-    const int ni = (int)h.size();
-    if (cluster_max >= 2 && 2 * ni <= grid_cap) {
-      // room for four (else two) blocks per instance
-      const int cs = (cluster_max >= 4 && 4 * ni <= grid_cap) ? 4 : 2;
-      const int cgrid = cs * ni;
-      if (cs == 4) {
+    const int ngroups = (cnt[0] > 0) + (cnt[1] > 0) + (cnt[2] > 0);
+    if (ngroups > 1 && !side[0]) {
+      for (int k = 0; k < 3; ++k) {
+        PSG_CUDA_TRY(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+        PSG_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+      }
+      PSG_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    }
+    // one group: on the engine's stream; more: each on a stream of its own,
+    // all after the copies above and before anything queued later
+    if (ngroups > 1) PSG_CUDA_TRY(cudaEventRecord(ev_fork, stream));
+    int off = 0;
+    for (int k = 0; k < 3; ++k) {
+      if (!cnt[k]) continue;
+      cudaStream_t st = stream;
+      if (ngroups > 1) {
+        st = side[k];
+        PSG_CUDA_TRY(cudaStreamWaitEvent(st, ev_fork, 0));
+      }
+      const InstTan2D<double>* d = d_inst + off;
+      const int m = cnt[k];
+      if (k == 0) {
         switch (n) {
-          case 16: tan2d_cluster<16, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 32: tan2d_cluster<32, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 64: tan2d_cluster<64, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 128: tan2d_cluster<128, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          default: tan2d_cluster<256, 4><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 16: tan2d_cluster<16, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
+          case 32: tan2d_cluster<32, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
+          case 64: tan2d_cluster<64, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
+          case 128: tan2d_cluster<128, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
+          default: tan2d_cluster<256, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
+        }
+      } else if (k == 1) {
+        switch (n) {
+          case 16: tan2d_cluster<16, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
+          case 32: tan2d_cluster<32, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
+          case 64: tan2d_cluster<64, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
+          case 128: tan2d_cluster<128, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
+          default: tan2d_cluster<256, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
         }
       } else {
+        const int grid = std::min<int>(m, grid_cap);
         switch (n) {
-          case 16: tan2d_cluster<16, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 32: tan2d_cluster<32, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 64: tan2d_cluster<64, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          case 128: tan2d_cluster<128, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
-          default: tan2d_cluster<256, 2><<<cgrid, 256, smem, stream>>>(d_inst, ni, tw); break;
+          case 16: tan2d_persistent<16><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
+          case 32: tan2d_persistent<32><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
+          case 64: tan2d_persistent<64><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
+          case 128: tan2d_persistent<128><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
+          default: tan2d_persistent<256><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
         }
       }
-      ++launches;
-      integrations += (long)ni;
       PSG_CUDA_TRY(cudaGetLastError());
-      return PSG_OK;
+      if (ngroups > 1) {
+        PSG_CUDA_TRY(cudaEventRecord(ev_join[k], st));
+        PSG_CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[k], 0));
+      }
+      ++launches;
+      off += m;
     }
-    const int grid = std::min<int>((int)h.size(), grid_cap);
-    switch (n) {
-      case 16: tan2d_persistent<16><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
-      case 32: tan2d_persistent<32><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
-      case 64: tan2d_persistent<64><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
-      case 128: tan2d_persistent<128><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
-      default: tan2d_persistent<256><<<grid, 256, smem, stream>>>(d_inst, (int)h.size(), d_next, tw); break;
-    }
-    ++launches;
-    integrations += (long)h.size();
-    PSG_CUDA_TRY(cudaGetLastError());
+    integrations += (long)ni;
     return PSG_OK;
   }
 

@@ -100,3 +100,26 @@ def test_cluster_sizes_give_the_same_integration(n, monkeypatch):
     for cs in ("2", "4"):
         np.testing.assert_array_equal(out[cs][0], out["1"][0])
         np.testing.assert_array_equal(out[cs][1], out["1"][1])
+
+
+def test_mixed_cluster_sizes_in_one_batch(monkeypatch):
+    """64 guesses with periods spread over a factor of six: with clusters
+    allowed, the longest guesses get four blocks, the middle two and the
+    shortest one, in three concurrent launches; one Newton iteration of the
+    whole batch must give bit for bit what one block per guess gives."""
+    n, nu, dt, ng = 32, 1 / 40, 0.005, 64
+    rng = np.random.default_rng(21)
+    periods = rng.uniform(0.05, 0.3, ng)
+    starts = [kolmogorov_ic2d(n, 100 + i) * 2.0 for i in range(ng)]
+    res = {}
+    for cs in ("1", "4"):
+        monkeypatch.setenv("PSG_UPO_CLUSTER", cs)
+        u = P.UPO2D(ng, n, kmax=6)
+        for i in range(ng):
+            u.set_guess(i, starts[i], T=float(periods[i]), nu=nu, dt=dt)
+        u.solve(max_newton=1, tol=1e-10)
+        res[cs] = [u.get(i) for i in range(ng)]
+        u.close()
+    for a, b in zip(res["4"], res["1"]):
+        np.testing.assert_array_equal(a["Z"], b["Z"])
+        assert (a["T"], a["sx"], a["residual"], a["gmres"]) == (b["T"], b["sx"], b["residual"], b["gmres"])
