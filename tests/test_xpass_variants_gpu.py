@@ -1,8 +1,8 @@
 """Every x-pass schedule the autotuner can pick (PSG_XPASS_VARIANT pins one;
 a variant that does not fit the device at that size is skipped) gives the
 same step as variant 1, for the RK4/CN and the Heun/CN (with the physical
-vorticity it keeps) schemes: 1e-12 in FP64, 2e-6 in FP32 (max-norm
-relative)."""
+vorticity it keeps) schemes and the Boussinesq RK4/CN scheme (nine fields
+through the x-pass): 1e-12 in FP64, 2e-6 in FP32 (max-norm relative)."""
 import numpy as np
 import pytest
 
@@ -16,10 +16,15 @@ TOL = {64: 1e-12, 32: 2e-6}
 
 def _run(monkeypatch, v, n, scheme, prec):
     monkeypatch.setenv("PSG_XPASS_VARIANT", str(v))
-    e = P.NS3D(n, scheme, precision=prec, nu=0.01, ampfor=-1.0, kf=4.0)
+    bous = scheme == P.SCHEME_BOUS_RK4
+    kw = dict(ri=1.0, sc=1.0, theta=np.pi / 2) if bous else {}
+    e = P.NS3D(n, scheme, precision=prec, nu=0.01, ampfor=-1.0, kf=4.0, **kw)
     if e.autotune(rerun=False)[0] != v:
         return None, None  # the variant does not fit: the pin is not taken
-    e.upload(*random_vorticity3d(n, 12))
+    comps = list(random_vorticity3d(n, 12))
+    if bous:
+        comps.append(random_vorticity3d(n, 13)[0])
+    e.upload(*comps)
     e.step(2e-3, 3, dump_last=(scheme == P.SCHEME_NS_HEUN))
     st = np.stack(e.download())
     ph = e.physical() if scheme == P.SCHEME_NS_HEUN else None
@@ -31,7 +36,7 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("prec", [64, 32])
-@pytest.mark.parametrize("scheme", [P.SCHEME_NS_RK4, P.SCHEME_NS_HEUN])
+@pytest.mark.parametrize("scheme", [P.SCHEME_NS_RK4, P.SCHEME_NS_HEUN, P.SCHEME_BOUS_RK4])
 @pytest.mark.parametrize("n", [32, 64])
 def test_xpass_variants_agree(monkeypatch, prec, scheme, n):
     ref, ref_ph = _run(monkeypatch, 1, n, scheme, prec)
