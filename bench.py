@@ -223,7 +223,9 @@ def run_ours(args, rank, world, dist):
 
     # e2e through the reference-facing C ABI with host buffers
     e2e = None if args.no_e2e else run_e2e(args, dev, dist, world, rank)
+    fp64_e2e = None if args.no_e2e else run_e2e(args, dev, dist, world, rank, precision=64)
     eng.close()
+    ref_steady = reference_steady() if (world == 1 and not args.no_ref) else None
 
     same_prec = run_fp64(args, dev, stream) if world == 1 and not args.no_fp64 else None
     upo = run_upo(args) if (world == 1 and not args.no_upo) else None
@@ -248,6 +250,9 @@ def run_ours(args, rank, world, dist):
                        "l2": "working set ~0.8 GB per replica >> 126 MB L2; no flush"},
             "e2e": e2e, "roofline": roof, "whole_step": whole, "cpu_baseline": cpu, "upo": upo,
             "ensemble2d": ens, "ns2d_single": single2d, "fp64_engine": same_prec,
+            "fp64_e2e": fp64_e2e,
+            "reference_steady_ms_per_step": ref_steady["steady_ms_per_step"] if ref_steady else None,
+            "reference_steady": ref_steady,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
                                 "variants": ["L=128/G,1 buffer per warp", "L=256/G,1 buffer per warp",
@@ -526,15 +531,62 @@ def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
     return out
 
 
-def run_e2e(args, dev, dist, world, rank):
-    import torch
+def run_e2e(args, dev, dist, world, rank, precision=32):
+    """The bench workload through the Boussinesq drop-in timestep_cuda_ with FP64
+    host arrays: precision 32 is the FP32 engine (PSG_PRECISION=32); 64 is the
+    drop-in's default, the reference's precision."""
     import psgpu_b200 as P
     from psgpu_b200.abi import TimestepLibrary
-    from psgpu_b200.fields import taylor_green3d
 
-    os.environ["PSG_PRECISION"] = "32"
-    lib = TimestepLibrary(P.dropin_path("bous3d"), "bous3d")
-    return time_abi_calls(lib, args, dev, dist, world, rank, ours=True)
+    if precision == 32:
+        os.environ["PSG_PRECISION"] = "32"
+    else:
+        os.environ.pop("PSG_PRECISION", None)
+    try:
+        lib = TimestepLibrary(P.dropin_path("bous3d"), "bous3d")
+        out = time_abi_calls(lib, args, dev, dist, world, rank, ours=True)
+    finally:
+        os.environ.pop("PSG_PRECISION", None)
+    out["precision"] = f"fp{precision}"
+    return out
+
+
+def reference_steady(steps=200, short=10):
+    """The reference's Boussinesq timestep_cuda_ on the bench workload, its
+    per-call set-up separated from its steady time per step: one call of
+    `short` steps and one of `short + steps`, both timed end to end (each call
+    allocates, plans, copies, steps and frees); steady = difference / steps,
+    set-up = short call - short * steady."""
+    import torch
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import Grid3D, taylor_green3d
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_bous3d.so")
+    if not os.path.exists(path):
+        return None
+    lib = TimestepLibrary(path, "bous3d")
+    g = Grid3D(N)
+    xi, et, zt = taylor_green3d(N, 1234, amp=1e-3)
+    comps0 = [np.ascontiguousarray(a, np.complex128) for a in (xi, et, zt, np.zeros_like(xi))]
+
+    def call(nsteps):
+        comps = [a.copy() for a in comps0]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lib.bous3d_inplace(comps, N, NU, DT, (nsteps + 0.5) * DT)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, rk4_evaluations(0.0, (nsteps + 0.5) * DT, DT)
+
+    with quiet_stdout():
+        call(short)  # first-call costs (context, cuFFT library load)
+        t_s, n_s = call(short)
+        t_l, n_l = call(short + steps)
+    steady = (t_l - t_s) / (n_l - n_s)
+    return {"steady_ms_per_step": round(1e3 * steady, 4),
+            "setup_ms_per_call": round(1e3 * (t_s - n_s * steady), 2),
+            "short_call_steps": n_s, "long_call_steps": n_l,
+            "how": "reference timestep_cuda_ (3D_Boussinesq/src/src_gmres/cuda.cu, FP64 cuFFT), "
+                   "a short and a long call on the same 256^3 workload, host arrays"}
 
 
 def time_abi_calls(lib, args, dev, dist, world, rank, ours):

@@ -238,10 +238,19 @@ long psg_upo2d_launches(psg_upo2d* h);
  * z_in == z_out is allowed.  The work is enqueued on `stream` (NULL: the
  * default stream).  The first call on a device looks up the array's address
  * and writes the twiddle tables (a synchronous copy), so make that first call
- * before any stream capture.  Every call uses the same array and leaves its
- * last contents there (no call relies on them: each scratch word is written
- * before it is read), so calls that overlap on the GPU -- e.g. on two streams
- * at once -- race; serialise them on one stream. */
+ * before any stream capture: a first call on a capturing stream is refused
+ * with PSG_ERR_UNSUPPORTED.  The set-up is remembered for the life of the
+ * process; calls after cudaDeviceReset are not supported.  Every call uses the
+ * same array and leaves its last contents there (no call relies on them: each
+ * scratch word is written, or cleared on the call's stream, before it is
+ * read), so calls that overlap on the GPU -- e.g. on two streams at once --
+ * race; serialise them on one stream.
+ *
+ * Precision 32 carries the rounding error of each state update in the array,
+ * as psg_batch2d_run's FP32 engine does, starting from zero at every call (the
+ * state is exactly the caller's FP32 input); the carried remainder is dropped
+ * when the call returns, so a long FP32 run split over many calls rounds once
+ * per call more than one long call. */
 int psg_ns2d_step_noalloc(int n, int precision, double nu, double dt, int nsteps,
                           const void* z_in, void* z_out, void* stream);
 

@@ -4,6 +4,14 @@
 // state after NSTOP RK4/CN steps and *Time = NSTOP*DELT (accumulated as the
 // reference does).  The Kolmogorov forcing (-2 at kx = 0, |ky| = 4) is part of
 // the scheme, as in the reference.  Device buffers persist between calls.
+//
+// Precision: FP64, the reference's, unless PSG_PRECISION=32 in the
+// environment selects the FP32 engine.  On any failure the state array is
+// filled with NaN (after one line on stderr): the reference has no error
+// channel, and its Newton driver detects a failed integration by the NaN it
+// leaves (src_gmres/main.F90:1527-1534, 1636-1665); an unchanged state would
+// read as Phi_T(z) = z, i.e. a false zero residual.
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -28,8 +36,15 @@ int g_n = 0, g_prec = 0;
 
 int env_precision() {
   const char* s = getenv("PSG_PRECISION");
-  if (s && (!strcmp(s, "64") || !strcmp(s, "fp64"))) return 64;
-  return 32;
+  if (s && (!strcmp(s, "32") || !strcmp(s, "fp32"))) return 32;
+  return 64;
+}
+
+// the caller's box as NaN: IKTX*IKTY complex entries, when the sizes are sane
+void fill_nan(double2* Z, int iktx, int ikty) {
+  if (!Z || iktx <= 0 || ikty <= 0 || (long)iktx * ikty > (1L << 28)) return;
+  const long n = (long)iktx * ikty;
+  for (long i = 0; i < n; ++i) Z[i].x = Z[i].y = NAN;
 }
 }  // namespace
 
@@ -40,8 +55,9 @@ extern "C" void timestep_cuda_(double2* Z, double* ZR, double* kx, double* ky, d
   (void)ZR; (void)kx; (void)ky; (void)TSTART; (void)TNEWT; (void)ikF; (void)ikN; (void)LC;
   const int n = *NY, K = n / 3;
   if (*NX != *NY || *alpha != 1.0 || *KTY != K || *IKTX != K + 1 || *IKTY != 2 * K + 1) {
-    fprintf(stderr, "psgpu_b200 timestep_cuda_: unsupported sizes NX=%d NY=%d IKTX=%d IKTY=%d KTY=%d alpha=%g\n",
-            *NX, *NY, *IKTX, *IKTY, *KTY, *alpha);
+    fprintf(stderr, "psgpu_b200 timestep_cuda_: unsupported sizes NX=%d NY=%d IKTX=%d IKTY=%d KTY=%d alpha=%g "
+            "(square boxes with alpha = 1 only)\n", *NX, *NY, *IKTX, *IKTY, *KTY, *alpha);
+    fill_nan(Z, *IKTX, *IKTY);
     return;
   }
   const int prec = env_precision();
@@ -51,6 +67,7 @@ extern "C" void timestep_cuda_(double2* Z, double* ZR, double* kx, double* ky, d
     if (psg_batch2d_create(&g_h, 1, &n, prec)) {
       fprintf(stderr, "psgpu_b200 timestep_cuda_: %s\n", psg_last_error());
       g_h = nullptr;
+      fill_nan(Z, *IKTX, *IKTY);
       return;
     }
     g_n = n; g_prec = prec;
@@ -60,6 +77,7 @@ extern "C" void timestep_cuda_(double2* Z, double* ZR, double* kx, double* ky, d
   if (psg_batch2d_upload(g_h, 0, (const double*)Z) || psg_batch2d_run(g_h, &nu, &dt, &ns) ||
       psg_batch2d_download(g_h, 0, (double*)Z)) {
     fprintf(stderr, "psgpu_b200 timestep_cuda_: %s\n", psg_last_error());
+    fill_nan(Z, *IKTX, *IKTY);
     return;
   }
   *Time = 0.0;

@@ -8,9 +8,12 @@
 // reference, device buffers persist between calls (one cached engine per grid
 // size), so a call costs one upload, the steps and one download.
 //
-// Precision: FP32 storage and transforms by default; PSG_PRECISION=64 in the
-// environment selects the FP64 engine.  Failures print one line to stderr and
-// leave the state arrays as they were (the reference has no error channel).
+// Precision: FP64 storage and transforms, the reference's, unless
+// PSG_PRECISION=32 in the environment selects the FP32 engine.  A failure
+// prints one line to stderr and fills the state arrays with NaN: the
+// reference has no error channel, and its Newton drivers detect a failed
+// integration by the NaN it leaves (2D_NavierStokes/src_RK4/src_gmres/
+// main.F90:1527-1534); an unchanged state would read as Phi_T(z) = z.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -31,12 +34,26 @@ Cached g_cache;
 
 int env_precision() {
   const char* s = getenv("PSG_PRECISION");
-  if (s && (!strcmp(s, "64") || !strcmp(s, "fp64"))) return 64;
-  return 32;
+  if (s && (!strcmp(s, "32") || !strcmp(s, "fp32"))) return 32;
+  return 64;
 }
 
 void report(const char* where) {
   fprintf(stderr, "psgpu_b200 %s: %s\n", where, psg_last_error());
+}
+
+// the caller's state arrays as NaN (nkt complex entries each), when nkt is sane
+void fill_nan(double2* const* comps, int ncomp, long nkt) {
+  if (nkt <= 0 || nkt > (1L << 31)) return;
+  for (int c = 0; c < ncomp; ++c) {
+    if (!comps[c]) continue;
+    for (long i = 0; i < nkt; ++i) comps[c][i].x = comps[c][i].y = NAN;
+  }
+}
+
+long box_nkt(int n) {
+  const long K = n / 3;
+  return (K + 1) * (2 * K + 1) * (2 * K + 1);
 }
 
 psg_ns3d* engine(int n, int scheme) {
@@ -80,16 +97,20 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double*
                                int* RANK) {
   (void)nuzn; (void)nu1; (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)ikF; (void)ikN;
   (void)LC; (void)NOUT; (void)NOUTV; (void)statsFLAG; (void)RecFLAG; (void)RANK;
-  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  double2* state[3] = {xii, eta, zet};
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) {
+    fill_nan(state, 3, *NKT);
+    return;
+  }
   psg_ns3d* h = engine(*NX, PSG_SCHEME_NS_HEUN);
-  if (!h) { report("timestep_cuda_"); return; }
   const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
   double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
   double* phys[3] = {xir, etr, ztr};
-  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, 0.0, 1.0, 0.0) ||
+  if (!h || psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, 0.0, 1.0, 0.0) ||
       psg_ns3d_upload(h, in) || psg_ns3d_step(h, *DELT, *NSTOP, 1) || psg_ns3d_download(h, out) ||
       (*NSTOP > 0 && psg_ns3d_download_phys(h, phys))) {
     report("timestep_cuda_");
+    fill_nan(state, 3, *NKT);
     return;
   }
   if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
@@ -108,14 +129,16 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double*
   (void)nuzn; (void)nu1; (void)kx; (void)ky; (void)kz; (void)ikF; (void)ikN; (void)LC;
   int n = 128;
   if (const char* e = getenv("PSG_NEWTON_N")) n = atoi(e);
+  double2* state[3] = {xii, eta, zet};
   psg_ns3d* h = engine(n, PSG_SCHEME_NS_HEUN);
-  if (!h) { report("timestep_cuda_"); return; }
   const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
   double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
-  if (psg_ns3d_set_forcing_form(h, PSG_FORCING_NEWTON) ||
+  if (!h || psg_ns3d_set_forcing_form(h, PSG_FORCING_NEWTON) ||
       psg_ns3d_set_params(h, *V2, *AMPFOR, (double)*KFY, 0.0, 1.0, 0.0) ||
       psg_ns3d_upload(h, in) || psg_ns3d_step(h, *DELT, *NSTOP, 0) || psg_ns3d_download(h, out)) {
     report("timestep_cuda_");
+    // the caller's arrays hold the box of the compiled-in grid
+    fill_nan(state, 3, box_nkt(n));
     return;
   }
   if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
@@ -131,16 +154,20 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double*
                                int* statsFLAG) {
   (void)kx; (void)ky; (void)kz; (void)ikF; (void)ikN; (void)LC; (void)NOUT; (void)NOUTV;
   (void)statsFLAG;
-  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  double2* state[3] = {xii, eta, zet};
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) {
+    fill_nan(state, 3, *NKT);
+    return;
+  }
   psg_ns3d* h = engine(*NX, PSG_SCHEME_EULER_HEUN);
-  if (!h) { report("timestep_cuda_"); return; }
   const double* in[3] = {(const double*)xii, (const double*)eta, (const double*)zet};
   double* out[3] = {(double*)xii, (double*)eta, (double*)zet};
   double* phys[3] = {xir, etr, ztr};
-  if (psg_ns3d_set_params(h, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0) || psg_ns3d_upload(h, in) ||
+  if (!h || psg_ns3d_set_params(h, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0) || psg_ns3d_upload(h, in) ||
       psg_ns3d_step(h, *DELT, *NSTOP, 1) || psg_ns3d_download(h, out) ||
       (*NSTOP > 0 && psg_ns3d_download_phys(h, phys))) {
     report("timestep_cuda_");
+    fill_nan(state, 3, *NKT);
     return;
   }
   if (*NSTOP > 0) *Time = *TSTART + (double)(*NSTOP) * (*DELT);
@@ -161,15 +188,14 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
                                int* RecFLAG, int* adaptFLAG, int* RANK) {
   (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)Dtarget; (void)ikF; (void)ikN; (void)LC;
   (void)NOUT; (void)NOUTV; (void)statsFLAG; (void)RecFLAG; (void)adaptFLAG; (void)RANK;
-  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
-  psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
-  if (!h) { report("timestep_cuda_"); return; }
-  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
-  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
-  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) || psg_ns3d_upload(h, in)) {
-    report("timestep_cuda_");
+  double2* state[4] = {xii, eta, zet, rho};
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) {
+    fill_nan(state, 4, *NKT);
     return;
   }
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
+  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
+  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
   const double delt = *DELT;
   double tme = *TSTART;
   int nfull = 0;
@@ -177,9 +203,13 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
     ++nfull;
     tme += delt;
   }
-  if (psg_ns3d_step(h, delt, nfull, 0)) { report("timestep_cuda_"); return; }
-  if (tme != *Tstep && psg_ns3d_step(h, *Tstep - tme, 1, 0)) { report("timestep_cuda_"); return; }
-  if (psg_ns3d_download(h, out)) { report("timestep_cuda_"); return; }
+  if (!h || psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) ||
+      psg_ns3d_upload(h, in) || psg_ns3d_step(h, delt, nfull, 0) ||
+      (tme != *Tstep && psg_ns3d_step(h, *Tstep - tme, 1, 0)) || psg_ns3d_download(h, out)) {
+    report("timestep_cuda_");
+    fill_nan(state, 4, *NKT);
+    return;
+  }
   for (int i = 0; i < nfull; ++i) *Time = *Time + delt;
 }
 
@@ -196,14 +226,19 @@ extern "C" void timederiv_cuda_(double2* xii, double2* eta, double2* zet, double
   (void)kx; (void)ky; (void)kz; (void)Time; (void)TSTART; (void)Tstep; (void)DELT;
   (void)ResThresh; (void)Dtarget; (void)ikF; (void)ikN; (void)LC; (void)NOUT; (void)NOUTV;
   (void)statsFLAG; (void)RecFLAG; (void)adaptFLAG; (void)RANK;
-  if (!check_sizes("timederiv_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) return;
+  double2* state[4] = {xii, eta, zet, rho};
+  if (!check_sizes("timederiv_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha)) {
+    fill_nan(state, 4, *NKT);
+    return;
+  }
   psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
-  if (!h) { report("timederiv_cuda_"); return; }
   const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
   double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
-  if (psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) || psg_ns3d_upload(h, in) ||
-      psg_ns3d_timederiv(h, out))
+  if (!h || psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) ||
+      psg_ns3d_upload(h, in) || psg_ns3d_timederiv(h, out)) {
     report("timederiv_cuda_");
+    fill_nan(state, 4, *NKT);
+  }
 }
 
 #else

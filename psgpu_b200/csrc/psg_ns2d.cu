@@ -472,7 +472,9 @@ extern "C" int psg_batch2d_device_state(psg_batch2d* h, int i, void** Z) {
 //
 // Size limit: grids up to 128 x 128 (FP32 or FP64).  The array is part of the
 // library image, so every GPU that loads the library holds these 512 KiB until
-// the process exits.
+// the process exits.  The FP32 step also keeps, in the array, the rounding
+// error its state updates carry (as psg_batch2d_run's FP32 engine does),
+// cleared at the start of every call, so a call's state is its FP32 input.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -482,7 +484,16 @@ constexpr int kNoallocMaxN = 128;
 constexpr size_t kNoallocBytes = 512 * 1024;
 constexpr size_t kTw64Off = 0;          // 480 complex doubles (n = 16..128, two plans each)
 constexpr size_t kTw32Off = 8192;       // 480 complex floats
-constexpr size_t kWorkOff = 12288;      // Z0..Z3 and row scratch
+constexpr size_t kWorkOff = 12288;      // Z0..Z3, the carried error (FP32) and row scratch
+
+constexpr long nkt2c(int n) { return (long)(n / 3 + 1) * (2 * (n / 3) + 1); }
+// bytes of the work area at the largest grid: FP64 (4 stage registers + 3 scratch
+// rows) and FP32 (the same plus the carried rounding error)
+constexpr size_t kWork64 = 16 * (4 * nkt2c(kNoallocMaxN) + 3L * kNoallocMaxN * (kNoallocMaxN / 3 + 1));
+constexpr size_t kWork32 = 8 * (5 * nkt2c(kNoallocMaxN) + 3L * kNoallocMaxN * (kNoallocMaxN / 3 + 1));
+static_assert(kWorkOff + kWork64 <= kNoallocBytes && kWorkOff + kWork32 <= kNoallocBytes,
+              "static scratch too small for the largest grid");
+static_assert(kTw64Off + 480 * 16 <= kTw32Off && kTw32Off + 480 * 8 <= kWorkOff, "twiddle tables");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
@@ -516,8 +527,10 @@ size_t noalloc_smem() {
 
 // One-time set-up on the current device: find the array's device address,
 // write the twiddle tables into it, raise the kernels' shared-memory limit.
-// Nothing here allocates device memory.
-int noalloc_setup(unsigned char** out) {
+// Nothing here allocates device memory.  The table copies are synchronous, so
+// a first call made while `stream` is being captured is refused (the capture
+// would be invalidated) with a message asking for a warm-up call.
+int noalloc_setup(unsigned char** out, cudaStream_t stream) {
   int dev = 0;
   PSG_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) {
@@ -526,6 +539,14 @@ int noalloc_setup(unsigned char** out) {
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (g_noalloc_addr[dev]) { *out = g_noalloc_addr[dev]; return PSG_OK; }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PSG_CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    psg_set_error("psg_ns2d_step_noalloc: the first call on device %d sets up the static scratch "
+                  "with synchronous copies and cannot run during stream capture; make one call "
+                  "before capturing", dev);
+    return PSG_ERR_UNSUPPORTED;
+  }
   void* addr = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
   if (e != cudaSuccess) {
@@ -558,8 +579,15 @@ int noalloc_run(unsigned char* base, int n, double nu, double dt, int nsteps, co
   I.n = n; I.nsteps = nsteps; I.nu = (T)nu; I.dt = (T)dt;
   I.Z = reinterpret_cast<cpx<T>*>(z_out);
   I.Z0 = work; I.Z1 = work + nk; I.Z2 = work + 2 * nk; I.Z3 = work + 3 * nk;
-  I.work = work + 4 * nk;
-  I.ZC = nullptr;
+  if (sizeof(T) == 4) {
+    // the carried rounding error starts at zero: the state is the caller's FP32 value
+    I.ZC = work + 4 * nk;
+    PSG_CUDA_TRY(cudaMemsetAsync(I.ZC, 0, sizeof(cpx<T>) * nk, stream));
+    I.work = work + 5 * nk;
+  } else {
+    I.ZC = nullptr;
+    I.work = work + 4 * nk;
+  }
   const cpx<T>* tw = reinterpret_cast<const cpx<T>*>(base + (sizeof(T) == 8 ? kTw64Off : kTw32Off));
   int off = 0;
   for (int m = 16; m < n; m *= 2) off += 2 * m;
@@ -586,15 +614,10 @@ extern "C" int psg_ns2d_step_noalloc(int n, int precision, double nu, double dt,
     psg_set_error("psg_ns2d_step_noalloc: bad arguments");
     return PSG_ERR_ARG;
   }
-  // the largest footprint must fit the array: 4 stage registers + 3 scratch rows
-  const size_t need = kWorkOff + (size_t)16 * (4 * nkt2(kNoallocMaxN) + 3L * kNoallocMaxN * (kNoallocMaxN / 3 + 1));
-  static_assert(kWorkOff + 16ull * (4 * 3655 + 3 * 128 * 43) <= kNoallocBytes, "scratch too small");
-  static_assert(kTw64Off + 480 * 16 <= kTw32Off && kTw32Off + 480 * 8 <= kWorkOff, "twiddle tables");
-  (void)need;
-  unsigned char* base = nullptr;
-  int rc = noalloc_setup(&base);
-  if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* base = nullptr;
+  int rc = noalloc_setup(&base, s);
+  if (rc) return rc;
   return precision == 64 ? noalloc_run<double>(base, n, nu, dt, nsteps, z_in, z_out, s)
                          : noalloc_run<float>(base, n, nu, dt, nsteps, z_in, z_out, s);
 }

@@ -1,9 +1,12 @@
 """psg_ns2d_step_noalloc: the 2D step for callers that cannot allocate device
-memory (a plugin inside a runtime that owns the GPU's memory, code running
-during stream capture, a fixed-budget embedded driver).  Its scratch is an
-array compiled into the library; the caller only hands over device pointers
-to the state.  Checked against the batched entry point on the same inputs,
-two calls in a row, through the C ABI.  This file is collected last."""
+memory when they step -- a plugin inside a runtime that owns the GPU's memory,
+code running during stream capture, a fixed-budget embedded driver.  Its
+scratch is an array compiled into the library; the caller only hands over
+device pointers to the state.  Checked against the batched entry point on the
+same inputs, two calls in a row, through the C ABI, at every grid the array
+holds; a long FP32 run checks that the carried rounding error matches the
+batched FP32 engine's; and a call is shown to allocate no device memory.
+This file is collected last."""
 import ctypes as C
 
 import numpy as np
@@ -38,8 +41,12 @@ def _batch(Z, n, prec, nu, dt, ns):
     return out
 
 
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
 @pytest.mark.parametrize("prec", [64, 32])
-@pytest.mark.parametrize("n", [32, 128])
+@pytest.mark.parametrize("n", [16, 32, 64, 128])
 def test_noalloc_matches_batched_entry_point(n, prec):
     import torch
     L = P.lib()
@@ -53,9 +60,7 @@ def test_noalloc_matches_batched_entry_point(n, prec):
                                  C.c_void_p(dout.data_ptr()), None)
     assert rc == 0, L.psg_last_error()
     torch.cuda.synchronize()
-    ref = _batch(Za, n, prec, nu, dt, 12)
-    err = np.abs(_to_host(dout, g.shape) - ref).max() / np.abs(ref).max()
-    assert err < TOL[prec]
+    assert _rel(_to_host(dout, g.shape), _batch(Za, n, prec, nu, dt, 12)) < TOL[prec]
     # call 2: another state, in place, 7 steps; the scratch keeps call 1's contents
     Zb = kolmogorov_ic2d(n, 72)
     dz = _to_device(Zb, prec)
@@ -63,9 +68,53 @@ def test_noalloc_matches_batched_entry_point(n, prec):
                                  C.c_void_p(dz.data_ptr()), None)
     assert rc == 0, L.psg_last_error()
     torch.cuda.synchronize()
-    ref = _batch(Zb, n, prec, nu, dt, 7)
-    err = np.abs(_to_host(dz, g.shape) - ref).max() / np.abs(ref).max()
-    assert err < TOL[prec]
+    assert _rel(_to_host(dz, g.shape), _batch(Zb, n, prec, nu, dt, 7)) < TOL[prec]
+
+
+def test_noalloc_fp32_long_run_carries_the_rounding_error():
+    """500 FP32 steps: the batched FP32 engine carries each update's rounding
+    error; so does this entry point.  Both start from the same FP32 values."""
+    import torch
+    L = P.lib()
+    n, nu, dt, ns = 64, 1 / 40, 0.005, 500
+    g = Grid2D(n)
+    Z = kolmogorov_ic2d(n, 73)
+    Z32 = Z.astype(np.complex64).astype(np.complex128)  # exactly representable in FP32
+    dz = _to_device(Z32, 32)
+    rc = L.psg_ns2d_step_noalloc(n, 32, nu, dt, ns, C.c_void_p(dz.data_ptr()),
+                                 C.c_void_p(dz.data_ptr()), None)
+    assert rc == 0, L.psg_last_error()
+    torch.cuda.synchronize()
+    ours = _to_host(dz, g.shape)
+    ref32 = _batch(Z32, n, 32, nu, dt, ns)
+    ref64 = _batch(Z32, n, 64, nu, dt, ns)
+    # same arithmetic as the batched FP32 engine up to its final hi+lo sum
+    assert _rel(ours, ref32) < 1e-6
+    # and as close to FP64 as the batched FP32 engine is
+    assert _rel(ours, ref64) < 3 * max(_rel(ref32, ref64), 1e-7)
+
+
+def test_noalloc_allocates_no_device_memory():
+    import torch
+    L = P.lib()
+    n = 128
+    Z = kolmogorov_ic2d(n, 74)
+    dz = _to_device(Z, 64)
+    for _ in range(2):  # the first call sets up the array; later calls only launch
+        assert L.psg_ns2d_step_noalloc(n, 64, 1 / 40, 0.005, 3, C.c_void_p(dz.data_ptr()),
+                                       C.c_void_p(dz.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for prec in (64, 32):
+        d = dz if prec == 64 else _to_device(Z, 32)
+        if prec == 32:
+            torch.cuda.synchronize()
+            free0, _ = torch.cuda.mem_get_info()
+        assert L.psg_ns2d_step_noalloc(n, prec, 1 / 40, 0.005, 3, C.c_void_p(d.data_ptr()),
+                                       C.c_void_p(d.data_ptr()), None) == 0
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (prec, free0 - free1)
 
 
 def test_noalloc_rejects_grids_beyond_the_array():
