@@ -348,70 +348,153 @@ def run_ref2d_probe(steps, n=None):
 UPO_N, UPO_NU, UPO_DT, UPO_GUESSES, UPO_KMAX = 128, 1.0 / 40.0, 0.005, 64, 60
 
 
-def run_upo(args):
-    """Batched Newton-GMRES-hookstep on 2D Kolmogorov flow, Re = 40, 128^2:
-    64 guesses from seeded turbulent states after a 500 time-unit spin-up
-    (one persistent launch), periods uniform in [5, 20], Krylov dimension 60,
-    FP64 integrations and Arnoldi, target residual 1e-10.  Newton iterations
-    per second with the exact tangent Jv and with the forward-difference Jv,
-    and the reference's plain form (one guess at a time, one timestep_cuda_
-    call per Krylov vector) from its measured time per integration."""
-    import torch
+def upo_guesses(G=UPO_GUESSES, search=60.0, seed=5000):
+    """64 guesses from turbulent 2D Kolmogorov states, Re = 40, 128^2: 64 seeded
+    runs (modes 1 <= |k| <= 8, enstrophy 1) spun up for 500 time units in one
+    persistent FP32 launch, then continued for `search` time units under the
+    GPU recurrence search (every 0.1 time units, a ring of 20 time units,
+    32 x 4 trial shifts over the 2 x 8^2 lowest modes, threshold 0.4).  Of the
+    emitted guesses those with periods in [5, 20] are kept, lowest residual
+    first; runs that emitted none (or too few overall) contribute their last
+    state with a period drawn uniformly in [5, 20]."""
     import psgpu_b200 as P
-    from psgpu_b200.abi import TimestepLibrary
     from psgpu_b200.fields import kolmogorov_ic2d
 
-    n, nu, dt, G = UPO_N, UPO_NU, UPO_DT, UPO_GUESSES
-    spin = P.Batch2D([n] * G, precision=32)
+    n, nu, dt = UPO_N, UPO_NU, UPO_DT
+    b = P.Batch2D([n] * G, precision=32)
     for i in range(G):
-        spin.upload(i, kolmogorov_ic2d(n, 5000 + i))
+        b.upload(i, kolmogorov_ic2d(n, seed + i))
     t0 = time.perf_counter()
-    spin.run([nu] * G, [dt] * G, [int(round(500.0 / dt))] * G)
-    spin.sync()
+    b.run([nu] * G, [dt] * G, [int(round(500.0 / dt))] * G)
+    b.sync()
     spin_s = time.perf_counter() - t0
-    guesses = [spin.download(i) for i in range(G)]
-    spin.close()
-    periods = np.random.default_rng(77).uniform(5.0, 20.0, G)
-    out = {"workload": "2D Kolmogorov Re=40 128^2, 64 guesses from turbulent states after a "
-                       "500 time-unit spin-up, periods U[5,20], Krylov 60, FP64, tol 1e-10",
-           "spinup_seconds": round(spin_s, 2), "newton_per_guess": args.upo_newton}
-    per_guess_integrations = None
-    for name, exact in (("exact_jv", True), ("fd_jv", False)):
-        u = P.UPO2D(G, n, kmax=UPO_KMAX, exact_jv=exact)
-        for i in range(G):
-            u.set_guess(i, guesses[i], T=float(periods[i]), nu=nu, dt=dt)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        u.solve(max_newton=args.upo_newton, tol=1e-10, gmres_tol=1e-3)
-        sec = time.perf_counter() - t0
-        info = [u.get(i) for i in range(G)]
-        newton = sum(x["newton"] for x in info)
-        res = np.array([x["residual"] for x in info])
-        out[name] = {"newton_iters_per_s": round(newton / sec, 4), "newton_iters": newton,
-                     "gmres_iters": sum(x["gmres"] for x in info),
-                     "integrations": u.integrations, "seconds": round(sec, 2),
-                     "converged": sum(x["status"] == "CONVERGED" for x in info),
-                     "median_rel_residual": float(np.median(res))}
-        if exact:
-            per_guess_integrations = [x["gmres"] + x["hookstep"] + x["newton"] for x in info]
-        u.close()
-    # plain form: the reference's own 2D step, one integration per call
+    nout = 20
+    rec = P.Recurrence2D(G, n, nout, dt, 0.4, nu, store_size=int(round(20.0 / (nout * dt))) + 1,
+                         norm_width=8, nshift=(32, 4), tstart=500.0)
+    t0 = time.perf_counter()
+    rec.start(b)
+    nchk = int(round(search / (nout * dt)))
+    for k in range(1, nchk + 1):
+        b.run(nu, dt, nout)
+        rec.add(k * nout, b)
+    b.sync()
+    search_s = time.perf_counter() - t0
+    found = [rec.guess(k) for k in range(rec.count)]
+    found = [g for g in found if 5.0 <= g[0]["period"] <= 20.0]
+    found.sort(key=lambda g: g[0]["residual"])
+    guesses = [(Z, m["period"], m["shift_x"], m["shift_y"], m["residual"]) for m, Z in found[:G]]
+    nrec = len(guesses)
+    rng = np.random.default_rng(77)
+    i = 0
+    while len(guesses) < G:
+        guesses.append((b.download(i % G), float(rng.uniform(5.0, 20.0)), 0.0, 0.0, None))
+        i += 1
+    b.close()
+    rec.close()
+    return guesses, {"spinup_seconds": round(spin_s, 2), "search_seconds": round(search_s, 2),
+                     "recurrence_guesses": nrec, "search_time_units": search,
+                     "median_recurrence_residual":
+                         float(np.median([g[4] for g in guesses[:nrec]])) if nrec else None}
+
+
+def solve_upo(guesses, form, max_newton):
+    """one batched Newton-GMRES-hookstep solve of all guesses; form: exact32,
+    exact64 or fd"""
+    import torch
+    import psgpu_b200 as P
+
+    n, nu, dt = UPO_N, UPO_NU, UPO_DT
+    G = len(guesses)
+    u = P.UPO2D(G, n, kmax=UPO_KMAX, exact_jv=form != "fd",
+                jv_precision=32 if form == "exact32" else 64)
+    for i, (Z, T, sx, sy, _) in enumerate(guesses):
+        u.set_guess(i, Z, T=float(T), sx=float(sx), sy=float(sy), nu=nu, dt=dt)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    u.solve(max_newton=max_newton, tol=1e-10, gmres_tol=1e-3)
+    sec = time.perf_counter() - t0
+    info = [u.get(i) for i in range(G)]
+    u.close()
+    newton = sum(x["newton"] for x in info)
+    conv = sum(x["status"] == "CONVERGED" for x in info)
+    res = np.array([x["residual"] for x in info])
+    status = {}
+    for x in info:
+        status[x["status"]] = status.get(x["status"], 0) + 1
+    return {"newton_iters_per_s": round(newton / sec, 4), "newton_iters": newton,
+            "gmres_iters": sum(x["gmres"] for x in info), "seconds": round(sec, 2),
+            "converged": int(conv),
+            "seconds_per_converged_orbit": round(sec / conv, 2) if conv else None,
+            "converged_periods": sorted(round(x["T"], 5) for x in info
+                                        if x["status"] == "CONVERGED"),
+            "median_rel_residual": float(np.median(res)),
+            "min_rel_residual": float(res.min()), "statuses": status}
+
+
+def plain_upo(guess, max_newton=1):
+    """The reference's plain form, run: its Newton-GMRES-hookstep (the FP64
+    restatement oracle/newton2d.py, one guess at a time, forward-difference Jv
+    with eps = 1e-7, DGESDD) with every integration one call of the reference's
+    own 2D timestep_cuda_ (oracle/_ref/libref_ns2d.so, FP64 cuFFT, allocations
+    and plans per call) and TIMEDERIV on the host; the host's linear algebra
+    is included, as in the reference's driver."""
+    from oracle import pyoracle as O
+    from oracle.newton2d import Newton2D
+    from psgpu_b200.abi import TimestepLibrary
+
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
-    if os.path.exists(path):
-        nst = int(round(12.5 / dt))
-        step_s = ref2d_step_ms(nst) / 1e3
-        plain_s = sum(k * (periods[i] / dt) * step_s for i, k in enumerate(per_guess_integrations))
-        newton = out["exact_jv"]["newton_iters"]
-        out["plain_reference"] = {
-            "newton_iters_per_s": round(newton / plain_s, 5),
-            "seconds_model": round(plain_s, 1),
-            "how": "the same Newton iterations as the exact-Jv run, each integration a "
-                   "reference timestep_cuda_ call (FP64 cuFFT, one guess at a time) costed at "
-                   f"its measured {1e3 * step_s:.4f} ms/step (one call of {nst} steps incl. "
-                   "its set-up, timed in a separate process); host Arnoldi/SVD time not "
-                   "included"}
-        out["exact_vs_plain"] = round(out["exact_jv"]["newton_iters_per_s"] /
-                                      out["plain_reference"]["newton_iters_per_s"], 2)
+    if not os.path.exists(path):
+        return None
+    n, nu, dt = UPO_N, UPO_NU, UPO_DT
+    lib = TimestepLibrary(path, "ns2d")
+
+    def phi(z, t, truedelt):
+        ns = int(t / truedelt)
+        return lib.ns2d(z, n, nu, t / ns, ns)[0]
+
+    def rhs(z):
+        return O.ns2d_timederiv(z, n, nu)
+
+    Z, T, sx, sy, _ = guess
+    solver = Newton2D(n, phi, rhs, gmresmax=UPO_KMAX)
+    with quiet_stdout():
+        t0 = time.perf_counter()
+        r = solver.solve(Z, float(T), float(sx), float(sy), 0, dt, max_newton=max_newton)
+        sec = time.perf_counter() - t0
+    return {"newton_iters_per_s": round(r.newton / sec, 6), "newton_iters": r.newton,
+            "gmres_iters": r.gmres, "integrations": r.integrations, "seconds": round(sec, 2),
+            "period": round(float(T), 4), "rel_residual": r.ner, "status": r.status,
+            "how": "one guess, the reference's Newton-GMRES-hookstep restated in FP64 on the "
+                   "host with every integration a call of the reference's own 2D "
+                   "timestep_cuda_ (FP64 cuFFT), run, not costed"}
+
+
+def run_upo(args):
+    """Batched Newton-GMRES-hookstep on 2D Kolmogorov flow, Re = 40, 128^2,
+    Krylov dimension 60, FP64 residuals, Arnoldi and hookstep, target 1e-10:
+    the 64 recurrence-derived guesses of upo_guesses() solved in the chosen
+    form (exact tangent Jv integrated in FP32), with the FP64 forward
+    difference of the same solver beside it, and the reference's plain form
+    (one guess at a time, one reference timestep_cuda_ call per integration)
+    run on the shortest-period guess."""
+    guesses, out = upo_guesses()
+    out["workload"] = ("2D Kolmogorov Re=40 128^2, 64 guesses from turbulent states after a "
+                       "500 time-unit spin-up, periods in [5,20] from the recurrence search, "
+                       "Krylov 60, FP64 residual/Arnoldi/hookstep, tol 1e-10")
+    out["newton_per_guess_max"] = args.upo_newton
+    forms = ("exact32", "fd") if not args.upo_all_forms else ("exact32", "exact64", "fd")
+    for form in forms:
+        out[{"exact32": "exact_jv", "exact64": "exact_jv_fp64", "fd": "fd_jv"}[form]] = \
+            solve_upo(guesses, form, args.upo_newton)
+    if not args.no_upo_plain:
+        short = min(guesses, key=lambda g: g[1])
+        plain = plain_upo(short)
+        if plain:
+            out["plain_reference"] = plain
+            out["exact_vs_plain"] = round(out["exact_jv"]["newton_iters_per_s"] /
+                                          plain["newton_iters_per_s"], 1)
+    out["exact_vs_fd"] = round(out["exact_jv"]["newton_iters_per_s"] /
+                               out["fd_jv"]["newton_iters_per_s"], 3)
     return out
 
 
@@ -521,14 +604,35 @@ def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
                               "threads": [128, 256, 512]}}
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
     if os.path.exists(path) and world == 1:
-        ms = {int(n): ref2d_step_ms(200, int(n)) for n in (64, 128, 256)}
-        ref_s = sum(steps * ms[int(n)] / 1e3 for n in sizes_all)
-        out["plain_reference"] = {"instance_steps_per_s": round(M * steps / ref_s, 2),
-                                  "ms_per_step": {str(k): round(v, 4) for k, v in ms.items()},
-                                  "how": "one reference timestep_cuda_ call per instance, costed "
-                                         "at its measured ms/step per size (200-step call in a "
-                                         "separate process)"}
+        out["plain_reference"] = ensemble_plain(sizes_all, nu_all, path)
     return out
+
+
+def ensemble_plain(sizes_all, nu_all, path, per_size=4, steps=200):
+    """The reference's plain form of the ensemble, run on a stated subset: the
+    first `per_size` instances of each grid size (their own initial states and
+    viscosities), one reference 2D timestep_cuda_ call of `steps` steps each,
+    one instance at a time, host arrays in and out (its set-up per call
+    included).  The subset holds equal numbers of each size, as the
+    ensemble's uniform size draw does on average."""
+    from psgpu_b200.abi import TimestepLibrary
+    from psgpu_b200.fields import kolmogorov_ic2d
+
+    lib = TimestepLibrary(path, "ns2d")
+    pick = []
+    for sz in (64, 128, 256):
+        pick += [i for i in range(len(sizes_all)) if int(sizes_all[i]) == sz][:per_size]
+    with quiet_stdout():
+        lib.ns2d(kolmogorov_ic2d(64, 1), 64, 1 / 40, 0.005, 2)  # first-call costs
+        t0 = time.perf_counter()
+        for i in pick:
+            n = int(sizes_all[i])
+            lib.ns2d(kolmogorov_ic2d(n, 9000 + i), n, float(nu_all[i]), 0.005, steps)
+        sec = time.perf_counter() - t0
+    return {"instance_steps_per_s": round(len(pick) * steps / sec, 2), "instances": len(pick),
+            "steps_each": steps, "seconds": round(sec, 2),
+            "how": f"the reference's 2D timestep_cuda_ run on {per_size} instances of each size "
+                   f"of the ensemble, {steps} steps each, one call per instance"}
 
 
 def run_e2e(args, dev, dist, world, rank, precision=32):
@@ -878,8 +982,14 @@ def main():
     ap.add_argument("--grid", type=int, default=256,
                     help="grid size (256 is the benchmark; smaller grids are for profiling)")
     ap.add_argument("--no-upo", action="store_true", help="skip the UPO Newton leg")
-    ap.add_argument("--upo-newton", type=int, default=1,
-                    help="Newton iterations per guess in the UPO leg")
+    ap.add_argument("--upo-newton", type=int, default=3,
+                    help="largest number of Newton iterations per guess in the UPO leg")
+    ap.add_argument("--upo-all-forms", action="store_true",
+                    help="also solve with the FP64 exact tangent")
+    ap.add_argument("--no-upo-plain", action="store_true",
+                    help="skip the run of the reference's plain UPO form")
+    ap.add_argument("--upo-only", action="store_true",
+                    help="run the UPO leg alone and print its JSON")
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
                     help="run the FP32-vs-FP64 accuracy study over STEPS steps instead")
     ap.add_argument("--adjoint", type=int, default=0, metavar="STEPS",
@@ -910,6 +1020,12 @@ def main():
     if args.adjoint:
         if rank == 0:
             print(json.dumps(run_adjoint(args)), flush=True)
+        return
+    if args.upo_only:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(0)
+            print(json.dumps(run_upo(args)), flush=True)
         return
     if args.impl == "reference":
         # rank 0 alone times the reference; the other ranks exit without work

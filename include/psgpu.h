@@ -188,12 +188,40 @@ int psg_rec3d_add_engine(psg_rec3d* h, int nt, psg_ns3d* engine, int* emitted);
 int psg_rec3d_count(psg_rec3d* h);
 long psg_rec3d_launches(psg_rec3d* h);
 
+/* Near-recurrence search for UPO guesses of 2D runs, batched over nrun runs of
+ * one grid (2D_NavierStokes/src_RK4/functions.h:105-309): per run a ring of
+ * store_size states; every output interval each run's newest state is
+ * compared with its earlier ones under nshift_x * nshift_y trial
+ * translations (2 pi i / (nshift_x alpha), 2 pi j / nshift_y) over the 2 W^2
+ * modes of the box 0 <= kx < W, -W <= ky < W (W = norm_width), and the
+ * reference's selection logic emits a guess when a run's minimum residual
+ * enters and then leaves the threshold.  psg_rec2d_start takes the initial
+ * states, psg_rec2d_add the states after step nt (nt = NOUT, 2 NOUT, ...):
+ * states[r] is run r's device box (complex of `precision`, [2K+1][K+1], e.g.
+ * psg_batch2d_device_state); *emitted counts the guesses this call added.
+ * psg_rec2d_guess returns guess k: meta[7] = run, start time, v2, period,
+ * shift x, shift y, residual, and its state (complex128 box, may be null). */
+typedef struct psg_rec2d psg_rec2d;
+int psg_rec2d_create(psg_rec2d** h, int nrun, int n, double alpha, int store_size,
+                     int norm_width, int nshift_x, int nshift_y, double threshold, int nout,
+                     double dt, double tstart, const double* v2);
+void psg_rec2d_destroy(psg_rec2d* h);
+int psg_rec2d_set_stream(psg_rec2d* h, void* cuda_stream);
+int psg_rec2d_start(psg_rec2d* h, void* const* states, int precision);
+int psg_rec2d_add(psg_rec2d* h, int nt, void* const* states, int precision, int* emitted);
+int psg_rec2d_count(psg_rec2d* h);
+int psg_rec2d_guess(psg_rec2d* h, int k, double* meta, double* Z);
+long psg_rec2d_launches(psg_rec2d* h);
+
 /* ---------------------------------------------------------------- UPO search */
 /* Batched Newton-GMRES-hookstep search for unstable periodic orbits of 2D
  * Kolmogorov flow (2D_NavierStokes/src_RK4/src_gmres/main.F90:688-1823), all
- * guesses in lock step, integrations in FP64 on the GPU.  jv_mode 0: exact
- * tangent Jacobian-vector products of the discrete step; 1: the reference's
- * forward difference (eps = 1e-7).  kmax: Krylov dimension (GMRESMAX). */
+ * guesses in lock step, on the GPU.  jv_mode 0: exact tangent
+ * Jacobian-vector products of the discrete step in FP64; 1: the reference's
+ * forward difference (eps = 1e-7) of FP64 integrations; 2: the exact tangent
+ * with base and tangent integrated in FP32 (Krylov products only: Phi_T, the
+ * residual, dz/dt, Arnoldi and the hookstep stay FP64).  kmax: Krylov
+ * dimension (GMRESMAX). */
 typedef struct psg_upo2d psg_upo2d;
 
 #define PSG_UPO_ACTIVE 0
@@ -219,6 +247,12 @@ int psg_upo2d_get(psg_upo2d* h, int i, double* Z, double* vals, int* info);
 /* building blocks at guess i (unshifted): mode 1 Phi_T(z) -> Zout; mode 0 also
  * the tangent dPhi_T(z) q (q in/out); mode 2 dz/dt -> Zout */
 int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, double* q);
+/* per-Newton-step record k of guess i, rec[10] = {Newton index, GMRES
+ * iterations of the step, hookstep trials, Delta after the step, mu of the
+ * last trial, T, shift x, residual |F|/|Phi_T(z)|, |F|, time step}; the
+ * quantities the reference prints per step (src_gmres/main.F90:1225-1760) */
+int psg_upo2d_trace(psg_upo2d* h, int i, int k, double* rec);
+int psg_upo2d_trace_count(psg_upo2d* h, int i);
 long psg_upo2d_integrations(psg_upo2d* h);
 long psg_upo2d_launches(psg_upo2d* h);
 

@@ -109,6 +109,16 @@ def _declare_2d(L):
     L.psg_rec3d_add.argtypes = [vp, i, C.POINTER(vp), C.POINTER(i)]
     L.psg_rec3d_guess.argtypes = [vp, dp, dp, dp, dp]
     L.psg_rec3d_count.argtypes = [vp]
+    L.psg_rec2d_create.argtypes = [C.POINTER(vp), i, i, d, i, i, i, i, d, i, d, d, dp]
+    L.psg_rec2d_destroy.argtypes = [vp]
+    L.psg_rec2d_destroy.restype = None
+    L.psg_rec2d_set_stream.argtypes = [vp, vp]
+    L.psg_rec2d_start.argtypes = [vp, C.POINTER(vp), i]
+    L.psg_rec2d_add.argtypes = [vp, i, C.POINTER(vp), i, C.POINTER(i)]
+    L.psg_rec2d_count.argtypes = [vp]
+    L.psg_rec2d_guess.argtypes = [vp, i, dp, dp]
+    L.psg_rec2d_launches.argtypes = [vp]
+    L.psg_rec2d_launches.restype = C.c_long
     L.psg_upo2d_create.argtypes = [C.POINTER(vp), i, i, i, i]
     L.psg_upo2d_destroy.argtypes = [vp]
     L.psg_upo2d_destroy.restype = None
@@ -118,6 +128,8 @@ def _declare_2d(L):
     L.psg_upo2d_apply.argtypes = [vp, i, i, dp, dp]
     L.psg_upo2d_integrations.argtypes = [vp]
     L.psg_upo2d_integrations.restype = C.c_long
+    L.psg_upo2d_trace.argtypes = [vp, i, i, dp]
+    L.psg_upo2d_trace_count.argtypes = [vp, i]
     L.psg_upo2d_launches.argtypes = [vp]
     L.psg_upo2d_launches.restype = C.c_long
 
@@ -317,6 +329,12 @@ class Batch2D:
         _check(lib().psg_batch2d_download(self._h, i, a.ctypes.data_as(C.POINTER(C.c_double))))
         return a
 
+    def device_state(self, i: int) -> int:
+        """device address of instance i's state (complex of the batch precision)"""
+        p = C.c_void_p()
+        _check(lib().psg_batch2d_device_state(self._h, i, C.byref(p)))
+        return p.value
+
     def _params(self, nu, dt, nsteps):
         m = len(self.sizes)
         nu = np.broadcast_to(np.asarray(nu, np.float64), (m,)).copy()
@@ -405,6 +423,67 @@ class Recurrence3D:
         return int(lib().psg_rec3d_count(self._h))
 
 
+class Recurrence2D:
+    """Near-recurrence search over rings of stored 2D states, batched over the
+    runs of an ensemble (the 2D DNS's UPO guess generator), residuals on the
+    GPU.  States are device boxes, one per run: torch CUDA tensors or the
+    instances of a Batch2D of one grid size."""
+
+    def __init__(self, nrun, n, nout, dt, threshold, v2, store_size=500, norm_width=8,
+                 nshift=(32, 4), alpha=1.0, tstart=0.0):
+        h = C.c_void_p()
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(v2, np.float64), (nrun,)))
+        _check(lib().psg_rec2d_create(C.byref(h), nrun, n, alpha, store_size, norm_width,
+                                      nshift[0], nshift[1], threshold, nout, dt, tstart,
+                                      v.ctypes.data_as(C.POINTER(C.c_double))))
+        self._h = h
+        self.nrun = nrun
+        self.grid = Grid2D(n)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().psg_rec2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ptrs(self, states):
+        if isinstance(states, Batch2D):
+            ptrs = [states.device_state(i) for i in range(self.nrun)]
+            return (C.c_void_p * self.nrun)(*ptrs), states.precision
+        prec = 64 if states[0].dtype in (getattr(__import__("torch"), "complex128"),) else 32
+        return (C.c_void_p * self.nrun)(*[t.data_ptr() for t in states]), prec
+
+    def start(self, states):
+        p, prec = self._ptrs(states)
+        _check(lib().psg_rec2d_start(self._h, p, prec))
+
+    def add(self, nt, states) -> int:
+        """the states after step nt; returns the number of guesses emitted"""
+        p, prec = self._ptrs(states)
+        e = C.c_int()
+        _check(lib().psg_rec2d_add(self._h, int(nt), p, prec, C.byref(e)))
+        return int(e.value)
+
+    @property
+    def count(self) -> int:
+        return int(lib().psg_rec2d_count(self._h))
+
+    def guess(self, k):
+        meta = np.zeros(7)
+        Z = np.zeros(self.grid.shape, np.complex128)
+        dp = C.POINTER(C.c_double)
+        _check(lib().psg_rec2d_guess(self._h, k, meta.ctypes.data_as(dp), Z.ctypes.data_as(dp)))
+        keys = ("run", "time", "v2", "period", "shift_x", "shift_y", "residual")
+        d = dict(zip(keys, meta.tolist()))
+        d["run"] = int(d["run"])
+        return d, Z
+
+
 UPO_STATUS = {0: "ACTIVE", 1: "CONVERGED", 2: "GMRES FAILED", 3: "H-STEP FAILED", 4: "NEWTON STALLED",
               5: "T-STEP FAILED", 6: "PERIOD TOO SMALL", 7: "NEWTON FAILED"}
 
@@ -413,9 +492,17 @@ class UPO2D:
     """Batched Newton-GMRES-hookstep search for periodic orbits of 2D Kolmogorov
     flow (all guesses of one grid size, FP64 integrations on the GPU)."""
 
-    def __init__(self, nguess: int, n: int, kmax: int = 60, exact_jv: bool = True):
+    def __init__(self, nguess: int, n: int, kmax: int = 60, exact_jv: bool = True,
+                 jv_precision: int = 64):
+        """exact_jv: Krylov products from the exact tangent (jv_precision 64: FP64,
+        32: base and tangent integrated in FP32) or, when False, the reference's
+        FP64 forward difference.  Phi_T, residuals, Arnoldi and the hookstep are
+        FP64 in every form."""
+        if jv_precision not in (32, 64):
+            raise ValueError("jv_precision must be 32 or 64")
+        mode = (0 if jv_precision == 64 else 2) if exact_jv else 1
         h = C.c_void_p()
-        _check(lib().psg_upo2d_create(C.byref(h), nguess, n, kmax, 0 if exact_jv else 1))
+        _check(lib().psg_upo2d_create(C.byref(h), nguess, n, kmax, mode))
         self._h = h
         self.n = n
         self.grid = Grid2D(n)
@@ -459,6 +546,19 @@ class UPO2D:
         _check(lib().psg_upo2d_apply(self._h, i, mode, Z.ctypes.data_as(C.POINTER(C.c_double)),
                                      qq.ctypes.data_as(C.POINTER(C.c_double)) if qq is not None else None))
         return Z, qq
+
+    def trace(self, i):
+        """Per-Newton-step records of guess i: dicts with the Newton index, GMRES
+        iterations and hookstep trials of the step, Delta after it, mu of its last
+        trial, T, shift, residual |F|/|Phi_T(z)|, |F| and the time step in use."""
+        out = []
+        rec = np.zeros(10)
+        for k in range(int(lib().psg_upo2d_trace_count(self._h, i))):
+            _check(lib().psg_upo2d_trace(self._h, i, k, rec.ctypes.data_as(C.POINTER(C.c_double))))
+            out.append({"newton": int(rec[0]), "gmres": int(rec[1]), "hook": int(rec[2]),
+                        "delta": rec[3], "mu": rec[4], "T": rec[5], "sx": rec[6],
+                        "ner": rec[7], "normfn": rec[8], "dt": rec[9]})
+        return out
 
     @property
     def integrations(self):

@@ -33,7 +33,8 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 
 # translation units of libpsgpu.so
 CORE = ["psg_api.cu", "psg_ns3d_api.cu", "psg_ns3d_f32.cu", "psg_ns3d_f64.cu",
-        "psg_ns2d.cu", "psg_newton2d.cu", "psg_recurrence.cu"]
+        "psg_ns2d.cu", "psg_newton2d.cu", "psg_tan2d_f64.cu", "psg_tan2d_f32.cu",
+        "psg_recurrence.cu", "psg_recurrence2d.cu"]
 # host-side C of libpsgpu.so (parameter files, random starts, record I/O)
 HOST_SRC = ["psg_host.c"]
 # driver programs: name -> source (linked to libpsgpu.so)

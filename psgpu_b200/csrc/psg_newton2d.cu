@@ -10,9 +10,12 @@
 // form, not in algorithm:
 //   * all guesses advance in lock step and every integration of a phase (one
 //     per GMRES iteration, one per hookstep trial) is a single persistent
-//     launch over the guesses, in FP64;
-//   * Jv is either the exact tangent of the discrete step (integrated with the
-//     base, psg_tan2d.cuh) or the reference's forward difference (eps = 1e-7);
+//     launch over the guesses;
+//   * Jv is the exact tangent of the discrete step (integrated with the base,
+//     psg_tan2d.cuh) in FP64 or in FP32, or the reference's forward
+//     difference (eps = 1e-7, FP64: a difference quotient of FP32
+//     integrations would be rounding noise).  Phi_T, the residual, dz/dt, the
+//     Arnoldi vectors and the hookstep are FP64 in every mode;
 //   * the Arnoldi orthogonalisation runs on the GPU in FP64, one block per
 //     guess; the small Hessenberg SVD runs on the host (one-sided Jacobi).
 #include <math.h>
@@ -20,51 +23,21 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <vector>
 
-#include "psg_tan2d.cuh"
-#include "psgpu_internal.h"
+#include "psg_tan2d_run.cuh"
 
 namespace psg {
+
+PSG_TAN2D_EXTERN(double)
+PSG_TAN2D_EXTERN(float)
 
 using C2 = cpx<double>;
 
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-// the same integrations with CS blocks per instance (a cluster of CS), for
-// batches too small to fill the device one block per instance; cluster c
-// takes instances c, c + C, ... (all blocks run the same instance sequence)
-template <int N, int CS>
-__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(256)
-    tan2d_cluster(const InstTan2D<double>* __restrict__ insts, int ninst,
-                  const C2* __restrict__ tw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2* smem = reinterpret_cast<C2*>(smem_raw);
-  unsigned rank;
-  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  const Team t{(int)rank, CS};
-  const int ncl = gridDim.x / CS;
-  for (int i = blockIdx.x / CS; i < ninst; i += ncl) Tan2D<double, N>::run(insts[i], tw, smem, t);
-}
-
-template <int N>
-__global__ void __launch_bounds__(256) tan2d_persistent(const InstTan2D<double>* __restrict__ insts,
-                                                        int ninst, int* __restrict__ next,
-                                                        const C2* __restrict__ tw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2* smem = reinterpret_cast<C2*>(smem_raw);
-  __shared__ int s_idx;
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_idx = atomicAdd(next, 1);
-    __syncthreads();
-    const int i = s_idx;
-    if (i >= ninst) break;
-    Tan2D<double, N>::run(insts[i], tw, smem);
-  }
-}
-
 // per-guess descriptor of the vector kernels
 struct VecJob {
   const C2* a;
@@ -285,6 +258,7 @@ struct Guess {
       *zn_trial, *zn2, *fnplus, *fnplus2, *scratch;
   std::vector<C2*> q;  // Krylov basis
   InstTan2D<double> inst;  // integration buffers
+  InstTan2D<float> inst32;  // FP32 integration buffers (exact Jv in FP32)
   // host state
   double T = 0, sx = 0, sy = 0, nu = 0, dt0 = 0, dt_true = 0;
   int rsym = 0;
@@ -305,15 +279,22 @@ struct Guess {
   double dT = 0, dS = 0;
   bool halve = false, dbl = false, hook_done = false;
   int ihook = 0;
+  // one record per Newton step: newton index, GMRES iterations, hookstep
+  // trials, Delta after the step, mu of the last trial, T, shift, residual,
+  // |F|, time step in use
+  std::vector<std::array<double, 10>> trace;
 };
 
 struct Upo2D {
+  // jv_mode 0: exact tangent (FP64), 1: forward difference, 2: exact tangent in FP32
   int ng = 0, n = 0, K = 0, X = 0, Y = 0, nkt = 0, kmax = 0, jv_mode = 0;
   double eps = 1e-7, gmtol = 1e-3;
   std::vector<Guess> G;
   C2* pool = nullptr;
-  C2* tw = nullptr;
-  InstTan2D<double>* d_inst = nullptr;
+  cpx<float>* pool32 = nullptr;
+  IntPlan<double> plan64;
+  IntPlan<float> plan32;
+  CvtJob* d_cvt = nullptr;
   VecJob* d_vec = nullptr;
   DotJob* d_dot = nullptr;
   MgsJob* d_mgs = nullptr;
@@ -323,9 +304,7 @@ struct Upo2D {
   double* d_H = nullptr;
   int* d_next = nullptr;
   cudaStream_t stream = 0;
-  size_t smem = 0;
   long launches = 0, integrations = 0;
-  int grid_cap = 148;
   // blocks per instance (a cluster) when the batch leaves room: at most this many
   int cluster_max = 4;
   // side streams and events of integrations split over several launches
@@ -334,7 +313,10 @@ struct Upo2D {
 
   ~Upo2D() {
     if (pool) cudaFree(pool);
-    if (d_inst) cudaFree(d_inst);
+    if (pool32) cudaFree(pool32);
+    if (d_cvt) cudaFree(d_cvt);
+    plan64.release();
+    plan32.release();
     if (d_vec) cudaFree(d_vec);
     if (d_dot) cudaFree(d_dot);
     if (d_mgs) cudaFree(d_mgs);
@@ -382,17 +364,23 @@ struct Upo2D {
       U_.qn.assign(2 * (kmax + 1), 0.0);
       U_.H.assign((size_t)(kmax + 1) * kmax, 0.0);
     }
-    tw = pool + per * ng;
-    std::vector<C2> h(2 * n);
-    switch (n) {
-      case 16: LineFFT<16, 1, double>::host_table(h.data()); LineFFT<16, 1, double, true>::host_table(h.data() + n); break;
-      case 32: LineFFT<32, 1, double>::host_table(h.data()); LineFFT<32, 1, double, true>::host_table(h.data() + n); break;
-      case 64: LineFFT<64, 1, double>::host_table(h.data()); LineFFT<64, 1, double, true>::host_table(h.data() + n); break;
-      case 128: LineFFT<128, 1, double>::host_table(h.data()); LineFFT<128, 1, double, true>::host_table(h.data() + n); break;
-      default: LineFFT<256, 1, double>::host_table(h.data()); LineFFT<256, 1, double, true>::host_table(h.data() + n); break;
+    if (int rc = plan64.init(n, ng, pool + per * ng)) return rc;
+    if (jv_mode == 2) {
+      // FP32 base + tangent buffers and twiddles for the Krylov products
+      const long per32 = 10L * nkt + work;
+      PSG_CUDA_TRY(cudaMalloc(&pool32, sizeof(cpx<float>) * (per32 * ng + twl)));
+      PSG_CUDA_TRY(cudaMemset(pool32, 0, sizeof(cpx<float>) * (per32 * ng + twl)));
+      for (int g = 0; g < ng; ++g) {
+        cpx<float>* p = pool32 + per32 * g;
+        InstTan2D<float>& I = G[g].inst32;
+        I.n = n;
+        I.Z = p; p += nkt; I.Z0 = p; p += nkt; I.Z1 = p; p += nkt; I.Z2 = p; p += nkt; I.Z3 = p; p += nkt;
+        I.D = p; p += nkt; I.D0 = p; p += nkt; I.D1 = p; p += nkt; I.D2 = p; p += nkt; I.D3 = p; p += nkt;
+        I.work = p;
+      }
+      if (int rc = plan32.init(n, ng, pool32 + per32 * ng)) return rc;
     }
-    PSG_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C2) * 2 * n, cudaMemcpyHostToDevice));
-    PSG_CUDA_TRY(cudaMalloc(&d_inst, sizeof(InstTan2D<double>) * ng));
+    PSG_CUDA_TRY(cudaMalloc(&d_cvt, sizeof(CvtJob) * 2 * ng));
     PSG_CUDA_TRY(cudaMalloc(&d_vec, sizeof(VecJob) * ng));
     PSG_CUDA_TRY(cudaMalloc(&d_dot, sizeof(DotJob) * ng * 4));
     PSG_CUDA_TRY(cudaMalloc(&d_mgs, sizeof(MgsJob) * ng));
@@ -405,52 +393,9 @@ struct Upo2D {
     for (int g = 0; g < ng; ++g)
       for (int j = 0; j <= kmax; ++j) qp[(size_t)g * (kmax + 1) + j] = G[g].q[j];
     PSG_CUDA_TRY(cudaMemcpy(d_qptr, qp.data(), sizeof(C2*) * qp.size(), cudaMemcpyHostToDevice));
-    int gg = 0, sm = 0;
-    switch (n) {
-      case 16: gg = LineFFT<16, 1, double>::G; sm = LineFFT<16, 1, double>::SMEM; break;
-      case 32: gg = LineFFT<32, 1, double>::G; sm = LineFFT<32, 1, double>::SMEM; break;
-      case 64: gg = LineFFT<64, 1, double>::G; sm = LineFFT<64, 1, double>::SMEM; break;
-      case 128: gg = LineFFT<128, 1, double>::G; sm = LineFFT<128, 1, double>::SMEM; break;
-      default: gg = LineFFT<256, 1, double>::G; sm = LineFFT<256, 1, double>::SMEM; break;
-    }
-    smem = sizeof(C2) * (2 * n + (256 / gg) * sm);
-    PSG_CUDA_TRY(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(cluster_kernel(2), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    PSG_CUDA_TRY(cudaFuncSetAttribute(cluster_kernel(4), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    int dev = 0, nsm = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(), 256, smem);
-    grid_cap = nsm * std::max(occ, 1);
     // PSG_UPO_CLUSTER: the largest cluster an integration may use (1, 2 or 4)
     if (const char* e = getenv("PSG_UPO_CLUSTER")) cluster_max = atoi(e);
     return PSG_OK;
-  }
-
-  template <int CS>
-  const void* cluster_kernel_cs() const {
-    switch (n) {
-      case 16: return (const void*)tan2d_cluster<16, CS>;
-      case 32: return (const void*)tan2d_cluster<32, CS>;
-      case 64: return (const void*)tan2d_cluster<64, CS>;
-      case 128: return (const void*)tan2d_cluster<128, CS>;
-      default: return (const void*)tan2d_cluster<256, CS>;
-    }
-  }
-  const void* cluster_kernel(int cs) const {
-    return cs == 4 ? cluster_kernel_cs<4>() : cluster_kernel_cs<2>();
-  }
-
-  const void* kernel() const {
-    switch (n) {
-      case 16: return (const void*)tan2d_persistent<16>;
-      case 32: return (const void*)tan2d_persistent<32>;
-      case 64: return (const void*)tan2d_persistent<64>;
-      case 128: return (const void*)tan2d_persistent<128>;
-      default: return (const void*)tan2d_persistent<256>;
-    }
   }
 
   // ----- batched integration: for every guess in `who`, integrate from z_in
@@ -464,12 +409,37 @@ struct Upo2D {
   };
   int integrate(const std::vector<IntReq>& reqs) {
     if (reqs.empty()) return PSG_OK;
-    std::vector<InstTan2D<double>> h;
+    // the Krylov products (mode 0) of jv_mode 2 integrate base and tangent in
+    // FP32; every other integration (Phi_T, dz/dt, FP64 tangents) in FP64
+    bool fp32 = jv_mode == 2;
+    for (const IntReq& r : reqs) fp32 = fp32 && r.mode == 0;
+    return fp32 ? integrate_t<float>(reqs, plan32) : integrate_t<double>(reqs, plan64);
+  }
+
+  InstTan2D<double>& inst_of(Guess& U_, double*) { return U_.inst; }
+  InstTan2D<float>& inst_of(Guess& U_, float*) { return U_.inst32; }
+
+  int convert(const std::vector<CvtJob>& jobs, bool to32) {
+    if (jobs.empty()) return PSG_OK;
+    PSG_CUDA_TRY(cudaMemcpyAsync(d_cvt, jobs.data(), sizeof(CvtJob) * jobs.size(),
+                                 cudaMemcpyHostToDevice, stream));
+    if (to32) cvt_launch<float>(d_cvt, (int)jobs.size(), nkt, stream);
+    else cvt_launch<double>(d_cvt, (int)jobs.size(), nkt, stream);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+
+  template <typename T>
+  int integrate_t(const std::vector<IntReq>& reqs, IntPlan<T>& plan) {
+    constexpr bool is32 = sizeof(T) == 4;
+    std::vector<InstTan2D<T>> h;
+    std::vector<CvtJob> in_jobs, out_jobs;
     for (const IntReq& r : reqs) {
       Guess& U_ = G[r.g];
-      InstTan2D<double> I = U_.inst;
+      InstTan2D<T> I = inst_of(U_, (T*)nullptr);
       I.mode = r.mode;
-      I.nu = U_.nu;
+      I.nu = (T)U_.nu;
       if (r.mode == 2) {
         I.nsteps = 0;
         I.dt = 0;
@@ -478,19 +448,30 @@ struct Upo2D {
         int ns = (int)(r.T / U_.dt_true);
         if (ns < 1) ns = 1;
         I.nsteps = ns;
-        I.dt = r.T / (double)ns;
+        I.dt = (T)(r.T / (double)ns);
       }
-      PSG_CUDA_TRY(cudaMemcpyAsync(I.Z, r.z_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
-      if (r.mode == 0)
-        PSG_CUDA_TRY(cudaMemcpyAsync(I.D, r.d_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
+      if (is32) {
+        // inputs rounded to FP32; outputs widened back into the FP64 buffers
+        in_jobs.push_back(CvtJob{r.z_in, I.Z});
+        in_jobs.push_back(CvtJob{r.d_in, I.D});
+        out_jobs.push_back(CvtJob{I.Z, U_.inst.Z});
+        out_jobs.push_back(CvtJob{I.D, U_.inst.D});
+      } else {
+        PSG_CUDA_TRY(cudaMemcpyAsync(I.Z, r.z_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
+        if (r.mode == 0)
+          PSG_CUDA_TRY(cudaMemcpyAsync(I.D, r.d_in, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream));
+      }
       h.push_back(I);
     }
-    // longest first
+    if (is32)
+      if (int rc = convert(in_jobs, true)) return rc;
     // blocks per guess: every guess starts with one; while blocks are left
-    // (one per SM: the integrator's registers), the guess that would finish
-    // last moves to a cluster of two, then four.  Relative speeds of one, two
-    // and four blocks on one guess (FP64 tangent at 128^2): 1, 1.67, 2.34.
+    // (the resident capacity of the device at the integrator's registers), the
+    // guess that would finish last moves to a cluster of two, then four.
+    // Relative speeds of one, two and four blocks on one guess (FP64 tangent
+    // at 128^2): 1, 1.67, 2.34.
     const int ni = (int)h.size();
+    const int grid_cap = plan.grid_cap;
     std::vector<int> cs(ni, 1);
     auto speed = [](int c) { return c == 4 ? 2.34 : c == 2 ? 1.67 : 1.0; };
     auto work = [&](int i) { return (double)h[i].nsteps * (h[i].mode == 0 ? 5 : 3); };
@@ -512,13 +493,13 @@ struct Upo2D {
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
       return cs[a] != cs[b] ? cs[a] > cs[b] : work(a) > work(b);
     });
-    std::vector<InstTan2D<double>> hs(ni);
+    std::vector<InstTan2D<T>> hs(ni);
     int cnt[3] = {0, 0, 0};  // four, two, one
     for (int i = 0; i < ni; ++i) {
       hs[i] = h[idx[i]];
       ++cnt[cs[idx[i]] == 4 ? 0 : cs[idx[i]] == 2 ? 1 : 2];
     }
-    PSG_CUDA_TRY(cudaMemcpyAsync(d_inst, hs.data(), sizeof(InstTan2D<double>) * ni,
+    PSG_CUDA_TRY(cudaMemcpyAsync(plan.d_inst, hs.data(), sizeof(InstTan2D<T>) * ni,
                                  cudaMemcpyHostToDevice, stream));
     PSG_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
     const int ngroups = (cnt[0] > 0) + (cnt[1] > 0) + (cnt[2] > 0);
@@ -533,6 +514,7 @@ struct Upo2D {
     // all after the copies above and before anything queued later
     if (ngroups > 1) PSG_CUDA_TRY(cudaEventRecord(ev_fork, stream));
     int off = 0;
+    const int csz[3] = {4, 2, 1};
     for (int k = 0; k < 3; ++k) {
       if (!cnt[k]) continue;
       cudaStream_t st = stream;
@@ -540,34 +522,9 @@ struct Upo2D {
         st = side[k];
         PSG_CUDA_TRY(cudaStreamWaitEvent(st, ev_fork, 0));
       }
-      const InstTan2D<double>* d = d_inst + off;
       const int m = cnt[k];
-      if (k == 0) {
-        switch (n) {
-          case 16: tan2d_cluster<16, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
-          case 32: tan2d_cluster<32, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
-          case 64: tan2d_cluster<64, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
-          case 128: tan2d_cluster<128, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
-          default: tan2d_cluster<256, 4><<<4 * m, 256, smem, st>>>(d, m, tw); break;
-        }
-      } else if (k == 1) {
-        switch (n) {
-          case 16: tan2d_cluster<16, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
-          case 32: tan2d_cluster<32, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
-          case 64: tan2d_cluster<64, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
-          case 128: tan2d_cluster<128, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
-          default: tan2d_cluster<256, 2><<<2 * m, 256, smem, st>>>(d, m, tw); break;
-        }
-      } else {
-        const int grid = std::min<int>(m, grid_cap);
-        switch (n) {
-          case 16: tan2d_persistent<16><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
-          case 32: tan2d_persistent<32><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
-          case 64: tan2d_persistent<64><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
-          case 128: tan2d_persistent<128><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
-          default: tan2d_persistent<256><<<grid, 256, smem, st>>>(d, m, d_next, tw); break;
-        }
-      }
+      tan2d_launch<T>(n, csz[k], m, std::min<int>(m, grid_cap), plan.smem, st, plan.d_inst + off,
+                      d_next, plan.tw);
       PSG_CUDA_TRY(cudaGetLastError());
       if (ngroups > 1) {
         PSG_CUDA_TRY(cudaEventRecord(ev_join[k], st));
@@ -576,6 +533,8 @@ struct Upo2D {
       ++launches;
       off += m;
     }
+    if (is32)
+      if (int rc = convert(out_jobs, false)) return rc;
     integrations += (long)ni;
     return PSG_OK;
   }
@@ -647,7 +606,7 @@ struct Upo2D {
               const std::vector<double>& qs, const std::vector<double>& qt, C2* Guess::*out) {
     std::vector<IntReq> reqs;
     std::vector<VecJob> jobs;
-    if (jv_mode == 0) {
+    if (jv_mode != 1) {
       for (size_t i = 0; i < who.size(); ++i)
         reqs.push_back(IntReq{who[i], G[who[i]].z, q[i], G[who[i]].T, 0});
       if (int rc = integrate(reqs)) return rc;
@@ -867,7 +826,11 @@ struct Upo2D {
             U_.m = k + 1;
             U_.gmres_done = true;
             U_.gmres += k + 1;
-            if (gmr > gmtol) U_.status = UPO_GMRES_FAILED;
+            if (gmr > gmtol) {
+              U_.status = UPO_GMRES_FAILED;
+              U_.trace.push_back({(double)U_.newton, (double)(k + 1), 0.0, U_.delta, 0.0, U_.T,
+                                  U_.sx, U_.ner, U_.normfn, U_.dt_true});
+            }
           }
         }
       }
@@ -990,11 +953,30 @@ struct Upo2D {
         }
       }
       // ------------------------------------------------------------- update
-      std::vector<int> up;
+      std::vector<int> up, redo;
       for (int g : ha) {
         Guess& U_ = G[g];
         U_.hook += U_.ihook;
-        if (U_.status != UPO_ACTIVE) continue;
+        const bool blown = U_.nfpred != U_.nfpred || U_.nfplus != U_.nfplus;
+        if (blown) {
+          // a trial integration blew up: halve the time step and redo the
+          // Newton step from the same z, T, s (src_gmres/main.F90:1636-1665)
+          U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
+                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true});
+          if (U_.dt_true < 0.1 * U_.dt0) {
+            U_.status = UPO_TSTEP_FAILED;
+          } else {
+            U_.dt_true *= 0.5;
+            U_.status = UPO_ACTIVE;
+            redo.push_back(g);
+          }
+          continue;
+        }
+        if (U_.status != UPO_ACTIVE) {
+          U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
+                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true});
+          continue;
+        }
         up.push_back(g);
         cudaMemcpyAsync(U_.zn, U_.zn_trial, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
         cudaMemcpyAsync(U_.z, U_.zplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
@@ -1003,6 +985,8 @@ struct Upo2D {
         U_.sx = U_.Splus;
         U_.normfn = U_.nfplus;
       }
+      // the shifted final state of a redone step is rebuilt from the old Phi_T(z)
+      if (int rc = shift(redo, &Guess::znshift, (const C2* Guess::*)&Guess::zn, &Guess::sx)) return rc;
       if (int rc = shift(up, &Guess::znshift, (const C2* Guess::*)&Guess::zn, &Guess::sx)) return rc;
       std::vector<std::pair<const C2*, const C2*>> ab;
       for (int g : up) ab.push_back({G[g].zn, G[g].zn});
@@ -1012,20 +996,27 @@ struct Upo2D {
         Guess& U_ = G[up[i]];
         U_.normz = sqrt(d[i]);
         const double ner = U_.normfn / U_.normz;
+        U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
+                            U_.T, U_.sx, ner, U_.normfn, U_.dt_true});
         if (ner != ner) { U_.status = UPO_TSTEP_FAILED; continue; }
-        // stall detection (src_gmres/main.F90:1752-1765)
+        // stall detection before the convergence test, as the reference
+        // orders them (src_gmres/main.F90:1752-1804)
         const double rel = fabs((ner - U_.ner_old) / ner);
+        bool stalled = false;
         if (rel < 0.001) {
-          if (++U_.ner_count > 3) U_.status = UPO_STALLED;
+          stalled = ++U_.ner_count > 3;
         } else {
           U_.ner_count = 0;
         }
         U_.ner_old = ner;
         U_.ner = ner;
-        if (ner <= tol) U_.status = UPO_CONVERGED;
+        if (stalled) U_.status = UPO_STALLED;
+        else if (ner <= tol) U_.status = UPO_CONVERGED;
         else if (U_.T < 0.1) U_.status = UPO_PERIOD_TOO_SMALL;
-        else if (U_.newton >= max_newton && U_.status == UPO_ACTIVE) U_.status = UPO_NEWTON_FAILED;
+        else if (U_.newton >= max_newton) U_.status = UPO_NEWTON_FAILED;
       }
+      for (int g : redo)
+        if (G[g].newton >= max_newton) G[g].status = UPO_NEWTON_FAILED;
     }
     for (int g = 0; g < ng; ++g)
       if (G[g].status == UPO_ACTIVE) G[g].status = UPO_NEWTON_FAILED;
@@ -1050,7 +1041,10 @@ struct psg_upo2d {
 extern "C" int psg_upo2d_create(psg_upo2d** out, int nguess, int n, int kmax, int jv_mode) {
   if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
   *out = nullptr;
-  if (jv_mode != 0 && jv_mode != 1) { psg_set_error("jv_mode: 0 exact tangent, 1 finite difference"); return PSG_ERR_ARG; }
+  if (jv_mode < 0 || jv_mode > 2) {
+    psg_set_error("jv_mode: 0 exact tangent, 1 finite difference, 2 exact tangent in FP32");
+    return PSG_ERR_ARG;
+  }
   psg_upo2d* h = new psg_upo2d();
   h->u = new Upo2D();
   int rc = h->u->init(nguess, n, kmax, jv_mode);
@@ -1085,6 +1079,7 @@ extern "C" int psg_upo2d_set_guess(psg_upo2d* h, int i, const double* Z, double 
   if (fabs(T - nearbyint(T / dt) * dt) < 1e-10) g.T = nearbyint(T / dt) * dt;
   g.delta = 0.1; g.status = UPO_ACTIVE; g.newton = g.gmres = g.hook = 0;
   g.ner_old = 0; g.ner_count = 0;
+  g.trace.clear();
   return PSG_OK;
 }
 
@@ -1123,6 +1118,25 @@ extern "C" int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, doub
   if (mode == 0) PSG_CUDA_TRY(cudaMemcpy(q, g.inst.D, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
   if (mode == 2 && Zout) PSG_CUDA_TRY(cudaMemcpy(Zout, g.inst.D, sizeof(C2) * U.nkt, cudaMemcpyDeviceToHost));
   return PSG_OK;
+}
+
+// the per-Newton-step record k of guess i (rec[10]; see Guess::trace)
+extern "C" int psg_upo2d_trace(psg_upo2d* h, int i, int k, double* rec) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  if (i < 0 || i >= U.ng || !rec) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  const Guess& g = U.G[i];
+  if (k < 0 || k >= (int)g.trace.size()) {
+    psg_set_error("guess %d has %d trace records", i, (int)g.trace.size());
+    return PSG_ERR_ARG;
+  }
+  for (int j = 0; j < 10; ++j) rec[j] = g.trace[k][j];
+  return PSG_OK;
+}
+
+extern "C" int psg_upo2d_trace_count(psg_upo2d* h, int i) {
+  if (!h || !h->u || i < 0 || i >= h->u->ng) return -1;
+  return (int)h->u->G[i].trace.size();
 }
 
 extern "C" long psg_upo2d_integrations(psg_upo2d* h) { return (h && h->u) ? h->u->integrations : -1; }
