@@ -105,6 +105,17 @@ int psg_ns3d_download_device(psg_ns3d* h, void* const* comps);
  * 3D_NavierStokes/src/functions.h:139-152), out[1] = sum |w|^2 (enstrophy),
  * out[2] = sum |rho|^2 (Boussinesq; 0 otherwise) */
 int psg_ns3d_energetics(psg_ns3d* h, double* out);
+/* max |u| over the grid of the physical x-velocity of the state the next step
+ * starts from, reduced on the device (RK4 schemes; the Boussinesq DNS's CFL
+ * input, 3D_Boussinesq/src/out_low.h:14).  One right-hand-side evaluation;
+ * the state is unchanged. */
+int psg_ns3d_max_velocity(psg_ns3d* h, double* umax);
+/* Boussinesq scheme: FP64 sums over the kept modes of the state, as the DNS's
+ * computeStats forms them (3D_Boussinesq/src/functions.h:288-362): out[0] =
+ * sum Re(conj(b) rho) with b = v sin(theta) + w cos(theta) from the spectral
+ * velocity (the buoyancy flux before the factor Ri), out[1] = Re zeta at
+ * (kx, ky, kz) = (0, kf, 0), the forced mode (0 when it is not kept) */
+int psg_ns3d_buoyancy_flux(psg_ns3d* h, double* out);
 
 /* Tangent-linear and adjoint of the RK4/CN step (PSG_SCHEME_NS_RK4, and
  * PSG_SCHEME_BOUS_RK4 with the density as a fourth component), exact to

@@ -8,7 +8,7 @@
  * drop-in library exports the same symbol names with the same argument
  * lists, so a driver links against it unchanged.  Every flavour exports
  * timestep_cuda_, hence one library per flavour; define exactly one of
- * PSG_ABI_NS2D, PSG_ABI_NS3D, PSG_ABI_EULER3D, PSG_ABI_BOUS3D before including
+ * PSG_ABI_NS2D, PSG_ABI_NS3D, PSG_ABI_EULER3D, PSG_ABI_BOUS3D, PSG_ABI_BOUS3D_DNS before including
  * this header to get that flavour's prototypes (PSG_ABI_NS3D_NEWTON for the
  * Newton-solver build's 3D step).
  *
@@ -74,10 +74,24 @@ void timestep_cuda_(double2* xii, double2* eta, double2* zet, double* xir, doubl
                     int* NZ, int* NSTOP, int* NOUT, int* NOUTV, int* statsFLAG);
 #endif
 
+#if defined(PSG_ABI_BOUS3D_DNS) || defined(PSG_FLAVOUR_BOUS3D_DNS)
+/* 3D Boussinesq RK4/CN as its DNS build steps it (libpsg_bous3d_dns.so):
+ * steps while t <= Tstep, the CFL-adaptive time step (adaptFLAG = 1) and the
+ * forcing throttle towards Dtarget at output times; replaces
+ * 3D_Boussinesq/src/cuda.cu:21-117 (called from src/main.F90:224-226). */
+void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
+                    double* ky, double* kz, double* Time, double* TSTART, double* Tstep,
+                    double* AMPFOR, double* DELT, double* ResThresh, double* KFY, double* V2,
+                    double* Ri, double* Sc, double* Theta, double* alpha, double* Dtarget,
+                    int* ikF, int* ikN, int* LC, int* IKTX, int* IKTY, int* IKTZ, int* KTZ,
+                    int* NKT, int* NX, int* NY, int* NZ, int* NOUT, int* NOUTV,
+                    int* statsFLAG, int* RecFLAG, int* adaptFLAG, int* RANK);
+#endif
+
 #if defined(PSG_ABI_BOUS3D) || defined(PSG_FLAVOUR_BOUS3D)
-/* 3D Boussinesq RK4 with per-stage Crank-Nicolson factors; replaces
- * 3D_Boussinesq/src/src_gmres/cuda.cu:12-49 (and the DNS build's signature
- * 3D_Boussinesq/src/cuda.cu:21-58, called from src/main.F90:224-226). */
+/* 3D Boussinesq RK4 with per-stage Crank-Nicolson factors as the Newton
+ * solver's build steps it (libpsg_bous3d.so: full steps while Tstep - t > dt,
+ * then one shorter step); replaces 3D_Boussinesq/src/src_gmres/cuda.cu:12-49. */
 void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
                     double* ky, double* kz, double* Time, double* TSTART, double* Tstep,
                     double* AMPFOR, double* DELT, double* ResThresh, double* KFY, double* V2,

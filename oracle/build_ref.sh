@@ -32,6 +32,9 @@ build ns2d     2D_NavierStokes/src_RK4           2D_NavierStokes/src_RK4/src_gmr
 build ns3d     3D_NavierStokes/src               3D_NavierStokes/src/cuda.cu &
 build euler3d  3D_Euler/src                      3D_Euler/src/cuda.cu &
 build bous3d   3D_Boussinesq/src                 3D_Boussinesq/src/src_gmres/cuda.cu &
+# the Boussinesq DNS build: adaptive time step and forcing throttle; writes its
+# diagnostics under JOB<rank>/ of the working directory
+build bous3d_dns 3D_Boussinesq/src               3D_Boussinesq/src/cuda.cu &
 # the 3D NS Newton-solver step (18 arguments, grid fixed at 128^3 by its kernels.h)
 build ns3d_gmres 3D_NavierStokes/src_gmres       3D_NavierStokes/src_gmres/cuda.cu &
 # The 3D NS DNS build formats "JOB0/xii001.raw" (16 bytes) into a 14-byte

@@ -45,6 +45,7 @@ DROPINS = {
     "ns3d_newton": ("psg_dropin3d.cu", "PSG_FLAVOUR_NS3D_NEWTON"),
     "euler3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_EULER3D"),
     "bous3d": ("psg_dropin3d.cu", "PSG_FLAVOUR_BOUS3D"),
+    "bous3d_dns": ("psg_dropin3d.cu", "PSG_FLAVOUR_BOUS3D_DNS"),
     "ns2d": ("psg_dropin2d.cu", "PSG_FLAVOUR_NS2D"),
 }
 

@@ -1,7 +1,7 @@
 // psg_dropin3d.cu -- reference-compatible timestep_cuda_ entry points (3D).
 //
 // Compiled once per flavour (-DPSG_FLAVOUR_NS3D / _NS3D_NEWTON / _EULER3D /
-// _BOUS3D) into
+// _BOUS3D / _BOUS3D_DNS) into
 // libpsg_<flavour>.so, because every flavour exports the same Fortran-mangled
 // symbol.  The argument lists are the reference's, all by pointer; the state
 // arrays are overwritten in place exactly as the reference does.  Unlike the
@@ -241,6 +241,94 @@ extern "C" void timederiv_cuda_(double2* xii, double2* eta, double2* zet, double
   }
 }
 
+#elif defined(PSG_FLAVOUR_BOUS3D_DNS)
+
+// The Boussinesq DNS build's step (3D_Boussinesq/src/cuda.cu:21-117): the
+// same 38 arguments as the Newton-solver build, a different loop.
+//   * the step: delt = Tstep/nStop when nStop*DELT != Tstep (nStop = Tstep/DELT
+//     in floating point), else DELT (init.h:23-29); steps while tme <= Tstep;
+//   * an output time is one that the previous step crossed: a multiple of
+//     Tout = NOUT*delt in (tme - delt + small, tme + small], small = 1e-10
+//     (out_low.h:8-9);
+//   * at output times with statsFLAG != 0 and adaptFLAG = 1, before the step:
+//     delt = max(C/|Umax|, deltp), C = 2 pi/NX, deltp the initial delt,
+//     Umax = max |u| of the physical x-velocity (out_low.h:11-16);
+//   * at output times with statsFLAG = 1 (or 2 past t = 50), after the step,
+//     the forcing throttle ampfor *= (Dtarget - bflux)/input from the state's
+//     buoyancy flux bflux = Ri sum Re(conj(v sin(theta) + w cos(theta)) rho) and
+//     energy input input = -ampfor Re zeta(0, kf, 0)/kf (functions.h:288-369);
+//   * with Dtarget != 0 the device forcing amplitude is set to the host's
+//     ampfor after every step (cuda.cu:104-106).  The host copy starts as
+//     -AMPFOR (init.h:18) while the device starts from AMPFOR (init.h:138), so
+//     from the first step on the forcing acts with the host's sign, as it
+//     does in the reference.
+// The DNS's diagnostic files (stats.dat, engy.dat, spectra, RiG, pdfs, raw
+// volumes) and its recurrence search (RecFLAG) are not written.
+extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
+                               double* ky, double* kz, double* Time, double* TSTART,
+                               double* Tstep, double* AMPFOR, double* DELT, double* ResThresh,
+                               double* KFY, double* V2, double* Ri, double* Sc, double* Theta,
+                               double* alpha, double* Dtarget, int* ikF, int* ikN, int* LC,
+                               int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT, int* NX,
+                               int* NY, int* NZ, int* NOUT, int* NOUTV, int* statsFLAG,
+                               int* RecFLAG, int* adaptFLAG, int* RANK) {
+  (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)ikF; (void)ikN; (void)LC; (void)NOUTV;
+  (void)RANK;
+  double2* state[4] = {xii, eta, zet, rho};
+  if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha) ||
+      *NOUT < 1) {
+    fill_nan(state, 4, *NKT);
+    return;
+  }
+  psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
+  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
+  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
+  const double small = 1e-10, twopi = 4.0 * asin(1.0);
+  const double nstop = *Tstep / *DELT;
+  double delt = (nstop * *DELT != *Tstep) ? *Tstep / nstop : *DELT;
+  const double C = twopi / *NX, Tout = *NOUT * delt, deltp = delt;
+  double tme = *TSTART;
+  double ampfor = -*AMPFOR;       // host copy
+  double dev_ampfor = *AMPFOR;    // device copy
+  const double dtarget = *Dtarget, kfy = *KFY, ri = *Ri;
+  auto fail = [&]() {
+    report("timestep_cuda_");
+    fill_nan(state, 4, *NKT);
+  };
+  if (!h || psg_ns3d_set_params(h, *V2, dev_ampfor, kfy, ri, *Sc, *Theta) ||
+      psg_ns3d_upload(h, in)) {
+    fail();
+    return;
+  }
+  int timestep = 0;
+  while (tme <= *Tstep) {
+    ++timestep;
+    const double tcrit = Tout * (double)(int)((tme + small) / Tout);
+    const double tcheck = (tme - delt - tcrit + small) * (tme + small - tcrit);
+    if (tcheck < 0.0 && *statsFLAG != 0 && *adaptFLAG == 1) {
+      double umax = 0.0;
+      if (psg_ns3d_max_velocity(h, &umax)) { fail(); return; }
+      delt = fmax(C / fabs(umax), deltp);
+    }
+    if (psg_ns3d_step(h, delt, 1, 0)) { fail(); return; }
+    *Time = *Time + delt;
+    tme += delt;
+    if (tcheck < 0.0 && (*RecFLAG == 1 || *statsFLAG != 0) && timestep != 0 &&
+        (*statsFLAG == 1 || (*statsFLAG == 2 && tme > 50.0))) {
+      double fl[2];
+      if (psg_ns3d_buoyancy_flux(h, fl)) { fail(); return; }
+      const double bflux = ri * fl[0];
+      const double input = -ampfor * fl[1] / kfy;
+      if (dtarget != 0.0) ampfor = ampfor * (dtarget - bflux) / input;
+    }
+    if (*Dtarget != 0 && dev_ampfor != ampfor) {
+      dev_ampfor = ampfor;
+      if (psg_ns3d_set_params(h, *V2, dev_ampfor, kfy, ri, *Sc, *Theta)) { fail(); return; }
+    }
+  }
+  if (psg_ns3d_download(h, out)) fail();
+}
+
 #else
 #error "define PSG_FLAVOUR_NS3D, PSG_FLAVOUR_EULER3D or PSG_FLAVOUR_BOUS3D"
 #endif
@@ -254,7 +342,7 @@ extern "C" void set_gpu_(int* go) {
     printf("cutil error: no devices supporting CUDA\n");
     exit(-1);
   }
-#if defined(PSG_FLAVOUR_BOUS3D)
+#if defined(PSG_FLAVOUR_BOUS3D) || defined(PSG_FLAVOUR_BOUS3D_DNS)
   dev = *go;
   cudaSetDevice(dev);
 #else

@@ -76,6 +76,8 @@ struct Engine3DBase {
   virtual int upload_device(const void* const* comps) = 0;
   virtual int download_device(void* const* comps) = 0;
   virtual int energetics(double* out) = 0;
+  virtual int max_velocity(double* out) = 0;
+  virtual int buoyancy_flux(double* out) = 0;
   virtual int set_forcing_form(int form) = 0;
   virtual int linear(int mode, double dt, const void* const* in, void* const* out) = 0;
   virtual int steps(double dt, int nsteps, int dump_last) = 0;

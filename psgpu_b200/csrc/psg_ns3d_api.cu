@@ -141,6 +141,18 @@ extern "C" int psg_ns3d_energetics(psg_ns3d* h, double* out) {
   return h->e->energetics(out);
 }
 
+extern "C" int psg_ns3d_max_velocity(psg_ns3d* h, double* umax) {
+  PSG_CHECK_HANDLE(h);
+  if (!umax) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  return h->e->max_velocity(umax);
+}
+
+extern "C" int psg_ns3d_buoyancy_flux(psg_ns3d* h, double* out) {
+  PSG_CHECK_HANDLE(h);
+  if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  return h->e->buoyancy_flux(out);
+}
+
 extern "C" int psg_ns3d_linear(psg_ns3d* h, int mode, double dt, void* const* in, void* const* out) {
   PSG_CHECK_HANDLE(h);
   if (!in || !out) { psg_set_error("null vector"); return PSG_ERR_ARG; }

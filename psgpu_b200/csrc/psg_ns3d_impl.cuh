@@ -393,7 +393,8 @@ template <typename T, int N, int NF, int L, int ST>
 __global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G,
                                   (sizeof(T) == 4 && NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt) {
+       const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt,
+       unsigned long long* __restrict__ umax) {
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
   constexpr int RPW = 32 / G, WPB = L / RPW;  // rows per warp tile, warps per block
@@ -483,6 +484,15 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
     R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
     if (!BOUS) release();
+    if (umax) {
+      // max |u| of the physical x-velocity (the Boussinesq DNS's CFL input,
+      // 3D_Boussinesq/src/out_low.h:14): non-negative doubles order as their bits
+      double m = 0.0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) m = fmax(m, fabs((double)u[e]));
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) atomicMax(umax, (unsigned long long)__double_as_longlong(m));
+    }
     if (dump) {
       const long base = row * N;
       const long nr = (long)N * N * N;
@@ -961,6 +971,54 @@ static __global__ void energetics_final(const double* __restrict__ part, int nbl
   }
 }
 
+// Boussinesq fluxes (3D_Boussinesq/src/functions.h:288-362): per block the
+// partial sums of Re(conj(b) rho), b = v sin(theta) + w cos(theta), and of
+// Re zeta at (0, kf, 0); summed by bflux_final in a fixed order
+template <typename T>
+__global__ void __launch_bounds__(256) bflux_partial(Geom3<T> g, Fields4<T> S, double sinth,
+                                                     double costh, double kf,
+                                                     double* __restrict__ part) {
+  const int W = kTileW;
+  const long total = (long)g.XP * g.Y * g.Y;
+  double f = 0.0, zf = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % W);
+    long q = i / W;
+    const int ikz = (int)(q % g.Y); q /= g.Y;
+    const int iky = (int)(q % g.Y);
+    const int ikx = (int)(q / g.Y) * W + w;
+    if (ikx >= g.X || !keep_mode<T>(ikx, iky - g.K, ikz - g.K, g.K, g.alpha)) continue;
+    const double kx = (double)ikx * (double)g.alpha, ky = iky - g.K, kz = ikz - g.K;
+    double wk = kx * kx + ky * ky + kz * kz;
+    wk = wk > 0.001 ? wk : 0.001;
+    const cpx<T> xa = S.c[0][i], ea = S.c[1][i], za = S.c[2][i], ra = S.c[3][i];
+    const double xr = xa.x, xc = xa.y, er = ea.x, ec = ea.y, zr = za.x, zc = za.y;
+    const double vr = (kz * xc - kx * zc) / wk, vc = (kx * zr - kz * xr) / wk;
+    const double wr = (kx * ec - ky * xc) / wk, wc = (ky * xr - kx * er) / wk;
+    const double br = vr * sinth + wr * costh, bc = vc * sinth + wc * costh;
+    f += br * (double)ra.x + bc * (double)ra.y;
+    if (ikx == 0 && ky == kf && kz == 0.0) zf += zr;
+  }
+  __shared__ double s[2][256];
+  s[0][threadIdx.x] = f; s[1][threadIdx.x] = zf;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int k = 0; k < 2; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < 2) part[blockIdx.x * 2 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+static __global__ void bflux_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  if (threadIdx.x < 2) {
+    double a = 0.0;
+    for (int b = 0; b < nblk; ++b) a += part[b * 2 + threadIdx.x];
+    out[threadIdx.x] = a;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // layout conversion between the reference's FP64 boxes and the tile layout
 // ---------------------------------------------------------------------------
@@ -1311,6 +1369,8 @@ struct Engine3D final : Engine3DBase {
   double2* stage_h = nullptr;  // device FP64 staging box
   int* d_status = nullptr;     // device error flag of the bounded waits
   double* d_energ = nullptr;   // energetics partial sums
+  unsigned long long* d_umax = nullptr;  // max |u| of the x-pass (bits of a non-negative double)
+  double* d_flux = nullptr;    // buoyancy-flux partial sums
   // linearised step (tangent / adjoint), allocated on first use
   cpx<T>* lin = nullptr;
   Fields4<T> Zb[4]{};          // base stage states z, z1, z2, z3
@@ -1485,9 +1545,11 @@ struct Engine3D final : Engine3DBase {
     if (dump) cudaFree(dump);
     if (d_status) cudaFree(d_status);
     if (d_energ) cudaFree(d_energ);
+    if (d_umax) cudaFree(d_umax);
+    if (d_flux) cudaFree(d_flux);
     if (lin) cudaFree(lin);
     lin = nullptr;
-    d_energ = nullptr;
+    d_energ = nullptr; d_umax = nullptr; d_flux = nullptr;
     pool = nullptr; stage_h = nullptr; dump = nullptr; d_status = nullptr;
   }
 
@@ -1551,7 +1613,7 @@ struct Engine3D final : Engine3DBase {
   template <int N>
   // nf: fields the x-pass reads (6: -(u x w); 9: + u.grad rho; 7: the
   // Boussinesq adjoint's scalar products); 0: the engine's own
-  int launch_c(int v, T scale, T* dp, int nf = 0) {
+  int launch_c(int v, T scale, T* dp, int nf = 0, unsigned long long* um = nullptr) {
     constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
     constexpr int RPW = 32 / LineFFT<N, 1, T>::G;  // rows per warp tile
     const int wpb = L1 * c_rows_mult(v) / RPW;     // warps per block
@@ -1562,9 +1624,9 @@ struct Engine3D final : Engine3DBase {
     const int th = c_threads<N>(v);
     if (!nf) nf = (scheme == SCHEME_BOUS_RK4) ? 9 : 6;
 #define PSG_LC(LL, STG)                                                                          \
-  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt); \
-  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt); \
-  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt);
+  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
+  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
+  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um);
     switch (v) {
       case 0: PSG_LC(L1, 1); break;
       case 1: PSG_LC(2 * L1, 1); break;
@@ -1662,7 +1724,7 @@ struct Engine3D final : Engine3DBase {
 
   // one right-hand-side evaluation followed by the stage update
   template <int N>
-  int rhs_n(int stage, bool want_dump) {
+  int rhs_n(int stage, bool want_dump, bool want_umax = false) {
     using FG = LineFFT<N, 1, T>;
     const int G = FG::G;
     const dim3 blk(kTileW * G);
@@ -1683,7 +1745,8 @@ struct Engine3D final : Engine3DBase {
     mark(1);
     const T scale = (T)1 / ((T)N * (T)N * (T)N);
     T* dp = want_dump ? dump : nullptr;
-    launch_c<N>(c_variant, scale, dp);
+    if (want_umax) PSG_CUDA_TRY(cudaMemsetAsync(d_umax, 0, sizeof(unsigned long long), stream));
+    launch_c<N>(c_variant, scale, dp, 0, want_umax ? d_umax : nullptr);
     mark(2);
     pass_d<T, N><<<dim3(XT, N, nfo), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
     mark(3);
@@ -1707,13 +1770,13 @@ struct Engine3D final : Engine3DBase {
     return PSG_OK;
   }
 
-  int rhs(int stage, bool want_dump = false) {
+  int rhs(int stage, bool want_dump = false, bool want_umax = false) {
     switch (g.n) {
-      case 16: return rhs_n<16>(stage, want_dump);
-      case 32: return rhs_n<32>(stage, want_dump);
-      case 64: return rhs_n<64>(stage, want_dump);
-      case 128: return rhs_n<128>(stage, want_dump);
-      default: return rhs_n<256>(stage, want_dump);
+      case 16: return rhs_n<16>(stage, want_dump, want_umax);
+      case 32: return rhs_n<32>(stage, want_dump, want_umax);
+      case 64: return rhs_n<64>(stage, want_dump, want_umax);
+      case 128: return rhs_n<128>(stage, want_dump, want_umax);
+      default: return rhs_n<256>(stage, want_dump, want_umax);
     }
   }
 
@@ -2107,6 +2170,50 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaStreamSynchronize(stream));
     return check_status();
   }
+  // max |u| over the grid of the physical x-velocity of the state the next
+  // step starts from (its first right-hand side's input); the evaluation
+  // leaves the state, the stage registers a step uses and the first-step
+  // velocity masking as they were
+  int max_velocity(double* out) override {
+    if (scheme != SCHEME_BOUS_RK4 && scheme != SCHEME_NS_RK4) {
+      psg_set_error("max velocity is provided for the RK4 schemes");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    if (!d_umax) PSG_CUDA_TRY(cudaMalloc(&d_umax, sizeof(unsigned long long)));
+    const int keep = first_rhs;
+    int rc = rhs(STAGE_DERIV, false, true);
+    first_rhs = keep;
+    if (rc) return rc;
+    unsigned long long bits = 0;
+    PSG_CUDA_TRY(cudaMemcpyAsync(&bits, d_umax, sizeof bits, cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    memcpy(out, &bits, sizeof(double));
+    return check_status();
+  }
+
+  // Boussinesq fluxes of the state, FP64 sums over the kept modes as the DNS's
+  // computeStats forms them (3D_Boussinesq/src/functions.h:288-362):
+  // out[0] = sum Re(conj(b) rho), b = v sin(theta) + w cos(theta) with the
+  // spectral velocity (v, w) = (i k x w / max(k^2, 0.001))_{y,z};
+  // out[1] = Re zeta at (kx, ky, kz) = (0, kf, 0) (0 when that mode is not kept)
+  int buoyancy_flux(double* out) override {
+    if (scheme != SCHEME_BOUS_RK4) {
+      psg_set_error("buoyancy flux is defined for the Boussinesq scheme");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    constexpr int kBlk = 296;
+    if (!d_flux) PSG_CUDA_TRY(cudaMalloc(&d_flux, sizeof(double) * (2 * kBlk + 2)));
+    bflux_partial<T><<<kBlk, 256, 0, stream>>>(g, R.S, (double)prm.sinth, (double)prm.costh,
+                                                (double)prm.kf, d_flux);
+    bflux_final<<<1, 32, 0, stream>>>(d_flux, kBlk, d_flux + 2 * kBlk);
+    launches += 2;
+    PSG_CUDA_TRY(cudaGetLastError());
+    PSG_CUDA_TRY(cudaMemcpyAsync(out, d_flux + 2 * kBlk, sizeof(double) * 2,
+                                 cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return check_status();
+  }
+
   int download_stage(double* const* comps) override {
     if (!R.X0.c[0]) { psg_set_error("scheme keeps no stage state"); return PSG_ERR_STATE; }
     return download_from(comps, &R.X0);

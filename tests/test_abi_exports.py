@@ -37,7 +37,8 @@ def test_core_exports_every_declared_symbol():
 @pytest.mark.parametrize("flavour,guard", [("ns2d", "PSG_ABI_NS2D"), ("ns3d", "PSG_ABI_NS3D"),
                                            ("ns3d_newton", "PSG_ABI_NS3D_NEWTON"),
                                            ("euler3d", "PSG_ABI_EULER3D"),
-                                           ("bous3d", "PSG_ABI_BOUS3D")])
+                                           ("bous3d", "PSG_ABI_BOUS3D"),
+                                           ("bous3d_dns", "PSG_ABI_BOUS3D_DNS")])
 def test_dropin_exports(flavour, guard):
     _load("libpsgpu.so")
     L = _load(f"libpsg_{flavour}.so")
