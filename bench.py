@@ -348,7 +348,7 @@ def run_ref2d_probe(steps, n=None):
 UPO_N, UPO_NU, UPO_DT, UPO_GUESSES, UPO_KMAX = 128, 1.0 / 40.0, 0.005, 64, 60
 
 
-def upo_guesses(G=UPO_GUESSES, search=60.0, seed=5000):
+def upo_guesses(G=UPO_GUESSES, search=400.0, seed=5000):
     """64 guesses from turbulent 2D Kolmogorov states, Re = 40, 128^2: 64 seeded
     runs (modes 1 <= |k| <= 8, enstrophy 1) spun up for 500 time units in one
     persistent FP32 launch, then continued for `search` time units under the
@@ -971,6 +971,87 @@ def run_adjoint(args):
     return out
 
 
+# ------------------------------------------------------------ profiling cases
+PROFILE_CASES = ("ns3d_rk4_fp32", "ns3d_rk4_fp64", "bous3d_fp32", "bous3d_fp64", "ns2d_batch",
+                 "upo_tangent64", "upo_tangent32", "adjoint3d", "rec2d")
+
+
+def run_profile_case(name, grid):
+    """One small workload per hot-kernel family, for ncu captures (inputs larger
+    than L2 where the family allows, a handful of launches after a warm-up):
+    ns3d_rk4_* / bous3d_*: two RK4/CN steps at `grid`^3 (default 128) after one
+    warm-up step; ns2d_batch: 148 instances of 128^2, 20 steps; upo_tangent*:
+    one Newton step of 64 guesses at 128^2, T = 1, Krylov dimension 1;
+    adjoint3d: one adjoint step at 64^3; rec2d: 60 checks of the 2D
+    recurrence search over 64 runs at 128^2."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.fields import kolmogorov_ic2d, random_vorticity3d, taylor_green3d
+
+    torch.cuda.set_device(0)
+    n = grid or 128
+    if name.startswith("ns3d_rk4") or name.startswith("bous3d"):
+        prec = 64 if name.endswith("fp64") else 32
+        bous = name.startswith("bous3d")
+        xi, et, zt = taylor_green3d(n, 1234, amp=1e-3)
+        eng = P.NS3D(n, P.SCHEME_BOUS_RK4 if bous else P.SCHEME_NS_RK4, precision=prec, nu=NU,
+                     ri=1.0 if bous else 0.0)
+        eng.upload(*((xi, et, zt, 0.01 * xi) if bous else (xi, et, zt)))
+        eng.step(DT, 1)
+        eng.sync()
+        eng.step(DT, 2)
+        eng.sync()
+        eng.close()
+    elif name == "ns2d_batch":
+        b = P.Batch2D([128] * 148, precision=32)
+        for i in range(148):
+            b.upload(i, kolmogorov_ic2d(128, i))
+        b.run(UPO_NU, UPO_DT, 2)
+        b.sync()
+        b.run(UPO_NU, UPO_DT, 20)
+        b.sync()
+        b.close()
+    elif name.startswith("upo_tangent"):
+        # one Newton step of 64 guesses (T = 1, 200 steps): the residual's Phi_T
+        # launches, two dz/dt launches, then the Krylov products (base +
+        # tangent) of the first GMRES iteration, each one to three launches
+        prec = 32 if name.endswith("32") else 64
+        G = 64
+        u = P.UPO2D(G, 128, kmax=1, exact_jv=True, jv_precision=prec)
+        for i in range(G):
+            u.set_guess(i, kolmogorov_ic2d(128, i), T=1.0, nu=UPO_NU, dt=UPO_DT)
+        u.solve(max_newton=1, tol=1e-10, gmres_tol=1e-3)
+        u.close()
+    elif name == "adjoint3d":
+        nn = grid or 64
+        eng = P.NS3D(nn, P.SCHEME_NS_RK4, precision=64, nu=1 / 400)
+        xi, et, zt = random_vorticity3d(nn, 3, solenoidal=True)
+        eng.upload(xi, et, zt)
+        lam = torch.from_numpy(np.stack([xi, et, zt])).cuda()
+        for _ in range(2):
+            lam = eng.linear(eng.LIN_ADJOINT_STEP, lam, dt=5e-3)
+        eng.sync()
+        eng.close()
+    elif name == "rec2d":
+        G = 64
+        b = P.Batch2D([128] * G, precision=32)
+        for i in range(G):
+            b.upload(i, kolmogorov_ic2d(128, i))
+        rec = P.Recurrence2D(G, 128, 20, UPO_DT, 0.4, UPO_NU, store_size=201, norm_width=8,
+                             nshift=(32, 4))
+        rec.start(b)
+        for k in range(1, 61):
+            b.run(UPO_NU, UPO_DT, 20)
+            rec.add(20 * k, b)
+        b.sync()
+        rec.close()
+        b.close()
+    else:
+        raise SystemExit(f"unknown profile case {name}; one of {PROFILE_CASES}")
+    torch.cuda.synchronize()
+    return {"profile_case": name, "ok": True}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -988,6 +1069,8 @@ def main():
                     help="also solve with the FP64 exact tangent")
     ap.add_argument("--no-upo-plain", action="store_true",
                     help="skip the run of the reference's plain UPO form")
+    ap.add_argument("--profile-case", default="", choices=("",) + PROFILE_CASES,
+                    help="run one small fixed workload of a kernel family (for ncu) and exit")
     ap.add_argument("--upo-only", action="store_true",
                     help="run the UPO leg alone and print its JSON")
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
@@ -1020,6 +1103,10 @@ def main():
     if args.adjoint:
         if rank == 0:
             print(json.dumps(run_adjoint(args)), flush=True)
+        return
+    if args.profile_case:
+        print(json.dumps(run_profile_case(args.profile_case, args.grid if args.grid != 256 else 0)),
+              flush=True)
         return
     if args.upo_only:
         if rank == 0:
