@@ -188,6 +188,14 @@ typedef struct psg_rec3d psg_rec3d;
 int psg_rec3d_create(psg_rec3d** h, int n, double alpha, int store_size, int norm_width,
                      int nshift_x, int nshift_y, int nshift_z, double threshold, int nout,
                      double dt, double tstart, double v2);
+/* The Boussinesq DNS's variant (3D_Boussinesq/src/functions.h:189-205,
+ * 416-616): states of four fields (xii, eta, zet, rho), the density terms
+ * weighted by ri, residuals normalised by the sum of both states' norms,
+ * periods below 0.5 skipped; psg_rec3d_guess_rho returns the guess's density. */
+int psg_rec3d_create_bous(psg_rec3d** h, int n, double alpha, int store_size, int norm_width,
+                          int nshift_x, int nshift_y, int nshift_z, double threshold, int nout,
+                          double dt, double tstart, double v2, double ri);
+int psg_rec3d_guess_rho(psg_rec3d* h, double* rho);
 void psg_rec3d_destroy(psg_rec3d* h);
 int psg_rec3d_set_stream(psg_rec3d* h, void* cuda_stream);
 int psg_rec3d_start(psg_rec3d* h, void* const* state);

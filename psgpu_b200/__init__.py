@@ -109,6 +109,8 @@ def _declare_2d(L):
     L.psg_rec3d_add.argtypes = [vp, i, C.POINTER(vp), C.POINTER(i)]
     L.psg_rec3d_guess.argtypes = [vp, dp, dp, dp, dp]
     L.psg_rec3d_count.argtypes = [vp]
+    L.psg_rec3d_create_bous.argtypes = [C.POINTER(vp), i, d, i, i, i, i, i, d, i, d, d, d, d]
+    L.psg_rec3d_guess_rho.argtypes = [vp, dp]
     L.psg_rec2d_create.argtypes = [C.POINTER(vp), i, i, d, i, i, i, i, d, i, d, d, dp]
     L.psg_rec2d_destroy.argtypes = [vp]
     L.psg_rec2d_destroy.restype = None
@@ -376,13 +378,21 @@ class Batch2D:
 class Recurrence3D:
     """Near-recurrence search over a ring of stored 3D states (the DNS's UPO guess
     generator), residuals on the GPU.  States are torch CUDA complex128 tensors
-    of shape (3, IKTZ, IKTY, IKTX) in the reference layout."""
+    of shape (3, IKTZ, IKTY, IKTX) in the reference layout; with ri given, the
+    Boussinesq DNS's variant on four fields (xii, eta, zet, rho)."""
 
     def __init__(self, n, nout, dt, threshold, store_size=500, norm_width=8, nshift=(30, 2, 2),
-                 alpha=1.0, tstart=0.0, v2=0.0):
+                 alpha=1.0, tstart=0.0, v2=0.0, ri=None):
         h = C.c_void_p()
-        _check(lib().psg_rec3d_create(C.byref(h), n, alpha, store_size, norm_width, nshift[0],
-                                      nshift[1], nshift[2], threshold, nout, dt, tstart, v2))
+        if ri is None:
+            _check(lib().psg_rec3d_create(C.byref(h), n, alpha, store_size, norm_width, nshift[0],
+                                          nshift[1], nshift[2], threshold, nout, dt, tstart, v2))
+            self.nc = 3
+        else:
+            _check(lib().psg_rec3d_create_bous(C.byref(h), n, alpha, store_size, norm_width,
+                                               nshift[0], nshift[1], nshift[2], threshold, nout,
+                                               dt, tstart, v2, ri))
+            self.nc = 4
         self._h = h
         self.grid = Grid3D(n)
 
@@ -397,9 +407,10 @@ class Recurrence3D:
         except Exception:
             pass
 
-    @staticmethod
-    def _ptrs(t):
-        return (C.c_void_p * 3)(*[t[q].data_ptr() for q in range(3)])
+    def _ptrs(self, t):
+        if t.shape[0] != self.nc:
+            raise ValueError(f"expected {self.nc} fields")
+        return (C.c_void_p * self.nc)(*[t[q].data_ptr() for q in range(self.nc)])
 
     def start(self, state):
         _check(lib().psg_rec3d_start(self._h, self._ptrs(state.contiguous())))
@@ -415,6 +426,10 @@ class Recurrence3D:
         dp = C.POINTER(C.c_double)
         _check(lib().psg_rec3d_guess(self._h, meta.ctypes.data_as(dp),
                                      *[o.ctypes.data_as(dp) for o in out]))
+        if self.nc == 4:
+            rho = np.zeros(self.grid.shape, np.complex128)
+            _check(lib().psg_rec3d_guess_rho(self._h, rho.ctypes.data_as(dp)))
+            out.append(rho)
         keys = ("time", "v2", "period", "shift_x", "shift_y", "shift_z", "residual")
         return dict(zip(keys, meta.tolist())), tuple(out)
 

@@ -167,13 +167,15 @@ class TimestepLibrary:
 
     def bous3d_dns(self, xii, eta, zet, rho, n, nu, dt, tend, ri=0.0, sc=1.0, theta=0.0,
                    ampfor=0.0, kf=4, dtarget=0.0, adapt=0, stats=0, nout=1, noutv=10 ** 6,
-                   tstart=0.0, time0=0.0, alpha=1.0, workdir=None):
+                   tstart=0.0, time0=0.0, alpha=1.0, workdir=None, rec=0, resthresh=1.0):
         """3D Boussinesq RK4/CN as the DNS build steps it (3D_Boussinesq/src/
         cuda.cu:21-58): integrate while t <= tend, with the adaptive step
         (adapt = 1) and the forcing throttle (dtarget != 0) at output times
-        (every nout steps, stats != 0).  The reference build writes its
+        (every nout steps, stats != 0), and with rec = 1 the recurrence search
+        (guesses to JOB0/UPO_ZK.out).  The reference build writes its
         diagnostics under JOB0/ of the working directory, so the call runs in a
-        scratch directory holding JOB0/.  Returns (xii, eta, zet, rho, time)."""
+        scratch directory holding JOB0/ (or in `workdir`).  Returns
+        (xii, eta, zet, rho, time)."""
         g, kx, ky, kz, LC, ikF, ikN = self._grid3(n, alpha)
         xii, eta, zet, rho = (_cplx(a, g.shape) for a in (xii, eta, zet, rho))
         t = np.array([time0], dtype=np.float64)
@@ -181,10 +183,10 @@ class TimestepLibrary:
             self.fn(_pd(xii.view(np.float64)), _pd(eta.view(np.float64)),
                     _pd(zet.view(np.float64)), _pd(rho.view(np.float64)),
                     _pd(kx), _pd(ky), _pd(kz), _pd(t), _d(tstart), _d(tend), _d(ampfor),
-                    _d(dt), _d(1.0), _d(float(kf)), _d(nu), _d(ri), _d(sc), _d(theta),
+                    _d(dt), _d(resthresh), _d(float(kf)), _d(nu), _d(ri), _d(sc), _d(theta),
                     _d(alpha), _d(dtarget), _pi(ikF), _pi(ikN), _pi(LC), _i(g.iktx),
                     _i(g.ikty), _i(g.iktz), _i(g.kt), _i(g.nkt), _i(n), _i(n), _i(n),
-                    _i(nout), _i(noutv), _i(stats), _i(0), _i(adapt), _i(0))
+                    _i(nout), _i(noutv), _i(stats), _i(rec), _i(adapt), _i(0))
         return xii, eta, zet, rho, float(t[0])
 
     def bous3d_inplace(self, comps, n, nu, dt, tend, ri=0.0, sc=1.0, theta=0.0, ampfor=0.0,

@@ -19,10 +19,13 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "../../include/psgpu.h"
 #include "../../include/psgpu_ref_abi.h"
+#include "psgpu_internal.h"
 
 namespace {
 
@@ -51,7 +54,7 @@ void fill_nan(double2* const* comps, int ncomp, long nkt) {
   }
 }
 
-long box_nkt(int n) {
+[[maybe_unused]] long box_nkt(int n) {
   const long K = n / 3;
   return (K + 1) * (2 * K + 1) * (2 * K + 1);
 }
@@ -82,6 +85,27 @@ bool check_sizes(const char* who, int IKTX, int IKTY, int IKTZ, int KTZ, int NKT
   }
   return true;
 }
+
+#if defined(PSG_FLAVOUR_BOUS3D_DNS)
+// one guess of the recurrence search in the reference's records
+// (3D_Boussinesq/src/functions.h:592-609): UPO_ZK.out gets start time, v2,
+// period, shifts x, y, z, residual and the four fields; UPOinfo_ts.dat a line
+int write_guess(psg_rec3d* rec, FILE* zk, FILE* info, long nkt, int izkout) {
+  double meta[7];
+  std::vector<double> f(4 * 2 * (size_t)nkt);
+  double* p = f.data();
+  if (psg_rec3d_guess(rec, meta, p, p + 2 * nkt, p + 4 * nkt) ||
+      psg_rec3d_guess_rho(rec, p + 6 * nkt))
+    return 1;
+  fwrite(meta, sizeof(double), 7, zk);
+  fwrite(p, sizeof(double), f.size(), zk);
+  fflush(zk);
+  fprintf(info, "%d %e %e %e %e %e %e \n", izkout, meta[0], meta[2], meta[3], meta[4], meta[5],
+          meta[6]);
+  fflush(info);
+  return 0;
+}
+#endif
 
 }  // namespace
 
@@ -262,8 +286,18 @@ extern "C" void timederiv_cuda_(double2* xii, double2* eta, double2* zet, double
 //     -AMPFOR (init.h:18) while the device starts from AMPFOR (init.h:138), so
 //     from the first step on the forcing acts with the host's sign, as it
 //     does in the reference.
-// The DNS's diagnostic files (stats.dat, engy.dat, spectra, RiG, pdfs, raw
-// volumes) and its recurrence search (RecFLAG) are not written.
+//   * RecFLAG = 1: the recurrence search for UPO guesses at output times, the
+//     DNS's Boussinesq variant (4 fields, storeSize 500, normWidth 8, 64 x 1 x 1
+//     trial shifts: 3D_Boussinesq/src/kernels.h:12-16, functions.h:416-616),
+//     with the initial state stored first (init.h:268-296); guesses go to
+//     JOB<RANK>/UPO_ZK.out and JOB<RANK>/UPOinfo_ts.dat in the reference's
+//     record layout.  The periods are counted in the initial delt.  The
+//     reference's check also assigns the loop's time variable,
+//     tme = tstart + (NT - nOut) delt (functions.h:501), which sets the loop
+//     back NOUT steps at the first check and so runs NOUT more steps; the same
+//     assignment is made here.
+// The DNS's other diagnostic files (stats.dat, engy.dat, spectra, RiG, pdfs,
+// raw volumes) are not written.
 extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2* rho, double* kx,
                                double* ky, double* kz, double* Time, double* TSTART,
                                double* Tstep, double* AMPFOR, double* DELT, double* ResThresh,
@@ -272,8 +306,7 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
                                int* IKTX, int* IKTY, int* IKTZ, int* KTZ, int* NKT, int* NX,
                                int* NY, int* NZ, int* NOUT, int* NOUTV, int* statsFLAG,
                                int* RecFLAG, int* adaptFLAG, int* RANK) {
-  (void)kx; (void)ky; (void)kz; (void)ResThresh; (void)ikF; (void)ikN; (void)LC; (void)NOUTV;
-  (void)RANK;
+  (void)kx; (void)ky; (void)kz; (void)ikF; (void)ikN; (void)LC; (void)NOUTV;
   double2* state[4] = {xii, eta, zet, rho};
   if (!check_sizes("timestep_cuda_", *IKTX, *IKTY, *IKTZ, *KTZ, *NKT, *NX, *NY, *NZ, *alpha) ||
       *NOUT < 1) {
@@ -300,6 +333,34 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
     fail();
     return;
   }
+  psg_rec3d* rec = nullptr;
+  FILE* upozk = nullptr;
+  FILE* upoinfo = nullptr;
+  int izkout = 0, rec_outputs = 0;
+  auto close_rec = [&]() {
+    if (rec) psg_rec3d_destroy(rec);
+    if (upozk) fclose(upozk);
+    if (upoinfo) fclose(upoinfo);
+    rec = nullptr; upozk = upoinfo = nullptr;
+  };
+  if (*RecFLAG == 1) {
+    char fn[64];
+    snprintf(fn, sizeof fn, "JOB%1d/UPO_ZK.out", *RANK);
+    upozk = fopen(fn, "wb");
+    snprintf(fn, sizeof fn, "JOB%1d/UPOinfo_ts.dat", *RANK);
+    upoinfo = fopen(fn, "w");
+    if (upoinfo)
+      fprintf(upoinfo, "Guess No : Start time : guess Period : guess Shift x: guess Shift y: guess Residual \n");
+    if (!upozk || !upoinfo ||
+        psg_rec3d_create_bous(&rec, *NX, *alpha, 500, 8, 64, 1, 1, *ResThresh, *NOUT, delt, tme,
+                              *V2, ri) ||
+        psg_rec3d_start_engine(rec, h)) {
+      if (!upozk || !upoinfo) psg_set_error("cannot open JOB%d/UPO_ZK.out or UPOinfo_ts.dat", *RANK);
+      close_rec();
+      fail();
+      return;
+    }
+  }
   int timestep = 0;
   while (tme <= *Tstep) {
     ++timestep;
@@ -313,19 +374,32 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
     if (psg_ns3d_step(h, delt, 1, 0)) { fail(); return; }
     *Time = *Time + delt;
     tme += delt;
-    if (tcheck < 0.0 && (*RecFLAG == 1 || *statsFLAG != 0) && timestep != 0 &&
-        (*statsFLAG == 1 || (*statsFLAG == 2 && tme > 50.0))) {
-      double fl[2];
-      if (psg_ns3d_buoyancy_flux(h, fl)) { fail(); return; }
-      const double bflux = ri * fl[0];
-      const double input = -ampfor * fl[1] / kfy;
-      if (dtarget != 0.0) ampfor = ampfor * (dtarget - bflux) / input;
+    if (tcheck < 0.0 && (*RecFLAG == 1 || *statsFLAG != 0) && timestep != 0) {
+      if (rec) {
+        int emitted = 0;
+        const bool checks = rec_outputs++ > 0;  // the first output only stores
+        if (psg_rec3d_add_engine(rec, timestep, h, &emitted)) { close_rec(); fail(); return; }
+        if (emitted && write_guess(rec, upozk, upoinfo, *NKT, ++izkout)) {
+          close_rec();
+          fail();
+          return;
+        }
+        if (checks) tme = *TSTART + (timestep - *NOUT) * delt;
+      }
+      if (*statsFLAG == 1 || (*statsFLAG == 2 && tme > 50.0)) {
+        double fl[2];
+        if (psg_ns3d_buoyancy_flux(h, fl)) { close_rec(); fail(); return; }
+        const double bflux = ri * fl[0];
+        const double input = -ampfor * fl[1] / kfy;
+        if (dtarget != 0.0) ampfor = ampfor * (dtarget - bflux) / input;
+      }
     }
     if (*Dtarget != 0 && dev_ampfor != ampfor) {
       dev_ampfor = ampfor;
-      if (psg_ns3d_set_params(h, *V2, dev_ampfor, kfy, ri, *Sc, *Theta)) { fail(); return; }
+      if (psg_ns3d_set_params(h, *V2, dev_ampfor, kfy, ri, *Sc, *Theta)) { close_rec(); fail(); return; }
     }
   }
+  close_rec();
   if (psg_ns3d_download(h, out)) fail();
 }
 

@@ -10,6 +10,13 @@
 // selection logic (first turning point in the period, minimum over periods,
 // entering and leaving the threshold) runs on the host over those residuals,
 // in the reference's order.  The ring of full states stays on the device.
+//
+// The Boussinesq DNS's variant (3D_Boussinesq/src/functions.h:189-205,
+// 416-616, driven from out_high.h:5-40) carries the density as a fourth
+// field: its residual weights the density terms by Ri, normalises by the sum
+// of both states' norms, skips periods below 0.5, and takes the norm over
+// the whole box without the mask, with Ri on the real part of the density
+// only (computeNorm, functions.h:202, as written).
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -23,20 +30,25 @@ typedef struct psg_ns3d psg_ns3d;
 
 namespace psg {
 
-// the comparison box of the newest state (and its norm over the kept modes)
-__global__ void rec_gather(const double2* __restrict__ a, const double2* __restrict__ b,
-                           const double2* __restrict__ c, const int* __restrict__ inorm,
-                           const unsigned char* __restrict__ ll, int nnorm,
-                           double2* __restrict__ sub, double* __restrict__ norm) {
+// the comparison box of the newest state and its norm: the Navier-Stokes
+// form sums the three vorticity components over the kept modes
+// (3D_NavierStokes/src/functions.h:111-126); the Boussinesq form (nc = 4)
+// sums over the whole box with ri * Re(rho)^2 + Im(rho)^2 for the density
+// (3D_Boussinesq/src/functions.h:189-205)
+__global__ void rec_gather(const double2* __restrict__ full, long nkt, int nc, double ri,
+                           const int* __restrict__ inorm, const unsigned char* __restrict__ ll,
+                           int nnorm, double2* __restrict__ sub, double* __restrict__ norm) {
   __shared__ double r[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < nnorm; i += blockDim.x) {
     const int ik = inorm[i];
-    const double2 x = a[ik], y = b[ik], z = c[ik];
-    sub[i] = x;
-    sub[nnorm + i] = y;
-    sub[2 * nnorm + i] = z;
-    if (ll[ik]) s += x.x * x.x + x.y * x.y + y.x * y.x + y.y * y.y + z.x * z.x + z.y * z.y;
+    double v = 0.0;
+    for (int q = 0; q < nc; ++q) {
+      const double2 x = full[q * nkt + ik];
+      sub[q * nnorm + i] = x;
+      v += (q == 3) ? ri * x.x * x.x + x.y * x.y : x.x * x.x + x.y * x.y;
+    }
+    if (nc == 4 || ll[ik]) s += v;
   }
   r[threadIdx.x] = s;
   __syncthreads();
@@ -51,7 +63,7 @@ __global__ void rec_gather(const double2* __restrict__ a, const double2* __restr
 // (computeZdash, functions.h:212-249), shift s fastest in x, then z, then y
 __global__ void rec_dash(const double2* __restrict__ sub, const double* __restrict__ kxyz,
                          const double* __restrict__ shifts, int nsx, int nsy, int nsz, int nnorm,
-                         double2* __restrict__ dash) {
+                         int nc, double2* __restrict__ dash) {
   const int s = blockIdx.y;
   const int isx = s % nsx, isz = (s / nsx) % nsz, isy = s / (nsx * nsz);
   const double sx = shifts[isx], sy = shifts[nsx + isy], sz = shifts[nsx + nsy + isz];
@@ -59,26 +71,28 @@ __global__ void rec_dash(const double2* __restrict__ sub, const double* __restri
     const double sh = kxyz[i] * sx + kxyz[nnorm + i] * sy + kxyz[2 * nnorm + i] * sz;
     double sn, cs;
     sincos(sh, &sn, &cs);
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < nc; ++q) {
       const double2 z = sub[q * nnorm + i];
-      dash[((long)s * 3 + q) * nnorm + i] = make_double2(cs * z.x + sn * z.y, cs * z.y - sn * z.x);
+      dash[((long)s * nc + q) * nnorm + i] = make_double2(cs * z.x + sn * z.y, cs * z.y - sn * z.x);
     }
   }
 }
 
-// res2[c][s] = -2 <dash_s, old_c> + |dash_s|^2 + norm(old_c)
+// res2[c][s] = -2 <dash_s, old_c> + |dash_s|^2 + norm(old_c), the density
+// terms (fourth field) weighted by ri
 __global__ void rec_resid(const double2* __restrict__ dash, const double2* __restrict__ ring,
                           const int* __restrict__ cand, const double* __restrict__ norms,
-                          int nnorm, int nshift, double* __restrict__ res2) {
+                          int nnorm, int nshift, int nc, double ri, double* __restrict__ res2) {
   const int s = blockIdx.x, ci = blockIdx.y;
   const int slot = cand[ci];
-  const double2* d = dash + (long)s * 3 * nnorm;
-  const double2* o = ring + (long)slot * 3 * nnorm;
+  const double2* d = dash + (long)s * nc * nnorm;
+  const double2* o = ring + (long)slot * nc * nnorm;
   double cross = 0.0, nd = 0.0;
-  for (int i = threadIdx.x; i < 3 * nnorm; i += blockDim.x) {
+  for (int i = threadIdx.x; i < nc * nnorm; i += blockDim.x) {
     const double2 x = d[i], y = o[i];
-    cross += x.x * y.x + x.y * y.y;
-    nd += x.x * x.x + x.y * x.y;
+    const double w = (i >= 3 * nnorm) ? ri : 1.0;
+    cross += w * (x.x * y.x + x.y * y.y);
+    nd += w * (x.x * x.x + x.y * x.y);
   }
   __shared__ double r1[256], r2[256];
   r1[threadIdx.x] = cross;
@@ -96,14 +110,16 @@ __global__ void rec_resid(const double2* __restrict__ dash, const double2* __res
 
 struct Rec3D {
   int n = 0, K = 0, X = 0, Y = 0, store = 0, nw = 0, nnorm = 0, nsx = 0, nsy = 0, nsz = 0;
+  int nc = 3;       // 3: Navier-Stokes; 4: Boussinesq (density as the fourth field)
+  double ri = 0.0;  // Boussinesq weight of the density terms
   long nkt = 0;
   double alpha = 1.0, thresh = 0.0, delt = 0.0, tstart = 0.0, v2 = 0.0, freq2 = 0.0;
   int nout = 1;
   cudaStream_t stream = 0;
   // device
-  double2* ring_full = nullptr;  // [store][3][nkt]
-  double2* ring_sub = nullptr;   // [store][3][nnorm]
-  double2* dash = nullptr;       // [nshift][3][nnorm]
+  double2* ring_full = nullptr;  // [store][nc][nkt]
+  double2* ring_sub = nullptr;   // [store][nc][nnorm]
+  double2* dash = nullptr;       // [nshift][nc][nnorm]
   double* d_norms = nullptr;     // [store]
   double* d_kxyz = nullptr;      // [3][nnorm]
   double* d_shifts = nullptr;
@@ -132,7 +148,8 @@ struct Rec3D {
   }
 
   int init(int n_, double alpha_, int store_, int nw_, int nsx_, int nsy_, int nsz_, double th,
-           int nout_, double delt_, double tstart_, double v2_) {
+           int nout_, double delt_, double tstart_, double v2_, int nc_ = 3, double ri_ = 0.0) {
+    nc = nc_; ri = ri_;
     n = n_; K = n / 3; X = K + 1; Y = 2 * K + 1; nkt = (long)X * Y * Y;
     store = store_; nw = nw_; nsx = nsx_; nsy = nsy_; nsz = nsz_;
     alpha = alpha_; thresh = th; nout = nout_; delt = delt_; tstart = tstart_; v2 = v2_;
@@ -175,9 +192,9 @@ struct Rec3D {
     sh.insert(sh.end(), shiftz.begin(), shiftz.end());
     norms.assign(store, 0.0);
     const int nshift = nsx * nsy * nsz;
-    PSG_CUDA_TRY(cudaMalloc(&ring_full, sizeof(double2) * (size_t)store * 3 * nkt));
-    PSG_CUDA_TRY(cudaMalloc(&ring_sub, sizeof(double2) * (size_t)store * 3 * nnorm));
-    PSG_CUDA_TRY(cudaMalloc(&dash, sizeof(double2) * (size_t)nshift * 3 * nnorm));
+    PSG_CUDA_TRY(cudaMalloc(&ring_full, sizeof(double2) * (size_t)store * nc * nkt));
+    PSG_CUDA_TRY(cudaMalloc(&ring_sub, sizeof(double2) * (size_t)store * nc * nnorm));
+    PSG_CUDA_TRY(cudaMalloc(&dash, sizeof(double2) * (size_t)nshift * nc * nnorm));
     PSG_CUDA_TRY(cudaMalloc(&d_norms, sizeof(double) * store));
     PSG_CUDA_TRY(cudaMalloc(&d_kxyz, sizeof(double) * 3 * nnorm));
     PSG_CUDA_TRY(cudaMalloc(&d_shifts, sizeof(double) * sh.size()));
@@ -193,14 +210,14 @@ struct Rec3D {
     return PSG_OK;
   }
 
-  // copy a state (3 device FP64 boxes) into ring slot `slot` and its box
+  // copy a state (nc device FP64 boxes) into ring slot `slot` and its box
   int put(int slot, const void* const* st) {
-    for (int q = 0; q < 3; ++q)
-      PSG_CUDA_TRY(cudaMemcpyAsync(ring_full + ((size_t)slot * 3 + q) * nkt, st[q],
+    for (int q = 0; q < nc; ++q)
+      PSG_CUDA_TRY(cudaMemcpyAsync(ring_full + ((size_t)slot * nc + q) * nkt, st[q],
                                    sizeof(double2) * nkt, cudaMemcpyDeviceToDevice, stream));
-    const double2* base = ring_full + (size_t)slot * 3 * nkt;
-    rec_gather<<<1, 256, 0, stream>>>(base, base + nkt, base + 2 * nkt, d_inorm, d_ll, nnorm,
-                                      ring_sub + (size_t)slot * 3 * nnorm, d_norms + slot);
+    const double2* base = ring_full + (size_t)slot * nc * nkt;
+    rec_gather<<<1, 256, 0, stream>>>(base, nkt, nc, ri, d_inorm, d_ll, nnorm,
+                                      ring_sub + (size_t)slot * nc * nnorm, d_norms + slot);
     ++launches;
     PSG_CUDA_TRY(cudaGetLastError());
     PSG_CUDA_TRY(cudaMemcpyAsync(&norms[slot], d_norms + slot, sizeof(double),
@@ -224,6 +241,7 @@ struct Rec3D {
       const double period = ((nStore - icount) * nout) * delt;
       int slot = icount + iStart;
       slot -= (int)floor((double)slot / store) * store;
+      if (nc == 4 && period < 0.5) continue;  // 3D_Boussinesq/src/functions.h:513
       if (period > 20.0 && fabs(period - freq2 * floor(period / freq2 + 0.5)) > 0.0001) continue;
       cand.push_back(Cand{icount, slot, period});
     }
@@ -235,9 +253,9 @@ struct Rec3D {
       PSG_CUDA_TRY(cudaMemcpyAsync(d_cand, slots.data(), sizeof(int) * slots.size(),
                                    cudaMemcpyHostToDevice, stream));
       rec_dash<<<dim3((nnorm + 255) / 256, nshift), 256, 0, stream>>>(
-          ring_sub + (size_t)nCopy * 3 * nnorm, d_kxyz, d_shifts, nsx, nsy, nsz, nnorm, dash);
+          ring_sub + (size_t)nCopy * nc * nnorm, d_kxyz, d_shifts, nsx, nsy, nsz, nnorm, nc, dash);
       rec_resid<<<dim3(nshift, (unsigned)cand.size()), 256, 0, stream>>>(
-          dash, ring_sub, d_cand, d_norms, nnorm, nshift, d_res2);
+          dash, ring_sub, d_cand, d_norms, nnorm, nshift, nc, ri, d_res2);
       launches += 2;
       PSG_CUDA_TRY(cudaGetLastError());
       PSG_CUDA_TRY(cudaMemcpyAsync(res2.data(), d_res2, sizeof(double) * res2.size(),
@@ -255,7 +273,9 @@ struct Rec3D {
         for (int iz = 0; iz < nsz; ++iz)
           for (int ix = 0; ix < nsx; ++ix) {
             const int s = ix + nsx * (iz + nsz * iy);
-            const double r = sqrt(res2[ci * nshift + s] / norms[nCopy]);
+            // Boussinesq: normalised by both states' norms (functions.h:546)
+            const double den = nc == 4 ? norms[cand[ci].slot] + norms[nCopy] : norms[nCopy];
+            const double r = sqrt(res2[ci * nshift + s] / den);
             if (r < res) { res = r; sx = shiftx[ix]; sy = shifty[iy]; sz = shiftz[iz]; }
           }
       if (res > resPrev && minPflag == 1) minPeriod = cand[ci].period;
@@ -331,6 +351,21 @@ extern "C" int psg_rec3d_create(psg_rec3d** h, int n, double alpha, int store_si
   return PSG_OK;
 }
 
+// the Boussinesq DNS's variant: states of four fields (xii, eta, zet, rho)
+extern "C" int psg_rec3d_create_bous(psg_rec3d** h, int n, double alpha, int store_size,
+                                     int norm_width, int nshift_x, int nshift_y, int nshift_z,
+                                     double threshold, int nout, double dt, double tstart,
+                                     double v2, double ri) {
+  if (!h) { psg_set_error("null handle"); return PSG_ERR_ARG; }
+  *h = nullptr;
+  psg_rec3d* p = new psg_rec3d();
+  int rc = p->r.init(n, alpha, store_size, norm_width, nshift_x, nshift_y, nshift_z, threshold,
+                     nout, dt, tstart, v2, 4, ri);
+  if (rc) { delete p; return rc; }
+  *h = p;
+  return PSG_OK;
+}
+
 extern "C" void psg_rec3d_destroy(psg_rec3d* h) { delete h; }
 
 extern "C" int psg_rec3d_set_stream(psg_rec3d* h, void* s) {
@@ -356,10 +391,21 @@ extern "C" int psg_rec3d_guess(psg_rec3d* h, double* meta, double* xii, double* 
   double* out[3] = {xii, eta, zet};
   for (int q = 0; q < 3; ++q)
     if (out[q]) {
-      cudaError_t e = cudaMemcpy(out[q], h->r.ring_full + ((size_t)h->r.gslot * 3 + q) * h->r.nkt,
+      cudaError_t e = cudaMemcpy(out[q], h->r.ring_full + ((size_t)h->r.gslot * h->r.nc + q) * h->r.nkt,
                                  sizeof(double2) * h->r.nkt, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) { psg_set_error("guess copy: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
     }
+  return PSG_OK;
+}
+
+// the density of the last guess (Boussinesq variant)
+extern "C" int psg_rec3d_guess_rho(psg_rec3d* h, double* rho) {
+  if (!h || !rho) { psg_set_error("null argument"); return PSG_ERR_ARG; }
+  if (h->r.nc != 4) { psg_set_error("not the Boussinesq variant"); return PSG_ERR_STATE; }
+  if (!h->r.have_guess) { psg_set_error("no guess emitted yet"); return PSG_ERR_STATE; }
+  cudaError_t e = cudaMemcpy(rho, h->r.ring_full + ((size_t)h->r.gslot * 4 + 3) * h->r.nkt,
+                             sizeof(double2) * h->r.nkt, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { psg_set_error("guess copy: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
   return PSG_OK;
 }
 
@@ -368,8 +414,8 @@ extern "C" int psg_ns3d_download_device(psg_ns3d* h, void* const* comps);
 
 static int engine_state(psg_rec3d* h, psg_ns3d* eng, void** ptrs) {
   Rec3D& r = h->r;
-  if (!r.staging) PSG_CUDA_TRY(cudaMalloc(&r.staging, sizeof(double2) * 3 * r.nkt));
-  for (int q = 0; q < 3; ++q) ptrs[q] = r.staging + q * r.nkt;
+  if (!r.staging) PSG_CUDA_TRY(cudaMalloc(&r.staging, sizeof(double2) * 4 * r.nkt));
+  for (int q = 0; q < 4; ++q) ptrs[q] = r.staging + q * r.nkt;
   if (int rc = psg_ns3d_download_device(eng, ptrs)) return rc;
   PSG_CUDA_TRY(cudaDeviceSynchronize());
   return PSG_OK;
@@ -377,14 +423,14 @@ static int engine_state(psg_rec3d* h, psg_ns3d* eng, void** ptrs) {
 
 extern "C" int psg_rec3d_start_engine(psg_rec3d* h, psg_ns3d* eng) {
   if (!h || !eng) { psg_set_error("null argument"); return PSG_ERR_ARG; }
-  void* p[3];
+  void* p[4];
   if (int rc = engine_state(h, eng, p)) return rc;
   return h->r.start((const void* const*)p);
 }
 
 extern "C" int psg_rec3d_add_engine(psg_rec3d* h, int nt, psg_ns3d* eng, int* emitted) {
   if (!h || !eng || !emitted) { psg_set_error("null argument"); return PSG_ERR_ARG; }
-  void* p[3];
+  void* p[4];
   if (int rc = engine_state(h, eng, p)) return rc;
   return h->r.add(nt, (const void* const*)p, emitted);
 }

@@ -17,7 +17,11 @@ pytestmark = pytest.mark.gpu
 
 
 class RecRef:
-    def __init__(self, n, store, nw, ns, thresh, nout, delt, tstart, v2, alpha=1.0):
+    """ri None: the 3D NS DNS's check; ri given: the Boussinesq DNS's
+    (3D_Boussinesq/src/functions.h:189-205, 416-616) on four fields"""
+
+    def __init__(self, n, store, nw, ns, thresh, nout, delt, tstart, v2, alpha=1.0, ri=None):
+        self.ri = ri
         g = Grid3D(n)
         K = n // 3
         self.K, self.store, self.nw, self.ns = K, store, nw, ns
@@ -44,7 +48,12 @@ class RecRef:
     def put(self, slot, st):
         self.ring[slot] = [a.copy() for a in st]
         sub = np.stack([a[self.idx] for a in st])
-        self.norms[slot] = float(np.sum(np.abs(sub[:, self.ll]) ** 2))
+        if self.ri is None:
+            self.norms[slot] = float(np.sum(np.abs(sub[:, self.ll]) ** 2))
+        else:  # whole box; ri on the density's real part only, as written
+            r = sub[3]
+            self.norms[slot] = float(np.sum(np.abs(sub[:3]) ** 2)
+                                     + np.sum(self.ri * r.real ** 2 + r.imag ** 2))
 
     def check(self, nt):
         tme = self.tstart + (nt - self.nout) * self.delt
@@ -55,6 +64,8 @@ class RecRef:
         for icount in range(self.nStore - 1, 0, -1):
             period = ((self.nStore - icount) * self.nout) * self.delt
             slot = (icount + self.iStart) % self.store
+            if self.ri is not None and period < 0.5:
+                continue
             if period > 20.0 and abs(period - self.freq2 * math.floor(period / self.freq2 + 0.5)) > 1e-4:
                 continue
             old = np.stack([a[self.idx] for a in self.ring[slot]])
@@ -64,9 +75,14 @@ class RecRef:
                     for sx in self.sx:
                         ph = np.exp(-1j * (self.k[0] * sx + self.k[1] * sy + self.k[2] * sz))
                         d = newest * ph
-                        r2 = -2 * np.sum(d.real * old.real + d.imag * old.imag) + np.sum(np.abs(d) ** 2) \
+                        w = np.ones(len(d))
+                        if self.ri is not None:
+                            w[3] = self.ri
+                        cr = np.sum(d.real * old.real + d.imag * old.imag, axis=1)
+                        r2 = -2 * np.sum(w * cr) + np.sum(w * np.sum(np.abs(d) ** 2, axis=1)) \
                             + self.norms[slot]
-                        x = r2 / self.norms[self.nCopy]
+                        den = self.norms[self.nCopy] + (self.norms[slot] if self.ri is not None else 0.0)
+                        x = r2 / den
                         r = math.sqrt(x) if x >= 0 else math.nan  # as C's sqrt
                         if r < res:
                             res, bs = r, (sx, sy, sz)
@@ -105,12 +121,12 @@ class RecRef:
         return emitted
 
 
-def _sequence(n, count, period, nsx, seed=5):
+def _sequence(n, count, period, nsx, seed=5, nc=3):
     g = Grid3D(n)
     kx, _, _ = g.wavenumbers()
     rng = np.random.default_rng(seed)
     m = g.mask()
-    z0 = [(rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * m for _ in range(3)]
+    z0 = [(rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * m for _ in range(nc)]
     a = 2 * math.pi * 7 / (nsx * period)  # after one period: a grid translation of 7 steps
     out = []
     for t in range(count):
@@ -123,7 +139,7 @@ def _sequence(n, count, period, nsx, seed=5):
                         * np.exp(-1j * kx * a * t) for z in z0])
         else:
             out.append([(rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)) * m
-                        for _ in range(3)])
+                        for _ in range(nc)])
     return out
 
 
@@ -156,3 +172,30 @@ def test_recurrence_matches_restatement(store):
         # +7 grid steps in x, so the shift that maps it back is -7 = 23 (mod 30)
         assert emitted and emitted[0]["period"] == pytest.approx(0.8)
         assert emitted[0]["shift_x"] == pytest.approx(2 * math.pi * 23 / 30)
+
+
+def test_boussinesq_recurrence_matches_restatement():
+    """The Boussinesq DNS's variant on four fields (density weighted by Ri)."""
+    n, nw, ns, nout, dt, thr, ri = 16, 4, (30, 2, 2), 1, 0.1, 0.05, 0.7
+    seq = _sequence(n, 30, 8, ns[0], seed=9, nc=4)
+    gpu = P.Recurrence3D(n, nout, dt, thr, store_size=40, norm_width=nw, nshift=ns, v2=0.02, ri=ri)
+    ref = RecRef(n, 40, nw, ns, thr, nout, dt, 0.0, 0.02, ri=ri)
+    dev = lambda st: torch.from_numpy(np.stack(st)).cuda()
+    gpu.start(dev(seq[0]))
+    ref.put(0, seq[0])
+    n_emit = 0
+    for t in range(1, len(seq)):
+        e_gpu = gpu.add(t * nout, dev(seq[t]))
+        e_ref = ref.add(t * nout, seq[t])
+        assert e_gpu == e_ref, t
+        if e_gpu:
+            n_emit += 1
+            meta, st = gpu.guess()
+            tm, v2, per, sx, sy, sz, res, slot = ref.guess
+            assert meta["period"] == pytest.approx(per, abs=1e-12)
+            assert (meta["shift_x"], meta["shift_y"], meta["shift_z"]) == pytest.approx((sx, sy, sz))
+            assert meta["residual"] == pytest.approx(res, rel=1e-10, abs=1e-13)
+            assert len(st) == 4
+            for a, b in zip(st, ref.ring[slot]):
+                np.testing.assert_array_equal(a, b)
+    assert n_emit >= 1
