@@ -9,7 +9,10 @@
  * Crank-Nicolson steps with the DNS forcing, writes JOBDIR/stats.dat and
  * JOBDIR/engy.dat every NOUT steps as the reference's statistics do
  * (3D_NavierStokes/src/cuda.cu:116-140), with RCFLAG = 1 the recurrence
- * search's UPO_ZK.out / UPOinfo_ts.dat, and JOBDIR/Zk.out: main.F90's header
+ * search's UPO_ZK.out / UPOinfo_ts.dat, every NOUTV steps (NT = 0, NOUTV, ...,
+ * when NSTOP > 1) the physical vorticity of the state before step NT as raw
+ * FP64 volumes JOBDIR/xii%03d.raw, eta%03d.raw, zet%03d.raw, x fastest
+ * (3D_NavierStokes/src/cuda.cu:72-93), and JOBDIR/Zk.out: main.F90's header
  * record (1, IKTX, IKTY, IKTZ) followed by the final state as a type "D"
  * restart record.  The grid is compile-time in the reference
  * (global_params.F90, 128^3); here it is -n (default 128). */
@@ -106,11 +109,40 @@ int main(int argc, char** argv) {
   }
   const double t0 = now();
   int done = 0;
+  /* raw physical vorticity volumes before steps NT = 0, NOUTV, 2 NOUTV, ...:
+   * step through NT with the last predictor's physical fields kept */
+  const long nr = (long)n * n * n;
+  double* vol[3] = {NULL, NULL, NULL};
+  int nvol = 0;
+  const int want_vol = P.noutv > 0 && P.nstop > 1;
+  if (want_vol)
+    for (int q = 0; q < 3; ++q)
+      if (!(vol[q] = (double*)malloc(sizeof(double) * nr))) FAIL("out of host memory");
+  int next_vol = want_vol ? 0 : P.nstop;
   /* statistics after step NT for NT = NOUT, 2 NOUT, ... (NT counted from 0) */
   int izkout = 0;
-  for (int nt = P.nout; nt < P.nstop && (S || rec); nt += P.nout) {
-    if (psg_ns3d_step(h, P.delt, nt + 1 - done, 0)) FAIL("%s", psg_last_error());
-    done = nt + 1;
+  int nt = (S || rec) ? P.nout : P.nstop;
+  for (;;) {
+    /* the next event: a volume before step next_vol, or the statistics after step nt */
+    const int upto = next_vol < nt + 1 ? next_vol + 1 : nt + 1;
+    if (upto > P.nstop) break;
+    if (upto > done && psg_ns3d_step(h, P.delt, upto - done, upto == next_vol + 1))
+      FAIL("%s", psg_last_error());
+    done = upto;
+    if (done == next_vol + 1) {
+      static const char* names[3] = {"xii", "eta", "zet"};
+      if (psg_ns3d_download_phys(h, vol)) FAIL("%s", psg_last_error());
+      ++nvol;
+      for (int q = 0; q < 3; ++q) {
+        snprintf(path, sizeof path, "%s/%s%03d.raw", dir, names[q], nvol);
+        FILE* fv = fopen(path, "wb");
+        if (!fv || fwrite(vol[q], sizeof(double), nr, fv) != (size_t)nr) FAIL("cannot write %s", path);
+        fclose(fv);
+      }
+      next_vol += P.noutv;
+      continue;
+    }
+    if (!(S || rec) || nt >= P.nstop) break;
     const double tme = done * P.delt;
     if (rec) {
       int emitted = 0;
@@ -127,9 +159,11 @@ int main(int argc, char** argv) {
         fflush(fi);
       }
     }
-    if (!S || (P.statsflag == 2 && tme <= 500.0)) continue;
-    if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
-    psg_stats3d_add(S, tme, st[0], st[1], st[2], fs, fe);
+    if (S && !(P.statsflag == 2 && tme <= 500.0)) {
+      if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
+      psg_stats3d_add(S, tme, st[0], st[1], st[2], fs, fe);
+    }
+    nt += P.nout;
   }
   if (done < P.nstop && psg_ns3d_step(h, P.delt, P.nstop - done, 0)) FAIL("%s", psg_last_error());
   if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
@@ -149,6 +183,7 @@ int main(int argc, char** argv) {
   psg_rec3d_destroy(rec);
   psg_stats3d_destroy(S);
   psg_ns3d_destroy(h);
+  for (int q = 0; q < 3; ++q) free(vol[q]);
   printf("time stepping done: %d steps in %.3f s (%.1f steps/s)\n", P.nstop, el,
          el > 0 ? P.nstop / el : 0.0);
   for (int q = 0; q < 3; ++q) free(st[q]);
