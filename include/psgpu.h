@@ -266,11 +266,21 @@ int psg_upo2d_get(psg_upo2d* h, int i, double* Z, double* vals, int* info);
 /* building blocks at guess i (unshifted): mode 1 Phi_T(z) -> Zout; mode 0 also
  * the tangent dPhi_T(z) q (q in/out); mode 2 dz/dt -> Zout */
 int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, double* q);
-/* per-Newton-step record k of guess i, rec[10] = {Newton index, GMRES
+/* per-Newton-step record k of guess i, rec[11] = {Newton index, GMRES
  * iterations of the step, hookstep trials, Delta after the step, mu of the
- * last trial, T, shift x, residual |F|/|Phi_T(z)|, |F|, time step}; the
+ * last trial, T, shift x, residual |F|/|Phi_T(z)|, |F|, time step, nu}; the
  * quantities the reference prints per step (src_gmres/main.F90:1225-1760) */
 int psg_upo2d_trace(psg_upo2d* h, int i, int k, double* rec);
+/* Arc-length continuation of guess i in the viscosity (src_gmres/main.F90:
+ * 408-640, 799-1823 with arclcFLAG): nu becomes an unknown with the
+ * pseudo-arclength row <dZ/dr, z - Zr2> + dT/dr (T - Tr2) + dS/dr (s - Sr2)
+ * + dnu/dr (nu - nu_r2) = ndelta; dZrdr and Zr2 are complex128 boxes.  Call
+ * after psg_upo2d_set_guess (the predicted z, T, s, nu), which clears it;
+ * psg_upo2d_get_nu returns the current nu of a guess. */
+int psg_upo2d_set_arc(psg_upo2d* h, int i, const double* dZrdr, const double* Zr2, double dTrdr,
+                      double dSrdr, double dv2rdr, double Tr2, double Sr2, double v2r2,
+                      double ndelta);
+int psg_upo2d_get_nu(psg_upo2d* h, int i, double* nu);
 int psg_upo2d_trace_count(psg_upo2d* h, int i);
 long psg_upo2d_integrations(psg_upo2d* h);
 long psg_upo2d_launches(psg_upo2d* h);

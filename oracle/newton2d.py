@@ -21,7 +21,14 @@ guess at a time, as the reference does:
   integration, NaN handling and the trust-region halve / double / revert
   logic (main.F90:1264-1623); dt halving after a blow-up (main.F90:1636-1665);
 * the update, stall detection, convergence, PERIOD TOO SMALL and NEWTON
-  FAILED statuses (main.F90:1667-1823).
+  FAILED statuses (main.F90:1667-1823);
+* with `arc` (arclcFLAG2, the pseudo-arclength corrector of continuation in
+  nu): the initial Narc (main.F90:633-640), |b| with Narc (806-812), the
+  extra unknown nu and row vN3 in GMRES (1049-1061, 1121-1155), DIFFv2 and
+  the trial's v2plus, Narcplus and |b{N+1}| against |b| (1350-1530,
+  1538), v2plus in the save / revert (1550-1614), the update and the new
+  Narc (1678, 1720-1727).  TIMEDERIV reads the one NU array the reference
+  keeps, which the last hookstep trial set (v2plus), also after a revert.
 
 The SVD is LAPACK's DGESDD through scipy.linalg.svd(lapack_driver='gesdd'),
 the routine the reference calls (main.F90:1164).  The period map, the time
@@ -74,6 +81,7 @@ class NewtonStep:
     sx: float
     ner: float
     normfn: float
+    nu: Optional[float] = None
 
 
 @dataclass
@@ -89,13 +97,17 @@ class Result:
     hook: int
     steps: list = field(default_factory=list)
     integrations: int = 0
+    nu: Optional[float] = None
 
 
 class Newton2D:
     """phi(Z, T, dt) -> Phi_T(Z) taking NSTOP = INT(T/dt) steps of T/NSTOP;
     rhs(Z) -> dZ/dt (TIMEDERIV: N(Z) + forcing - nu k^2 Z on the kept modes);
     tangent(Z, q, T, dt) -> dPhi_T(Z) q, or None for the reference's forward
-    difference."""
+    difference.  With solve(..., arc=...) each is called with a further
+    keyword nu= (the viscosity of that integration).  The exact-tangent form
+    of the corrector takes dPhi_T/dnu by the central difference
+    (Phi(nu (1 + 1e-5)) - Phi(nu (1 - 1e-5))) / (2e-5 nu)."""
 
     def __init__(self, n: int, phi: Callable, rhs: Callable, tangent: Optional[Callable] = None,
                  gmresmax: int = 60, netol: float = 1e-12, gmtol: float = 1e-3,
@@ -121,13 +133,33 @@ class Newton2D:
         src = np.conj(Z[::-1, :]) if rsym else Z
         return self._mask(np.exp(-1j * self.kx * sx) * np.exp(-1j * self.ky * sy) * src)
 
-    def _step(self, Z, T, truedelt):
+    def _step(self, Z, T, truedelt, nu=None):
         self.integrations += 1
-        return self._mask(np.asarray(self.phi(self._mask(Z), T, truedelt), np.complex128))
+        kw = {} if nu is None else {"nu": nu}
+        return self._mask(np.asarray(self.phi(self._mask(Z), T, truedelt, **kw), np.complex128))
+
+    def _rhs(self, Z, nu=None):
+        kw = {} if nu is None else {"nu": nu}
+        return self._mask(np.asarray(self.rhs(Z, **kw), np.complex128))
 
     # ------------------------------------------------------------------ solve
-    def solve(self, Z, T, sx=0.0, sy=0.0, rsym=0, dt=0.005, max_newton=None) -> Result:
+    def solve(self, Z, T, sx=0.0, sy=0.0, rsym=0, dt=0.005, max_newton=None, nu=None,
+              arc=None) -> Result:
+        """arc: None, or the corrector of a continuation step, a dict with dZrdr,
+        Zr2, dTrdr, dSrdr, dv2rdr, Tr2, Sr2, v2r2, ndelta (then nu, the predicted
+        viscosity, is an unknown too)."""
         LL = self.LL
+        if arc is not None and nu is None:
+            raise ValueError("an arc-length corrector needs the predicted nu")
+        v2n = nu_rhs = nu
+        if arc is not None:
+            dzrdr = self._mask(np.asarray(arc["dZrdr"], np.complex128))
+            zr2 = self._mask(np.asarray(arc["Zr2"], np.complex128))
+
+            def narc_of(z, t, s, v):
+                return (self._dot(dzrdr, z - zr2) + arc["dSrdr"] * (s - arc["Sr2"])
+                        + arc["dv2rdr"] * (v - arc["v2r2"]) - arc["ndelta"]
+                        + arc["dTrdr"] * (t - arc["Tr2"]))
         newtonmax = self.newtonmax if max_newton is None else max_newton
         truedelt0 = truedelt = dt
         delta = self.delta0
@@ -136,13 +168,14 @@ class Newton2D:
             T = round(T / truedelt) * truedelt
         znewt = self._mask(np.asarray(Z, np.complex128))
         tnewt, snewtx, snewty = float(T), float(sx), float(sy)
-        znn = self._step(znewt, tnewt, truedelt)
+        znn = self._step(znewt, tnewt, truedelt, v2n)
         znshift = self._shift(znn, snewtx, snewty, rsym)
         normz = math.sqrt(float(np.sum(np.abs(znn) ** 2)))
         fn = self._mask(znshift - znewt)
         normfn = math.sqrt(self._dot(fn, fn))
         ner = normfn / normz
-        res = Result("NEWTON FAILED", tnewt, snewtx, snewty, ner, znewt, 0, 0, 0)
+        narc = narc_of(znewt, tnewt, snewtx, v2n) if arc is not None else 0.0
+        res = Result("NEWTON FAILED", tnewt, snewtx, snewty, ner, znewt, 0, 0, 0, nu=v2n)
         if ner <= self.netol:
             res.status = "CONVERGED"
             res.integrations = self.integrations
@@ -152,49 +185,66 @@ class Newton2D:
         kmax = self.gmresmax
         ine = 0
         for ine in range(1, newtonmax + 1):
-            normb = normfn
+            normb = math.sqrt(normfn * normfn + narc * narc) if arc is not None else normfn
             q = [None] * (kmax + 1)
             qn1 = np.zeros(kmax + 1)
             qn2 = np.zeros(kmax + 1)
+            qn3 = np.zeros(kmax + 1)
             q[0] = self._mask(-fn / normb)
-            dzndt = self._mask(self.rhs(znshift))
-            dzdt = self._mask(self.rhs(znewt))
+            qn3[0] = -narc / normb
+            dphidnu = None
+            if arc is not None and self.tangent is not None:
+                zp = self._step(znewt, tnewt, truedelt, v2n * (1.0 + 1e-5))
+                zm = self._step(znewt, tnewt, truedelt, v2n * (1.0 - 1e-5))
+                dphidnu = self._shift((zp - zm) * (0.5e5 / v2n), snewtx, snewty, rsym)
+            dzndt = self._rhs(znshift, nu_rhs)
+            dzdt = self._rhs(znewt, nu_rhs)
             dznds = self._mask(-1j * self.kx * znshift)
             dzds = self._mask(-1j * self.kx * znewt)
             H = np.zeros((kmax + 1, kmax))
 
-            def jv(vec, vn_t, vn_s):
-                """J (vec, dT, dS) rows 1..N (main.F90:1100-1116 / 1362-1404)"""
+            def jv(vec, vn_t, vn_s, vn_v=0.0):
+                """J (vec, dT, dS, dnu) rows 1..N (main.F90:1047-1116 / 1360-1404)"""
                 if self.tangent is None:
                     zo = self._mask(znewt + self.eps * vec)
-                    zn = self._step(zo, tnewt, truedelt)
+                    nu_j = v2n + self.eps * vn_v if arc is not None else v2n
+                    zn = self._step(zo, tnewt, truedelt, nu_j)
                     d = (zn - znn) / self.eps
                 else:
                     self.integrations += 1
+                    kw = {} if v2n is None else {"nu": v2n}
                     d = self._mask(np.asarray(self.tangent(znewt, self._mask(vec), tnewt,
-                                                           truedelt), np.complex128))
-                return self._mask(self._shift(d, snewtx, snewty, rsym) - vec
-                                  + dznds * vn_s + dzndt * vn_t)
+                                                           truedelt, **kw), np.complex128))
+                out = self._shift(d, snewtx, snewty, rsym) - vec + dznds * vn_s + dzndt * vn_t
+                if dphidnu is not None:
+                    out = out + dphidnu * vn_v
+                return self._mask(out)
 
             # ------------------------------------------------------------ GMRES
             igm_done = 0
             gmr = float("inf")
             P = S = VH = None
             for igm in range(1, kmax + 1):
-                v = jv(q[igm - 1], qn1[igm - 1], qn2[igm - 1])
+                v = jv(q[igm - 1], qn1[igm - 1], qn2[igm - 1], qn3[igm - 1])
                 vn1 = self._dot(dzdt, q[igm - 1])
                 vn2 = self._dot(dzds, q[igm - 1])
+                vn3 = 0.0
+                if arc is not None:
+                    vn3 = (self._dot(dzrdr, q[igm - 1]) + arc["dTrdr"] * qn1[igm - 1]
+                           + arc["dSrdr"] * qn2[igm - 1] + arc["dv2rdr"] * qn3[igm - 1])
                 for j in range(igm):
-                    h = self._dot(q[j], v) + qn1[j] * vn1 + qn2[j] * vn2
+                    h = self._dot(q[j], v) + qn1[j] * vn1 + qn2[j] * vn2 + qn3[j] * vn3
                     H[j, igm - 1] = h
                     v = self._mask(v - h * q[j])
                     vn1 -= h * qn1[j]
                     vn2 -= h * qn2[j]
-                hn = math.sqrt(self._dot(v, v) + vn1 * vn1 + vn2 * vn2)
+                    vn3 -= h * qn3[j]
+                hn = math.sqrt(self._dot(v, v) + vn1 * vn1 + vn2 * vn2 + vn3 * vn3)
                 H[igm, igm - 1] = hn
                 q[igm] = self._mask(v / hn)
                 qn1[igm] = vn1 / hn
                 qn2[igm] = vn2 / hn
+                qn3[igm] = vn3 / hn
                 Hm = H[:igm + 1, :igm]
                 U, S, VH = sla.svd(Hm, full_matrices=True, lapack_driver="gesdd")
                 P = normb * U[0, :]
@@ -217,10 +267,10 @@ class Newton2D:
             halve = dbl = False
             trials = []
             zplus2 = zn2 = fnplus2 = None
-            tplus2 = splus2 = nfplus2 = 0.0
+            tplus2 = splus2 = nfplus2 = v2plus2 = 0.0
             nfpred = nfplus = float("nan")
             zplus = zn = fnplus = None
-            tplus = splus = 0.0
+            tplus = splus = v2plus = 0.0
             while True:
                 ihook += 1
                 if ihook > self.ihookmax:
@@ -250,25 +300,38 @@ class Newton2D:
                 diffz = self._mask(sum(q[j] * yh[j] for j in range(igm)))
                 difft = float(np.dot(qn1[:igm], yh))
                 diffs = float(np.dot(qn2[:igm], yh))
-                jfdiff = jv(diffz, difft, diffs)
+                diffv = float(np.dot(qn3[:igm], yh))
+                jfdiff = jv(diffz, difft, diffs, diffv)
                 fnpred = self._mask(fn + jfdiff)
                 nfpred = math.sqrt(self._dot(fnpred, fnpred))
                 nbpredc = math.sqrt(self._dot(fn, fn))  # |FN + const*J DIFF|, const = 0
+                if arc is not None:
+                    nbpredc = math.sqrt(nbpredc * nbpredc + narc * narc)
                 zplus = self._mask(znewt + diffz)
                 tplus = tnewt + difft
                 splus = snewtx + diffs
-                zn = self._step(zplus, tplus, truedelt)
+                if arc is not None:
+                    v2plus = v2n + diffv
+                    nu_rhs = v2plus
+                else:
+                    v2plus = v2n
+                zn = self._step(zplus, tplus, truedelt, v2plus)
                 fnplus = self._mask(self._shift(zn, splus, snewty, rsym) - zplus)
                 nfplus = math.sqrt(self._dot(fnplus, fnplus))
+                nbplus = nfplus
+                if arc is not None:
+                    narcplus = narc_of(zplus, tplus, splus, v2plus)
+                    nbplus = math.sqrt(nfplus * nfplus + narcplus * narcplus)
                 if nfplus != nfplus or nfpred != nfpred:
                     delta /= 2.0
                     halve = True
                     trials.append(Trial(delta_now, mumid, normx, nfpred, nfplus, "nan"))
                     continue
-                if nfplus >= nbpredc:
+                if nbplus >= nbpredc:
                     if dbl:
                         zplus, tplus, splus, zn, fnplus, nfplus = (zplus2, tplus2, splus2, zn2,
                                                                    fnplus2, nfplus2)
+                        v2plus = v2plus2
                         delta /= 2.0
                         trials.append(Trial(delta_now, mumid, normx, nfpred, nfplus, "revert"))
                         break
@@ -282,6 +345,7 @@ class Newton2D:
                     if dbl and nfplus > nfplus2:
                         zplus, tplus, splus, zn, fnplus, nfplus = (zplus2, tplus2, splus2, zn2,
                                                                    fnplus2, nfplus2)
+                        v2plus = v2plus2
                         delta /= 2.0
                         trials.append(Trial(delta_now, mumid, normx, nfpred, nfplus, "revert"))
                         break
@@ -294,6 +358,7 @@ class Newton2D:
                         dbl = True
                         zplus2, tplus2, splus2, zn2, fnplus2, nfplus2 = (zplus, tplus, splus, zn,
                                                                          fnplus, nfplus)
+                        v2plus2 = v2plus
                         trials.append(Trial(delta_now, mumid, normx, nfpred, nfplus, "double"))
                     else:
                         trials.append(Trial(delta_now, mumid, normx, nfpred, nfplus, "accept"))
@@ -307,24 +372,28 @@ class Newton2D:
                 truedelt /= 2.0
                 znshift = self._shift(znn, snewtx, snewty, rsym)
                 res.steps.append(NewtonStep(ine, igm, gmr, ihook, trials, delta, tnewt, snewtx,
-                                            ner, normfn))
+                                            ner, normfn, v2n))
                 continue
             if ihook > self.ihookmax:
                 res.status = "H-STEP FAILED"
                 res.steps.append(NewtonStep(ine, igm, gmr, ihook, trials, delta, tnewt, snewtx,
-                                            ner, normfn))
+                                            ner, normfn, v2n))
                 break
             # ----------------------------------------------------------- update
             znn = zn
             znewt = zplus
             tnewt, snewtx = tplus, splus
+            if arc is not None:
+                v2n = v2plus
             znshift = self._shift(znn, snewtx, snewty, rsym)
             normz = math.sqrt(self._dot(znn, znn))
             fn = fnplus
             normfn = nfplus
+            if arc is not None:
+                narc = narc_of(znewt, tnewt, snewtx, v2n)
             ner = normfn / normz
             res.steps.append(NewtonStep(ine, igm, gmr, ihook, trials, delta, tnewt, snewtx, ner,
-                                        normfn))
+                                        normfn, v2n))
             rel = abs((ner - nerold) / ner)
             stalled = False
             if rel < 0.001:
@@ -342,7 +411,7 @@ class Newton2D:
             if tnewt < 0.1:
                 res.status = "PERIOD TOO SMALL"
                 break
-        res.T, res.sx, res.sy, res.ner, res.Z = tnewt, snewtx, snewty, ner, znewt
+        res.T, res.sx, res.sy, res.ner, res.Z, res.nu = tnewt, snewtx, snewty, ner, znewt, v2n
         res.newton = ine
         res.gmres, res.hook = gmrescount, hookcount
         res.integrations = self.integrations

@@ -134,6 +134,8 @@ def _declare_2d(L):
     L.psg_upo2d_trace_count.argtypes = [vp, i]
     L.psg_upo2d_launches.argtypes = [vp]
     L.psg_upo2d_launches.restype = C.c_long
+    L.psg_upo2d_set_arc.argtypes = [vp, i, dp, dp] + [C.c_double] * 7
+    L.psg_upo2d_get_nu.argtypes = [vp, i, dp]
 
 
 def _check(rc):
@@ -553,6 +555,23 @@ class UPO2D:
                 "status": UPO_STATUS[int(info[0])], "newton": int(info[1]),
                 "gmres": int(info[2]), "hookstep": int(info[3])}
 
+    def set_arc(self, i, dZrdr, Zr2, dTrdr, dSrdr, dv2rdr, Tr2, Sr2, v2r2, ndelta):
+        """Make guess i a pseudo-arclength corrector: nu becomes one more
+        unknown and <dZrdr, z - Zr2> + dTrdr (T - Tr2) + dSrdr (sx - Sr2)
+        + dv2rdr (nu - v2r2) = ndelta one more equation (call after set_guess)."""
+        dz = np.ascontiguousarray(dZrdr, np.complex128).reshape(-1)
+        z2 = np.ascontiguousarray(Zr2, np.complex128).reshape(-1)
+        if dz.size != self.grid.nkt or z2.size != self.grid.nkt:
+            raise ValueError("arc fields must have the grid's size")
+        _check(lib().psg_upo2d_set_arc(self._h, i, dz.ctypes.data_as(C.POINTER(C.c_double)),
+                                       z2.ctypes.data_as(C.POINTER(C.c_double)), dTrdr, dSrdr,
+                                       dv2rdr, Tr2, Sr2, v2r2, ndelta))
+
+    def nu(self, i):
+        v = C.c_double()
+        _check(lib().psg_upo2d_get_nu(self._h, i, C.byref(v)))
+        return v.value
+
     def apply(self, i, mode, q=None):
         Z = np.zeros(self.grid.shape, np.complex128)
         qq = None
@@ -565,14 +584,15 @@ class UPO2D:
     def trace(self, i):
         """Per-Newton-step records of guess i: dicts with the Newton index, GMRES
         iterations and hookstep trials of the step, Delta after it, mu of its last
-        trial, T, shift, residual |F|/|Phi_T(z)|, |F| and the time step in use."""
+        trial, T, shift, residual |F|/|Phi_T(z)|, |F|, the time step in use and
+        nu (which arc-length continuation moves)."""
         out = []
-        rec = np.zeros(10)
+        rec = np.zeros(11)
         for k in range(int(lib().psg_upo2d_trace_count(self._h, i))):
             _check(lib().psg_upo2d_trace(self._h, i, k, rec.ctypes.data_as(C.POINTER(C.c_double))))
             out.append({"newton": int(rec[0]), "gmres": int(rec[1]), "hook": int(rec[2]),
                         "delta": rec[3], "mu": rec[4], "T": rec[5], "sx": rec[6],
-                        "ner": rec[7], "normfn": rec[8], "dt": rec[9]})
+                        "ner": rec[7], "normfn": rec[8], "dt": rec[9], "nu": rec[10]})
         return out
 
     @property

@@ -138,21 +138,22 @@ __global__ void __launch_bounds__(256) vec_dot(const DotJob* jobs, int K, int X,
   if (threadIdx.x == 0) *J.out = s;
 }
 
-// Modified Gram-Schmidt of the augmented vector (v, vN1, vN2) against
-// (q_j, qN1_j, qN2_j), j < m, then H[m+1,m] and q_{m+1}
-// (src_gmres/main.F90:1130-1155).  One block per guess, FP64.
+// Modified Gram-Schmidt of the augmented vector (v, vN1, vN2, vN3) against
+// (q_j, qN1_j, qN2_j, qN3_j), j < m, then H[m+1,m] and q_{m+1}
+// (src_gmres/main.F90:1130-1155; the third row is arc-length continuation's,
+// zero otherwise).  One block per guess, FP64.
 struct MgsJob {
   C2* v;
   C2* const* q;     // device array of m+1 basis pointers (q[m] receives the new vector)
-  const double* qn; // host-mirrored extra rows: qN1[j], qN2[j] (2*(m+1))
-  double vn1, vn2;  // extra rows of v
+  const double* qn; // host-mirrored extra rows: qN1[j], qN2[j], qN3[j] (3*(m+1))
+  double vn1, vn2, vn3;  // extra rows of v
   int m;            // number of basis vectors to orthogonalise against
-  double* H;        // out: H[0..m] of column m (m+1 entries) + vN1, vN2 of q_{m+1}
+  double* H;        // out: H[0..m] of column m (m+1 entries) + vN1, vN2, vN3 of q_{m+1}
 };
 __global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int X, int nkt) {
   __shared__ double red[32];
   const MgsJob J = jobs[blockIdx.x];
-  double vn1 = J.vn1, vn2 = J.vn2;
+  double vn1 = J.vn1, vn2 = J.vn2, vn3 = J.vn3;
   for (int j = 0; j < J.m; ++j) {
     const C2* qj = J.q[j];
     double s = 0.0;
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int
         const C2 a = qj[ik], b = J.v[ik];
         s += a.x * b.x + a.y * b.y;
       }
-    double h = block_sum(s, red) + J.qn[2 * j] * vn1 + J.qn[2 * j + 1] * vn2;
+    double h = block_sum(s, red) + J.qn[3 * j] * vn1 + J.qn[3 * j + 1] * vn2 + J.qn[3 * j + 2] * vn3;
     for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
       if (keep_ik(ik, K, X)) {
         const C2 a = qj[ik];
@@ -170,8 +171,9 @@ __global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int
         b.y -= h * a.y;
         J.v[ik] = b;
       }
-    vn1 -= h * J.qn[2 * j];
-    vn2 -= h * J.qn[2 * j + 1];
+    vn1 -= h * J.qn[3 * j];
+    vn2 -= h * J.qn[3 * j + 1];
+    vn3 -= h * J.qn[3 * j + 2];
     if (threadIdx.x == 0) J.H[j] = h;
     __syncthreads();
   }
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int
       const C2 b = J.v[ik];
       s += b.x * b.x + b.y * b.y;
     }
-  const double hn = sqrt(block_sum(s, red) + vn1 * vn1 + vn2 * vn2);
+  const double hn = sqrt(block_sum(s, red) + vn1 * vn1 + vn2 * vn2 + vn3 * vn3);
   C2* qn = J.q[J.m];
   for (int ik = threadIdx.x; ik < nkt; ik += blockDim.x)
     qn[ik] = keep_ik(ik, K, X) ? C2{J.v[ik].x / hn, J.v[ik].y / hn} : czero<double>();
@@ -189,6 +191,7 @@ __global__ void __launch_bounds__(256) mgs_kernel(const MgsJob* jobs, int K, int
     J.H[J.m] = hn;
     J.H[J.m + 1] = vn1 / hn;
     J.H[J.m + 2] = vn2 / hn;
+    J.H[J.m + 3] = vn3 / hn;
   }
 }
 
@@ -256,18 +259,29 @@ struct Guess {
   // device vectors (nkt complex each)
   C2 *z, *zn, *znshift, *fn, *dzdt, *dzndt, *dzds, *dznds, *v, *diff, *jdiff, *zplus, *zplus2,
       *zn_trial, *zn2, *fnplus, *fnplus2, *scratch;
+  // arc-length continuation: the branch tangent dZ/dr, the last converged state
+  // Zr2 and shift(dPhi_T/dnu) (exact Jv), device vectors
+  C2 *dzrdr, *zr2, *dphidnu;
+  bool arc = false;
+  double dTrdr = 0, dSrdr = 0, dv2rdr = 0, Tr2 = 0, Sr2 = 0, v2r2 = 0, ndelta = 0;
+  double c0 = 0;     // <dZ/dr, Zr2>
+  double narc = 0, narcplus = 0, narcplus2 = 0, v2plus = 0, v2plus2 = 0, dV = 0;
   std::vector<C2*> q;  // Krylov basis
   InstTan2D<double> inst;  // integration buffers
   InstTan2D<float> inst32;  // FP32 integration buffers (exact Jv in FP32)
   // host state
   double T = 0, sx = 0, sy = 0, nu = 0, dt0 = 0, dt_true = 0;
+  // viscosity TIMEDERIV sees: the reference keeps one NU array, set last by
+  // the previous hookstep trial (v2plus), not reset when the trial is
+  // reverted (src_gmres/main.F90:1458-1470, 816-821)
+  double nu_rhs = 0;
   int rsym = 0;
   double delta = 0.1;
   double normfn = 0, normz = 1, ner = 0, ner_old = 0;
   int ner_count = 0;
   int status = UPO_ACTIVE;
   int newton = 0, gmres = 0, hook = 0;
-  std::vector<double> qn;  // qN1, qN2 per basis vector
+  std::vector<double> qn;  // qN1, qN2, qN3 per basis vector
   std::vector<double> H;   // (kmax+1) x kmax column-major
   int m = 0;               // GMRES iterations done in this Newton step
   bool gmres_done = false;
@@ -281,8 +295,8 @@ struct Guess {
   int ihook = 0;
   // one record per Newton step: newton index, GMRES iterations, hookstep
   // trials, Delta after the step, mu of the last trial, T, shift, residual,
-  // |F|, time step in use
-  std::vector<std::array<double, 10>> trace;
+  // |F|, time step in use, viscosity
+  std::vector<std::array<double, 11>> trace;
 };
 
 struct Upo2D {
@@ -340,7 +354,7 @@ struct Upo2D {
     }
     if (kmax < 1 || kmax > 500 || ng < 1) { psg_set_error("bad UPO sizes"); return PSG_ERR_ARG; }
     K = n / 3; X = K + 1; Y = 2 * K + 1; nkt = X * Y;
-    const long nvec = 18 + (kmax + 1) + 10;
+    const long nvec = 21 + (kmax + 1) + 10;
     const long work = 6L * n * X;
     const long per = nvec * nkt + work;
     const long twl = 2L * n;
@@ -352,7 +366,7 @@ struct Upo2D {
       Guess& U_ = G[g];
       C2** v[] = {&U_.z, &U_.zn, &U_.znshift, &U_.fn, &U_.dzdt, &U_.dzndt, &U_.dzds, &U_.dznds,
                   &U_.v, &U_.diff, &U_.jdiff, &U_.zplus, &U_.zplus2, &U_.zn_trial, &U_.zn2,
-                  &U_.fnplus, &U_.fnplus2, &U_.scratch};
+                  &U_.fnplus, &U_.fnplus2, &U_.scratch, &U_.dzrdr, &U_.zr2, &U_.dphidnu};
       for (auto pp : v) { *pp = p; p += nkt; }
       U_.q.resize(kmax + 1);
       for (int j = 0; j <= kmax; ++j) { U_.q[j] = p; p += nkt; }
@@ -361,7 +375,7 @@ struct Upo2D {
       I.Z = p; p += nkt; I.Z0 = p; p += nkt; I.Z1 = p; p += nkt; I.Z2 = p; p += nkt; I.Z3 = p; p += nkt;
       I.D = p; p += nkt; I.D0 = p; p += nkt; I.D1 = p; p += nkt; I.D2 = p; p += nkt; I.D3 = p; p += nkt;
       I.work = p; p += work;
-      U_.qn.assign(2 * (kmax + 1), 0.0);
+      U_.qn.assign(3 * (kmax + 1), 0.0);
       U_.H.assign((size_t)(kmax + 1) * kmax, 0.0);
     }
     if (int rc = plan64.init(n, ng, pool + per * ng)) return rc;
@@ -386,8 +400,8 @@ struct Upo2D {
     PSG_CUDA_TRY(cudaMalloc(&d_mgs, sizeof(MgsJob) * ng));
     PSG_CUDA_TRY(cudaMalloc(&d_scalars, sizeof(double) * ng * 4));
     PSG_CUDA_TRY(cudaMalloc(&d_qptr, sizeof(C2*) * ng * (kmax + 1)));
-    PSG_CUDA_TRY(cudaMalloc(&d_qn, sizeof(double) * ng * 2 * (kmax + 1)));
-    PSG_CUDA_TRY(cudaMalloc(&d_H, sizeof(double) * ng * (kmax + 3)));
+    PSG_CUDA_TRY(cudaMalloc(&d_qn, sizeof(double) * ng * 3 * (kmax + 1)));
+    PSG_CUDA_TRY(cudaMalloc(&d_H, sizeof(double) * ng * (kmax + 4)));
     PSG_CUDA_TRY(cudaMalloc(&d_next, sizeof(int)));
     std::vector<C2*> qp((size_t)ng * (kmax + 1));
     for (int g = 0; g < ng; ++g)
@@ -406,6 +420,7 @@ struct Upo2D {
     const C2* d_in;
     double T;
     int mode;
+    double nu = -1.0;  // viscosity of this integration (< 0: the guess's)
   };
   int integrate(const std::vector<IntReq>& reqs) {
     if (reqs.empty()) return PSG_OK;
@@ -439,7 +454,7 @@ struct Upo2D {
       Guess& U_ = G[r.g];
       InstTan2D<T> I = inst_of(U_, (T*)nullptr);
       I.mode = r.mode;
-      I.nu = (T)U_.nu;
+      I.nu = (T)(r.nu >= 0.0 ? r.nu : U_.nu);
       if (r.mode == 2) {
         I.nsteps = 0;
         I.dt = 0;
@@ -601,9 +616,13 @@ struct Upo2D {
   }
 
   // J q for every guess in `who` (q from the pointer list), written to `out`:
-  // shift(dPhi_T(z) q) - q + dZN/dS q_s + dZN/dt q_T (src_gmres/main.F90:1100-1116)
+  // shift(dPhi_T(z) q) - q + dZN/dS q_s + dZN/dt q_T (src_gmres/main.F90:1100-1116),
+  // and with arc-length continuation + shift(dPhi_T/dnu) q_v: the forward
+  // difference perturbs the viscosity with the state (main.F90:1050-1063), the
+  // exact form adds the derivative formed once per Newton step
   int apply_j(const std::vector<int>& who, const std::vector<const C2*>& q,
-              const std::vector<double>& qs, const std::vector<double>& qt, C2* Guess::*out) {
+              const std::vector<double>& qs, const std::vector<double>& qt,
+              const std::vector<double>& qv, C2* Guess::*out) {
     std::vector<IntReq> reqs;
     std::vector<VecJob> jobs;
     if (jv_mode != 1) {
@@ -619,7 +638,11 @@ struct Upo2D {
       // forward difference with eps = 1e-7 (src_gmres/main.F90:1048-1108)
       for (size_t i = 0; i < who.size(); ++i) jobs.push_back(lc(G[who[i]].scratch, G[who[i]].z, 1.0, q[i], eps));
       if (int rc = lincomb(jobs)) return rc;
-      for (int g : who) reqs.push_back(IntReq{g, G[g].scratch, nullptr, G[g].T, 1});
+      for (size_t i = 0; i < who.size(); ++i) {
+        const Guess& U_ = G[who[i]];
+        reqs.push_back(IntReq{who[i], U_.scratch, nullptr, U_.T, 1,
+                              U_.arc ? U_.nu + eps * qv[i] : -1.0});
+      }
       if (int rc = integrate(reqs)) return rc;
       jobs.clear();
       for (int g : who) jobs.push_back(lc(G[g].scratch, G[g].inst.Z, 1.0 / eps, G[g].zn, -1.0 / eps));
@@ -635,8 +658,12 @@ struct Upo2D {
       jobs.push_back(lc(G[who[i]].*out, G[who[i]].*out, 1.0, q[i], -1.0, G[who[i]].dznds, qs[i]));
     if (int rc = lincomb(jobs)) return rc;
     jobs.clear();
-    for (size_t i = 0; i < who.size(); ++i)
-      jobs.push_back(lc(G[who[i]].*out, G[who[i]].*out, 1.0, G[who[i]].dzndt, qt[i]));
+    for (size_t i = 0; i < who.size(); ++i) {
+      const Guess& U_ = G[who[i]];
+      const bool dnu = U_.arc && jv_mode != 1;
+      jobs.push_back(lc(U_.*out, U_.*out, 1.0, U_.dzndt, qt[i], dnu ? U_.dphidnu : nullptr,
+                        dnu ? qv[i] : 0.0));
+    }
     return lincomb(jobs);
   }
 
@@ -723,22 +750,49 @@ struct Upo2D {
       for (int g : act) {
         Guess& U_ = G[g];
         U_.newton += 1;
-        U_.normb = U_.normfn;
+        // |b| with the arc-length residual as one more row (main.F90:802-815)
+        U_.normb = U_.arc ? sqrt(U_.normfn * U_.normfn + U_.narc * U_.narc) : U_.normfn;
         U_.m = 0;
         U_.gmres_done = false;
         std::fill(U_.H.begin(), U_.H.end(), 0.0);
         std::fill(U_.qn.begin(), U_.qn.end(), 0.0);
+        if (U_.arc) U_.qn[2] = -U_.narc / U_.normb;
         jobs.push_back(lc(U_.q[0], U_.fn, -1.0 / U_.normb));
       }
       if (int rc = lincomb(jobs)) return rc;
+      // exact Jv with continuation: shift(dPhi_T/dnu) by a central difference in
+      // nu (step 1e-5 nu: truncation and round-off both near 1e-10 relative)
+      if (jv_mode != 1) {
+        std::vector<int> an;
+        for (int g : act)
+          if (G[g].arc) an.push_back(g);
+        if (!an.empty()) {
+          std::vector<IntReq> reqs;
+          for (int g : an) reqs.push_back(IntReq{g, G[g].z, nullptr, G[g].T, 1, G[g].nu * (1.0 + 1e-5)});
+          if (int rc = integrate(reqs)) return rc;
+          if (int rc = copy_out(an, &Guess::dphidnu, false)) return rc;
+          reqs.clear();
+          for (int g : an) reqs.push_back(IntReq{g, G[g].z, nullptr, G[g].T, 1, G[g].nu * (1.0 - 1e-5)});
+          if (int rc = integrate(reqs)) return rc;
+          std::vector<VecJob> dj;
+          for (int g : an)
+            dj.push_back(lc(G[g].scratch, G[g].dphidnu, 0.5e5 / G[g].nu, G[g].inst.Z, -0.5e5 / G[g].nu));
+          if (int rc = lincomb(dj)) return rc;
+          std::vector<const C2*> src;
+          std::vector<C2*> dst;
+          std::vector<double> sx;
+          for (int g : an) { src.push_back(G[g].scratch); dst.push_back(G[g].dphidnu); sx.push_back(G[g].sx); }
+          if (int rc = shift_ptr(an, src, dst, sx)) return rc;
+        }
+      }
       // dZN/dt and dz/dt (TIMEDERIV), dZN/dS and dz/dS
       {
         std::vector<IntReq> reqs;
-        for (int g : act) reqs.push_back(IntReq{g, G[g].znshift, nullptr, 0.0, 2});
+        for (int g : act) reqs.push_back(IntReq{g, G[g].znshift, nullptr, 0.0, 2, G[g].nu_rhs});
         if (int rc = integrate(reqs)) return rc;
         if (int rc = copy_out(act, &Guess::dzndt, true)) return rc;
         reqs.clear();
-        for (int g : act) reqs.push_back(IntReq{g, G[g].z, nullptr, 0.0, 2});
+        for (int g : act) reqs.push_back(IntReq{g, G[g].z, nullptr, 0.0, 2, G[g].nu_rhs});
         if (int rc = integrate(reqs)) return rc;
         if (int rc = copy_out(act, &Guess::dzdt, true)) return rc;
         std::vector<VecJob> dj;
@@ -755,11 +809,20 @@ struct Upo2D {
           if (!G[g].gmres_done) ga.push_back(g);
         if (ga.empty()) break;
         std::vector<const C2*> q;
-        std::vector<double> qs, qt;
-        for (int g : ga) { q.push_back(G[g].q[k]); qt.push_back(G[g].qn[2 * k]); qs.push_back(G[g].qn[2 * k + 1]); }
-        if (int rc = apply_j(ga, q, qs, qt, &Guess::v)) return rc;
+        std::vector<double> qs, qt, qv;
+        for (int g : ga) {
+          q.push_back(G[g].q[k]);
+          qt.push_back(G[g].qn[3 * k]);
+          qs.push_back(G[g].qn[3 * k + 1]);
+          qv.push_back(G[g].qn[3 * k + 2]);
+        }
+        if (int rc = apply_j(ga, q, qs, qt, qv, &Guess::v)) return rc;
         std::vector<std::pair<const C2*, const C2*>> ab;
-        for (int g : ga) { ab.push_back({G[g].dzdt, G[g].q[k]}); ab.push_back({G[g].dzds, G[g].q[k]}); }
+        for (int g : ga) {
+          ab.push_back({G[g].dzdt, G[g].q[k]});
+          ab.push_back({G[g].dzds, G[g].q[k]});
+          ab.push_back({G[g].dzrdr, G[g].q[k]});
+        }
         std::vector<double> vn;
         if (int rc = dots(ab, vn)) return rc;
         std::vector<MgsJob> mj;
@@ -769,11 +832,16 @@ struct Upo2D {
           MgsJob J{};
           J.v = G[g].v;
           J.q = d_qptr + (size_t)g * (kmax + 1);
-          J.qn = d_qn + (size_t)i * 2 * (kmax + 1);
-          J.vn1 = vn[2 * i];
-          J.vn2 = vn[2 * i + 1];
+          J.qn = d_qn + (size_t)i * 3 * (kmax + 1);
+          J.vn1 = vn[3 * i];
+          J.vn2 = vn[3 * i + 1];
+          // the arc-length row (main.F90:1123-1126)
+          const Guess& U_ = G[g];
+          J.vn3 = U_.arc ? vn[3 * i + 2] + U_.dTrdr * U_.qn[3 * k] + U_.dSrdr * U_.qn[3 * k + 1] +
+                               U_.dv2rdr * U_.qn[3 * k + 2]
+                         : 0.0;
           J.m = k + 1;
-          J.H = d_H + (size_t)i * (kmax + 3);
+          J.H = d_H + (size_t)i * (kmax + 4);
           mj.push_back(J);
           qnh.insert(qnh.end(), G[g].qn.begin(), G[g].qn.end());
         }
@@ -782,17 +850,18 @@ struct Upo2D {
         // MgsJob.q points at the basis pointer array: q[0..k] existing, q[k+1] new
         mgs_kernel<<<(unsigned)mj.size(), 256, 0, stream>>>(d_mgs, K, X, nkt);
         ++launches;
-        std::vector<double> hh(ga.size() * (kmax + 3));
+        std::vector<double> hh(ga.size() * (kmax + 4));
         PSG_CUDA_TRY(cudaMemcpyAsync(hh.data(), d_H, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, stream));
         PSG_CUDA_TRY(cudaStreamSynchronize(stream));
         PSG_CUDA_TRY(cudaGetLastError());
         for (size_t i = 0; i < ga.size(); ++i) {
           Guess& U_ = G[ga[i]];
-          const double* h = hh.data() + i * (kmax + 3);
+          const double* h = hh.data() + i * (kmax + 4);
           const int rows = kmax + 1;
           for (int j = 0; j <= k + 1; ++j) U_.H[(size_t)k * rows + j] = h[j];
-          U_.qn[2 * (k + 1)] = h[k + 2];
-          U_.qn[2 * (k + 1) + 1] = h[k + 3];
+          U_.qn[3 * (k + 1)] = h[k + 2];
+          U_.qn[3 * (k + 1) + 1] = h[k + 3];
+          U_.qn[3 * (k + 1) + 2] = h[k + 4];
           // SVD of H(1:k+2, 1:k+1) and the GMRES residual (src_gmres/main.F90:1161-1228)
           const int r = k + 2, c = k + 1;
           std::vector<double> A((size_t)r * c);
@@ -829,7 +898,7 @@ struct Upo2D {
             if (gmr > gmtol) {
               U_.status = UPO_GMRES_FAILED;
               U_.trace.push_back({(double)U_.newton, (double)(k + 1), 0.0, U_.delta, 0.0, U_.T,
-                                  U_.sx, U_.ner, U_.normfn, U_.dt_true});
+                                  U_.sx, U_.ner, U_.normfn, U_.dt_true, U_.nu});
             }
           }
         }
@@ -861,8 +930,12 @@ struct Upo2D {
           Guess& U_ = G[live[i]];
           std::vector<double> y;
           hook_step(U_, U_.m, y);
-          U_.dT = 0; U_.dS = 0;
-          for (int j = 0; j < U_.m; ++j) { U_.dT += U_.qn[2 * j] * y[j]; U_.dS += U_.qn[2 * j + 1] * y[j]; }
+          U_.dT = 0; U_.dS = 0; U_.dV = 0;
+          for (int j = 0; j < U_.m; ++j) {
+            U_.dT += U_.qn[3 * j] * y[j];
+            U_.dS += U_.qn[3 * j + 1] * y[j];
+            U_.dV += U_.qn[3 * j + 2] * y[j];
+          }
           // diff = sum_j y_j q_j, accumulated three basis vectors per launch
           for (int j = 0; j < U_.m; ++j) coef[i * (kmax + 1) + j] = y[j];
         }
@@ -881,9 +954,14 @@ struct Upo2D {
         }
         // J DIFF and the predicted residual
         std::vector<const C2*> dq;
-        std::vector<double> qs, qt;
-        for (int g : live) { dq.push_back(G[g].diff); qs.push_back(G[g].dS); qt.push_back(G[g].dT); }
-        if (int rc = apply_j(live, dq, qs, qt, &Guess::jdiff)) return rc;
+        std::vector<double> qs, qt, qv;
+        for (int g : live) {
+          dq.push_back(G[g].diff);
+          qs.push_back(G[g].dS);
+          qt.push_back(G[g].dT);
+          qv.push_back(G[g].dV);
+        }
+        if (int rc = apply_j(live, dq, qs, qt, qv, &Guess::jdiff)) return rc;
         jobs2.clear();
         for (int g : live) jobs2.push_back(lc(G[g].scratch, G[g].fn, 1.0, G[g].jdiff, 1.0));
         if (int rc = lincomb(jobs2)) return rc;
@@ -895,7 +973,9 @@ struct Upo2D {
         for (int g : live) {
           G[g].Tplus = G[g].T + G[g].dT;
           G[g].Splus = G[g].sx + G[g].dS;
-          reqs.push_back(IntReq{g, G[g].zplus, nullptr, G[g].Tplus, 1});
+          G[g].v2plus = G[g].nu + (G[g].arc ? G[g].dV : 0.0);
+          G[g].nu_rhs = G[g].v2plus;
+          reqs.push_back(IntReq{g, G[g].zplus, nullptr, G[g].Tplus, 1, G[g].v2plus});
         }
         if (int rc = integrate(reqs)) return rc;
         if (int rc = copy_out(live, &Guess::zn_trial, false)) return rc;
@@ -910,32 +990,47 @@ struct Upo2D {
         for (int g : live) jobs2.push_back(lc(G[g].fnplus, G[g].fnplus, 1.0, G[g].zplus, -1.0));
         if (int rc = lincomb(jobs2)) return rc;
         std::vector<std::pair<const C2*, const C2*>> ab;
-        for (int g : live) { ab.push_back({G[g].scratch, G[g].scratch}); ab.push_back({G[g].fnplus, G[g].fnplus}); }
+        for (int g : live) {
+          ab.push_back({G[g].scratch, G[g].scratch});
+          ab.push_back({G[g].fnplus, G[g].fnplus});
+          ab.push_back({G[g].dzrdr, G[g].zplus});
+        }
         std::vector<double> d;
         if (int rc = dots(ab, d)) return rc;
         // accept / retry logic (src_gmres/main.F90:1523-1622)
         for (size_t i = 0; i < live.size(); ++i) {
           Guess& U_ = G[live[i]];
-          U_.nfpred = sqrt(d[2 * i]);
-          U_.nfplus = sqrt(d[2 * i + 1]);
-          const double normb_pred = U_.normfn;  // |FN + 0*J DIFF|
+          U_.nfpred = sqrt(d[3 * i]);
+          U_.nfplus = sqrt(d[3 * i + 1]);
+          // |b| of the trial and of the prediction with const = 0, with the
+          // arc-length residual when continuing (main.F90:1420-1480)
+          double normb_pred = U_.normfn, normb_plus = U_.nfplus;
+          if (U_.arc) {
+            U_.narcplus = d[3 * i + 2] - U_.c0 + U_.dSrdr * (U_.Splus - U_.Sr2) +
+                          U_.dv2rdr * (U_.v2plus - U_.v2r2) - U_.ndelta +
+                          U_.dTrdr * (U_.Tplus - U_.Tr2);
+            normb_pred = sqrt(U_.normfn * U_.normfn + U_.narc * U_.narc);
+            normb_plus = sqrt(U_.nfplus * U_.nfplus + U_.narcplus * U_.narcplus);
+          }
           auto save = [&]() {
             cudaMemcpyAsync(U_.zplus2, U_.zplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             cudaMemcpyAsync(U_.zn2, U_.zn_trial, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             cudaMemcpyAsync(U_.fnplus2, U_.fnplus, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             U_.Tplus2 = U_.Tplus; U_.Splus2 = U_.Splus; U_.nfplus2 = U_.nfplus;
+            U_.v2plus2 = U_.v2plus; U_.narcplus2 = U_.narcplus;
           };
           auto revert = [&]() {
             cudaMemcpyAsync(U_.zplus, U_.zplus2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             cudaMemcpyAsync(U_.zn_trial, U_.zn2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             cudaMemcpyAsync(U_.fnplus, U_.fnplus2, sizeof(C2) * nkt, cudaMemcpyDeviceToDevice, stream);
             U_.Tplus = U_.Tplus2; U_.Splus = U_.Splus2; U_.nfplus = U_.nfplus2;
+            U_.v2plus = U_.v2plus2; U_.narcplus = U_.narcplus2;
           };
           if (U_.nfplus != U_.nfplus || U_.nfpred != U_.nfpred) {
             U_.delta *= 0.5; U_.halve = true;
             continue;
           }
-          if (U_.nfplus >= normb_pred) {
+          if (normb_plus >= normb_pred) {
             if (U_.dbl) { revert(); U_.delta *= 0.5; U_.hook_done = true; continue; }
             U_.delta *= 0.5; U_.halve = true;
           } else {
@@ -962,7 +1057,7 @@ struct Upo2D {
           // a trial integration blew up: halve the time step and redo the
           // Newton step from the same z, T, s (src_gmres/main.F90:1636-1665)
           U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
-                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true});
+                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true, U_.nu});
           if (U_.dt_true < 0.1 * U_.dt0) {
             U_.status = UPO_TSTEP_FAILED;
           } else {
@@ -974,7 +1069,7 @@ struct Upo2D {
         }
         if (U_.status != UPO_ACTIVE) {
           U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
-                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true});
+                              U_.T, U_.sx, U_.ner, U_.normfn, U_.dt_true, U_.nu});
           continue;
         }
         up.push_back(g);
@@ -984,6 +1079,10 @@ struct Upo2D {
         U_.T = U_.Tplus;
         U_.sx = U_.Splus;
         U_.normfn = U_.nfplus;
+        if (U_.arc) {
+          U_.nu = U_.v2plus;
+          U_.narc = U_.narcplus;
+        }
       }
       // the shifted final state of a redone step is rebuilt from the old Phi_T(z)
       if (int rc = shift(redo, &Guess::znshift, (const C2* Guess::*)&Guess::zn, &Guess::sx)) return rc;
@@ -997,7 +1096,7 @@ struct Upo2D {
         U_.normz = sqrt(d[i]);
         const double ner = U_.normfn / U_.normz;
         U_.trace.push_back({(double)U_.newton, (double)U_.m, (double)U_.ihook, U_.delta, U_.mu,
-                            U_.T, U_.sx, ner, U_.normfn, U_.dt_true});
+                            U_.T, U_.sx, ner, U_.normfn, U_.dt_true, U_.nu});
         if (ner != ner) { U_.status = UPO_TSTEP_FAILED; continue; }
         // stall detection before the convergence test, as the reference
         // orders them (src_gmres/main.F90:1752-1804)
@@ -1073,13 +1172,14 @@ extern "C" int psg_upo2d_set_guess(psg_upo2d* h, int i, const double* Z, double 
     z[ik] = keep ? C2{Z[2 * ik], Z[2 * ik + 1]} : C2{0.0, 0.0};
   }
   PSG_CUDA_TRY(cudaMemcpy(g.z, z.data(), sizeof(C2) * U.nkt, cudaMemcpyHostToDevice));
-  g.T = T; g.sx = sx; g.sy = sy; g.rsym = rsym; g.nu = nu; g.dt0 = dt; g.dt_true = dt;
+  g.T = T; g.sx = sx; g.sy = sy; g.rsym = rsym; g.nu = nu; g.nu_rhs = nu; g.dt0 = dt; g.dt_true = dt;
   // a guess period from a run with this time step is taken as exact
   // (src_gmres/main.F90:688-695)
   if (fabs(T - nearbyint(T / dt) * dt) < 1e-10) g.T = nearbyint(T / dt) * dt;
   g.delta = 0.1; g.status = UPO_ACTIVE; g.newton = g.gmres = g.hook = 0;
   g.ner_old = 0; g.ner_count = 0;
   g.trace.clear();
+  g.arc = false;
   return PSG_OK;
 }
 
@@ -1120,7 +1220,48 @@ extern "C" int psg_upo2d_apply(psg_upo2d* h, int i, int mode, double* Zout, doub
   return PSG_OK;
 }
 
-// the per-Newton-step record k of guess i (rec[10]; see Guess::trace)
+// Arc-length continuation of guess i (src_gmres/main.F90:408-640): the
+// viscosity becomes an unknown, with the pseudo-arclength row
+// <dZ/dr, z - Zr2> + dT/dr (T - Tr2) + dS/dr (s - Sr2) + dv2/dr (nu - v2r2) = ndelta
+// (dZrdr, Zr2: complex128 boxes, reference layout).  Call after
+// psg_upo2d_set_guess, which puts the prediction in place and clears this.
+extern "C" int psg_upo2d_set_arc(psg_upo2d* h, int i, const double* dZrdr, const double* Zr2,
+                                 double dTrdr, double dSrdr, double dv2rdr, double Tr2,
+                                 double Sr2, double v2r2, double ndelta) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  if (i < 0 || i >= U.ng || !dZrdr || !Zr2) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  Guess& g = U.G[i];
+  std::vector<C2> a((size_t)U.nkt), b((size_t)U.nkt);
+  const int K = U.K, X = U.X;
+  for (int ik = 0; ik < U.nkt; ++ik) {
+    const int ikx = ik % X, ky = ik / X - K;
+    const bool keep = !(ikx == 0 && ky <= 0) && 4 * (ikx * ikx + ky * ky) <= (2 * K - 1) * (2 * K - 1);
+    a[ik] = keep ? C2{dZrdr[2 * ik], dZrdr[2 * ik + 1]} : C2{0.0, 0.0};
+    b[ik] = keep ? C2{Zr2[2 * ik], Zr2[2 * ik + 1]} : C2{0.0, 0.0};
+  }
+  PSG_CUDA_TRY(cudaMemcpy(g.dzrdr, a.data(), sizeof(C2) * U.nkt, cudaMemcpyHostToDevice));
+  PSG_CUDA_TRY(cudaMemcpy(g.zr2, b.data(), sizeof(C2) * U.nkt, cudaMemcpyHostToDevice));
+  std::vector<double> d;
+  if (int rc = U.dots({{g.dzrdr, g.zr2}, {g.dzrdr, g.z}}, d)) return rc;
+  g.dTrdr = dTrdr; g.dSrdr = dSrdr; g.dv2rdr = dv2rdr;
+  g.Tr2 = Tr2; g.Sr2 = Sr2; g.v2r2 = v2r2; g.ndelta = ndelta;
+  g.c0 = d[0];
+  // the initial arc-length residual (main.F90:633-640)
+  g.narc = d[1] - g.c0 + dSrdr * (g.sx - Sr2) + dv2rdr * (g.nu - v2r2) - ndelta + dTrdr * (g.T - Tr2);
+  g.arc = true;
+  return PSG_OK;
+}
+
+// the current viscosity of guess i (the continuation parameter)
+extern "C" int psg_upo2d_get_nu(psg_upo2d* h, int i, double* nu) {
+  PSG_U2(h);
+  if (i < 0 || i >= h->u->ng || !nu) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  *nu = h->u->G[i].nu;
+  return PSG_OK;
+}
+
+// the per-Newton-step record k of guess i (rec[11]; see Guess::trace)
 extern "C" int psg_upo2d_trace(psg_upo2d* h, int i, int k, double* rec) {
   PSG_U2(h);
   Upo2D& U = *h->u;
@@ -1130,7 +1271,7 @@ extern "C" int psg_upo2d_trace(psg_upo2d* h, int i, int k, double* rec) {
     psg_set_error("guess %d has %d trace records", i, (int)g.trace.size());
     return PSG_ERR_ARG;
   }
-  for (int j = 0; j < 10; ++j) rec[j] = g.trace[k][j];
+  for (int j = 0; j < 11; ++j) rec[j] = g.trace[k][j];
   return PSG_OK;
 }
 
