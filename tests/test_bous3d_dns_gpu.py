@@ -13,7 +13,10 @@ zeta at (0, kf, 0), output every NOUT = 5 steps with statsFLAG = 1:
 * RecFLAG = 1: the recurrence search writes the same guesses to
   JOB0/UPO_ZK.out as the reference's build (3D_Boussinesq/src/
   functions.h:592-609) at a threshold the run crosses, and the run ends at
-  the same state and time.
+  the same state and time.  The flow there recurs: small internal gravity
+  waves with horizontal wavevectors (|k| <= 1.5, kz = 0, gravity along z)
+  at Ri = 100 oscillate at the buoyancy frequency N = 10 (period 0.63 > the
+  check's 0.5 minimum) around a steady vortical part, unforced.
 TSTART = 1 keeps the reference from writing raw volumes at t = 0
 (out_low.h:79-80 fires when t < dt).
 """
@@ -92,14 +95,19 @@ def test_recurrence_guesses_match_reference(monkeypatch, tmp_path):
     P.lib()
     ours_lib = TimestepLibrary(P.dropin_path("bous3d_dns"), "bous3d_dns")
     ref_lib = TimestepLibrary(REF, "bous3d_dns")
-    nkt = P.Grid3D(N).nkt
-    xi, et, zt, rho = _state()
-    kw = dict(ri=1.0, sc=1.0, theta=np.pi / 2, ampfor=-0.5 * KF, kf=KF, stats=1, nout=2,
+    g = P.Grid3D(N)
+    nkt = g.nkt
+    hz = g.wavenumbers()[2] == 0
+    xi, et, zt = (0.05 * a * hz for a in random_vorticity3d(N, 21, kmin=0.5, kmax=1.5,
+                                                             solenoidal=True))
+    rho = 0.05 * random_vorticity3d(N, 22, kmin=0.5, kmax=1.5)[0] * hz
+    kw = dict(ri=100.0, sc=1.0, theta=np.pi / 2, ampfor=0.0, kf=KF, stats=1, nout=2,
               tstart=1.0, time0=1.0, rec=1)
+    tend = 1.0 + 200 * DT
     found = None
     for thr in (0.8, 0.5, 0.3, 0.2, 0.12, 0.08, 0.05, 0.03):
         wd = tmp_path / f"ours_{thr}"
-        out = ours_lib.bous3d_dns(xi, et, zt, rho, N, NU, DT, 1.0 + 80 * DT, resthresh=thr,
+        out = ours_lib.bous3d_dns(xi, et, zt, rho, N, NU, DT, tend, resthresh=thr,
                                   workdir=str(wd), **kw)
         r = _records(wd / "JOB0" / "UPO_ZK.out", nkt)
         lines = (wd / "JOB0" / "UPOinfo_ts.dat").read_text().splitlines()
@@ -111,7 +119,7 @@ def test_recurrence_guesses_match_reference(monkeypatch, tmp_path):
     thr, ours, out = found
     assert (ours[:, 6] < thr).all() and (ours[:, 2] >= 0.5 - 1e-12).all()
     wd = tmp_path / "ref"
-    ref_out = ref_lib.bous3d_dns(xi, et, zt, rho, N, NU, DT, 1.0 + 80 * DT, resthresh=thr,
+    ref_out = ref_lib.bous3d_dns(xi, et, zt, rho, N, NU, DT, tend, resthresh=thr,
                                  workdir=str(wd), **kw)
     ref = _records(wd / "JOB0" / "UPO_ZK.out", nkt)
     assert ours.shape == ref.shape

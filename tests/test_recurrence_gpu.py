@@ -175,9 +175,15 @@ def test_recurrence_matches_restatement(store):
 
 
 def test_boussinesq_recurrence_matches_restatement():
-    """The Boussinesq DNS's variant on four fields (density weighted by Ri)."""
+    """The Boussinesq DNS's variant on four fields (density weighted by Ri).
+    Its norm of a stored state weights only the density's real part by Ri
+    (3D_Boussinesq/src/functions.h:199) while the residual weights both parts,
+    so an exact recurrence leaves a floor of sqrt((1 - Ri) sum Im(rho)^2 /
+    (|Z_old|^2 + |Z_new|^2)); the density here is a tenth of the vorticity
+    (floor ~ 0.015, below the threshold 0.05).  The selection reports twice the
+    period (1.6) with the matching shift 16 (= -2 x 7 mod 30) grid steps."""
     n, nw, ns, nout, dt, thr, ri = 16, 4, (30, 2, 2), 1, 0.1, 0.05, 0.7
-    seq = _sequence(n, 30, 8, ns[0], seed=9, nc=4)
+    seq = [[a, b, c, 0.1 * d] for a, b, c, d in _sequence(n, 30, 8, ns[0], seed=9, nc=4)]
     gpu = P.Recurrence3D(n, nout, dt, thr, store_size=40, norm_width=nw, nshift=ns, v2=0.02, ri=ri)
     ref = RecRef(n, 40, nw, ns, thr, nout, dt, 0.0, 0.02, ri=ri)
     dev = lambda st: torch.from_numpy(np.stack(st)).cuda()
@@ -198,4 +204,6 @@ def test_boussinesq_recurrence_matches_restatement():
             assert len(st) == 4
             for a, b in zip(st, ref.ring[slot]):
                 np.testing.assert_array_equal(a, b)
+            assert meta["period"] == pytest.approx(1.6)
+            assert meta["shift_x"] == pytest.approx(2 * math.pi * 16 / 30)
     assert n_emit >= 1
