@@ -122,31 +122,32 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n, word=8):
+def algorithmic_bytes(n, word=8, nc=3, nfi=6):
     """HBM bytes of one right-hand side per pass, complex words of `word` bytes,
     counting only kept modes (IKTX = n/3+1 columns, IKTY = IKTZ = 2(n/3)+1 rows)
-    and one read plus one write per pass; pass A also reads the 3 stage-state
+    and one read plus one write per pass; pass A also reads the nc stage-state
     components, pass E writes/reads the scheme registers (counted per stage in
-    stage_bytes)."""
+    stage_bytes).  nc state components, nfi fields through the x-pass (3, 6
+    for Navier-Stokes; 4, 9 for Boussinesq)."""
     K = n // 3
     X, Y = K + 1, 2 * K + 1
-    a = (3 * X * Y * Y + 6 * X * Y * n) * word
-    b = (6 * X * Y * n + 6 * X * n * n) * word
-    c = (6 * X * n * n + 3 * X * n * n) * word
-    d = (3 * X * n * n + 3 * X * Y * n) * word
-    e = (3 * X * Y * n) * word
+    a = (nc * X * Y * Y + nfi * X * Y * n) * word
+    b = (nfi * X * Y * n + nfi * X * n * n) * word
+    c = (nfi * X * n * n + nc * X * n * n) * word
+    d = (nc * X * n * n + nc * X * Y * n) * word
+    e = (nc * X * Y * n) * word
     return [a, b, c, d, e]
 
 
-def stage_bytes(n, stage, word=8):
-    """state/register traffic of pass E for RK4 stage 0..3 (3 components each):
+def stage_bytes(n, stage, word=8, nc=3, carried=True):
+    """state/register traffic of pass E for RK4 stage 0..3 (nc components each):
     stages 0-2 read S and write K_s and X0; the final stage reads S, K1, K2, K3
-    and the carried rounding error of the FP32 state, and writes S, X0 and that
-    error."""
+    (and the carried rounding error of the FP32 state) and writes S, X0 (and
+    that error)."""
     K = n // 3
     nkt = (K + 1) * (2 * K + 1) ** 2
-    arrays = 3 if stage < 3 else 8
-    return arrays * 3 * nkt * word
+    arrays = 3 if stage < 3 else (8 if carried else 6)
+    return arrays * nc * nkt * word
 
 
 # ---------------------------------------------------------------- our arm
@@ -261,6 +262,58 @@ def run_ours(args, rank, world, dist):
         }
         if out_note:
             out["note"] = out_note
+    return out
+
+
+def pass_table(args, nsteps=10):
+    """Per-pass live timings (CUDA events at the engine's pass boundaries,
+    psg_ns3d_profile_read) at args.grid^3 for the Navier-Stokes and
+    Boussinesq RK4/CN engines in FP32 and FP64, after 3 warm-up steps: average
+    launch time, algorithmic bytes (algorithmic_bytes / stage_bytes, the final
+    stage's registers averaged over the four stages) and the achieved fraction
+    of the measured HBM copy bandwidth.  Every pass input at 256^3 exceeds
+    the 126 MB L2."""
+    import torch
+    import psgpu_b200 as P
+    from psgpu_b200.fields import taylor_green3d
+
+    torch.cuda.set_device(0)
+    n = args.grid
+    peak, kind = measured_peaks()
+    xi, et, zt = taylor_green3d(n, 1234, amp=1e-3)
+    out = {"grid": n, "steps": nsteps, "peak_GBps": peak, "peak_kind": kind, "engines": {}}
+    for name, scheme, prec in (("ns_rk4_fp32", P.SCHEME_NS_RK4, 32),
+                               ("ns_rk4_fp64", P.SCHEME_NS_RK4, 64),
+                               ("bous_fp32", P.SCHEME_BOUS_RK4, 32),
+                               ("bous_fp64", P.SCHEME_BOUS_RK4, 64)):
+        bous = scheme == P.SCHEME_BOUS_RK4
+        eng = P.NS3D(n, scheme, precision=prec, nu=NU, ri=1.0 if bous else 0.0)
+        eng.upload(*((xi, et, zt, 0.01 * xi) if bous else (xi, et, zt)))
+        eng.step(DT, 3)
+        eng.sync()
+        eng.profile(True)
+        eng.step(DT, nsteps)
+        eng.sync()
+        prof = eng.profile_read()
+        eng.profile(False)
+        nc, nfi = (4, 9) if bous else (3, 6)
+        word = 8 if prec == 32 else 16
+        alg = algorithmic_bytes(n, word, nc, nfi)
+        stage = sum(stage_bytes(n, s, word, nc, carried=(prec == 32)) for s in range(4)) / 4.0
+        rows = {}
+        for i, (pname, (ms, cnt)) in enumerate(prof.items()):
+            b = alg[i] + (stage if i == 4 else 0)
+            t = ms / cnt / 1e3
+            rows[pname] = {"avg_launch_us": round(t * 1e6, 2), "algorithmic_MB": round(b / 1e6, 1),
+                           "achieved_GBps": round(b / t / 1e9, 1),
+                           "frac": round(b / t / 1e9 / peak, 4)}
+        tot_ms = sum(v[0] for v in prof.values())
+        step_b = 4 * sum(alg) + sum(stage_bytes(n, s, word, nc, carried=(prec == 32))
+                                    for s in range(4))
+        out["engines"][name] = {"passes": rows, "xpass_variant": eng.autotune(rerun=False),
+                                "ms_per_step_passes": round(tot_ms / nsteps, 4),
+                                "step_frac": round(step_b / (tot_ms / nsteps / 1e3) / 1e9 / peak, 4)}
+        eng.close()
     return out
 
 
@@ -1069,6 +1122,8 @@ def main():
                     help="also solve with the FP64 exact tangent")
     ap.add_argument("--no-upo-plain", action="store_true",
                     help="skip the run of the reference's plain UPO form")
+    ap.add_argument("--pass-table", action="store_true",
+                    help="per-pass live timings and roofline fractions of the 3D engines, then exit")
     ap.add_argument("--profile-case", default="", choices=("",) + PROFILE_CASES,
                     help="run one small fixed workload of a kernel family (for ncu) and exit")
     ap.add_argument("--upo-only", action="store_true",
@@ -1107,6 +1162,10 @@ def main():
     if args.profile_case:
         print(json.dumps(run_profile_case(args.profile_case, args.grid if args.grid != 256 else 0)),
               flush=True)
+        return
+    if args.pass_table:
+        if rank == 0:
+            print(json.dumps(pass_table(args)), flush=True)
         return
     if args.upo_only:
         if rank == 0:

@@ -88,12 +88,13 @@ int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps);
  * passes A..E (z-inverse, y-inverse, x, y-forward, z-forward + update) */
 int psg_ns3d_profile(psg_ns3d* h, int enable);
 int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts);
-/* re-run the set-up autotuner (x-pass rows per block and buffers per warp, timed on
- * this device); variant receives the choice, ms[4] the timing of each variant
- * (-1: does not fit) */
+/* re-run the set-up autotuner (x-pass rows per block, buffers per warp and, in FP32,
+ * packed f32x2 transforms; timed on this device); variant receives the choice (0..7:
+ * bit 0 twice the rows, bit 1 two buffers, bit 2 packed), ms[8] the timing of each
+ * variant (-1: does not fit, or packed in FP64) */
 int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
 /* the autotuner's current choice and timings, without re-running it
- * (PSG_XPASS_VARIANT=0..3 in the environment pins the choice at set-up) */
+ * (PSG_XPASS_VARIANT=0..7 in the environment pins the choice at set-up) */
 int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms);
 /* the state from / to device arrays: FP64 complex boxes in the reference
  * layout (IKTX*IKTY*IKTZ double2 per component), ordered on the engine's
@@ -284,6 +285,14 @@ int psg_upo2d_get_nu(psg_upo2d* h, int i, double* nu);
 int psg_upo2d_trace_count(psg_upo2d* h, int i);
 long psg_upo2d_integrations(psg_upo2d* h);
 long psg_upo2d_launches(psg_upo2d* h);
+/* Phase timing of psg_upo2d_solve.  psg_upo2d_profile(h, 1) clears the counters
+ * and synchronises the stream around every batched integration from then on
+ * (0 turns it off); psg_upo2d_profile_read fills out[6] = {seconds in solve,
+ * exact-Jv integrations in FP64, exact-Jv integrations in FP32, Phi_T
+ * integrations (residuals, hookstep trials, forward differences), dz/dt, host
+ * SVDs of the Hessenberg matrices}. */
+int psg_upo2d_profile(psg_upo2d* h, int enable);
+int psg_upo2d_profile_read(psg_upo2d* h, double* out);
 
 /* Allocation-free 2D step.  No counterpart in the reference.
  *

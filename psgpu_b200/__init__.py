@@ -135,6 +135,8 @@ def _declare_2d(L):
     L.psg_upo2d_launches.argtypes = [vp]
     L.psg_upo2d_launches.restype = C.c_long
     L.psg_upo2d_set_arc.argtypes = [vp, i, dp, dp] + [C.c_double] * 7
+    L.psg_upo2d_profile.argtypes = [vp, i]
+    L.psg_upo2d_profile_read.argtypes = [vp, dp]
     L.psg_upo2d_get_nu.argtypes = [vp, i, dp]
 
 
@@ -278,7 +280,7 @@ class NS3D:
     def autotune(self, rerun: bool = True):
         """x-pass autotuner: (chosen variant, ms per launch of each variant)"""
         v = C.c_int()
-        ms = (C.c_float * 4)()
+        ms = (C.c_float * 8)()
         fn = lib().psg_ns3d_autotune if rerun else lib().psg_ns3d_tuning
         _check(fn(self._h, C.byref(v), ms))
         return v.value, list(ms)
@@ -598,3 +600,13 @@ class UPO2D:
     @property
     def integrations(self):
         return int(lib().psg_upo2d_integrations(self._h))
+
+    def profile(self, enable: bool = True):
+        """phase timing of solve() (synchronises around every batched integration)"""
+        _check(lib().psg_upo2d_profile(self._h, int(enable)))
+
+    def profile_read(self):
+        out = np.zeros(6)
+        _check(lib().psg_upo2d_profile_read(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return dict(zip(("solve", "jv_exact64", "jv_exact32", "phi", "dzdt", "host_svd"),
+                        out.tolist()))

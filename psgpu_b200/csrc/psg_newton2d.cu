@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <vector>
 
 #include "psg_tan2d_run.cuh"
@@ -319,6 +320,12 @@ struct Upo2D {
   int* d_next = nullptr;
   cudaStream_t stream = 0;
   long launches = 0, integrations = 0;
+  // phase timing (psg_upo2d_profile): seconds in the batched integrations by
+  // kind (exact Jv FP64, exact Jv FP32, Phi_T, dz/dt), in the host SVDs, and in
+  // solve() as a whole; the stream is synchronised around each integration
+  // while it is on
+  bool prof = false;
+  double t_int[4] = {0, 0, 0, 0}, t_svd = 0, t_solve = 0;
   // blocks per instance (a cluster) when the batch leaves room: at most this many
   int cluster_max = 4;
   // side streams and events of integrations split over several launches
@@ -428,7 +435,18 @@ struct Upo2D {
     // FP32; every other integration (Phi_T, dz/dt, FP64 tangents) in FP64
     bool fp32 = jv_mode == 2;
     for (const IntReq& r : reqs) fp32 = fp32 && r.mode == 0;
-    return fp32 ? integrate_t<float>(reqs, plan32) : integrate_t<double>(reqs, plan64);
+    std::chrono::steady_clock::time_point t0;
+    if (prof) {
+      PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+      t0 = std::chrono::steady_clock::now();
+    }
+    const int rc = fp32 ? integrate_t<float>(reqs, plan32) : integrate_t<double>(reqs, plan64);
+    if (prof && !rc) {
+      PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+      const int kind = reqs[0].mode == 0 ? (fp32 ? 1 : 0) : reqs[0].mode == 1 ? 2 : 3;
+      t_int[kind] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return rc;
   }
 
   InstTan2D<double>& inst_of(Guess& U_, double*) { return U_.inst; }
@@ -868,7 +886,9 @@ struct Upo2D {
           for (int cc = 0; cc < c; ++cc)
             for (int rr = 0; rr < r; ++rr) A[(size_t)cc * r + rr] = U_.H[(size_t)cc * rows + rr];
           std::vector<double> Um, Sm, Vm;
+          const auto ts0 = std::chrono::steady_clock::now();
           jacobi_svd(r, c, A, Um, Sm, Vm);
+          if (prof) t_svd += std::chrono::duration<double>(std::chrono::steady_clock::now() - ts0).count();
           U_.P.assign(c, 0.0);
           for (int j = 0; j < c; ++j) U_.P[j] = U_.normb * Um[(size_t)j * r + 0];
           U_.S = Sm;
@@ -1186,7 +1206,13 @@ extern "C" int psg_upo2d_set_guess(psg_upo2d* h, int i, const double* Z, double 
 extern "C" int psg_upo2d_solve(psg_upo2d* h, int max_newton, double tol, double gmres_tol) {
   PSG_U2(h);
   h->u->gmtol = gmres_tol;
-  return h->u->solve(max_newton, tol);
+  const auto t0 = std::chrono::steady_clock::now();
+  const int rc = h->u->solve(max_newton, tol);
+  if (h->u->prof) {
+    cudaStreamSynchronize(h->u->stream);
+    h->u->t_solve += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return rc;
 }
 
 extern "C" int psg_upo2d_get(psg_upo2d* h, int i, double* Z, double* vals, int* info) {
@@ -1282,3 +1308,28 @@ extern "C" int psg_upo2d_trace_count(psg_upo2d* h, int i) {
 
 extern "C" long psg_upo2d_integrations(psg_upo2d* h) { return (h && h->u) ? h->u->integrations : -1; }
 extern "C" long psg_upo2d_launches(psg_upo2d* h) { return (h && h->u) ? h->u->launches : -1; }
+
+// phase timing of the solver: enable (1) clears the counters and synchronises
+// around every batched integration from then on; 0 turns it off
+extern "C" int psg_upo2d_profile(psg_upo2d* h, int enable) {
+  PSG_U2(h);
+  Upo2D& U = *h->u;
+  U.prof = enable != 0;
+  if (U.prof) {
+    for (double& t : U.t_int) t = 0;
+    U.t_svd = U.t_solve = 0;
+  }
+  return PSG_OK;
+}
+
+// out[6] = {seconds in solve, exact-Jv integrations FP64, exact-Jv FP32,
+// Phi_T integrations (residuals, trials, forward differences), dz/dt, host SVDs}
+extern "C" int psg_upo2d_profile_read(psg_upo2d* h, double* out) {
+  PSG_U2(h);
+  if (!out) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  const Upo2D& U = *h->u;
+  out[0] = U.t_solve;
+  for (int k = 0; k < 4; ++k) out[1 + k] = U.t_int[k];
+  out[5] = U.t_svd;
+  return PSG_OK;
+}

@@ -23,6 +23,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "psg_fft2.cuh"
 #include "psg_ns3d.cuh"
 #include "psg_tma.cuh"
 #include "psgpu_internal.h"
@@ -308,29 +309,117 @@ struct RowOps {
   static constexpr int G = FI::G, E = FI::E;
   static constexpr int SX = RowStride<FI::SMEM, FI::G>::value;
 
+  // row position r of the complex line a + i b whose inverse transform gives the
+  // real fields a, b (half spectra A, B in shared memory; B == nullptr: b = 0)
+  static __device__ __forceinline__ cpx<T> line_in(const cpx<T>* A, const cpx<T>* B, int r, int K) {
+    cpx<T> z = czero<T>();
+    if (r == 0) {
+      z = cpx<T>{A[0].x, B ? B[0].x : (T)0};
+    } else if (r <= K) {
+      const cpx<T> a = A[r], b = B ? B[r] : czero<T>();
+      z = cpx<T>{a.x - b.y, a.y + b.x};  // a + i b
+    } else if (r >= N - K) {
+      const cpx<T> a = A[N - r], b = B ? B[N - r] : czero<T>();
+      z = cpx<T>{a.x + b.y, -a.y + b.x};  // conj(a) + i conj(b)
+    }
+    return z;
+  }
+
   // inverse transform of two real fields a, b given by their half spectra (smem rows)
   static __device__ __forceinline__ void c2r_pair(const cpx<T>* A, const cpx<T>* B, int K,
                                                   int gi, const cpx<T>* tw, cpx<T>* ex,
                                                   T (&ra)[E], T (&rb)[E]) {
     cpx<T> v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int r = FI::in_index(gi, e);
-      cpx<T> z = czero<T>();
-      if (r == 0) {
-        z = cpx<T>{A[0].x, B ? B[0].x : (T)0};
-      } else if (r <= K) {
-        const cpx<T> a = A[r], b = B ? B[r] : czero<T>();
-        z = cpx<T>{a.x - b.y, a.y + b.x};  // a + i b
-      } else if (r >= N - K) {
-        const cpx<T> a = A[N - r], b = B ? B[N - r] : czero<T>();
-        z = cpx<T>{a.x + b.y, -a.y + b.x};  // conj(a) + i conj(b)
-      }
-      v[e] = z;
-    }
+    for (int e = 0; e < E; ++e) v[e] = line_in(A, B, FI::in_index(gi, e), K);
     FI::run(v, gi, tw, ex, WarpSync());
 #pragma unroll
     for (int e = 0; e < E; ++e) { ra[e] = v[e].x; rb[e] = v[e].y; }
+  }
+
+  // FP32: four real fields as two complex lines (a + i b, c + i d) through one
+  // packed f32x2 transform, the instruction count of one scalar line.  PK 1:
+  // the exchange crosses the scalar-sized buffer in two halves; PK 2: one
+  // pass through a buffer of twice the size.
+  template <int PK>
+  static __device__ __forceinline__ void c2r_quad(const cpx<T>* A, const cpx<T>* B, const cpx<T>* C,
+                                                  const cpx<T>* D, int K, int gi, const cpx<T>* tw,
+                                                  cpx<T>* ex, T (&ra)[E], T (&rb)[E], T (&rc)[E],
+                                                  T (&rd)[E]) {
+    static_assert(sizeof(T) == 4 && PK >= 1 && PK <= 2, "packed transforms are FP32");
+    Pk v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int r = FI::in_index(gi, e);
+      const cpx<T> z1 = line_in(A, B, r, K), z2 = line_in(C, D, r, K);
+      v[e] = Pk{make_float2(z1.x, z2.x), make_float2(z1.y, z2.y)};
+    }
+    if constexpr (PK == 2) LineFFT2<N, +1>::run(v, gi, tw, reinterpret_cast<float4*>(ex), WarpSync());
+    else LineFFT2<N, +1>::run(v, gi, tw, reinterpret_cast<float2*>(ex), WarpSync());
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      ra[e] = v[e].re.x; rb[e] = v[e].im.x; rc[e] = v[e].re.y; rd[e] = v[e].im.y;
+    }
+  }
+
+  // the split of a forward-transformed pair line Z = FFT(p + i q) into P, Q for
+  // k < XP (zero beyond K); z: this lane's outputs, ex: N words of exchange
+  static __device__ __forceinline__ void split_store(const cpx<T> (&z)[E], int K, int XP, int gi,
+                                                     cpx<T>* ex, cpx<T>* __restrict__ P,
+                                                     cpx<T>* __restrict__ Q, long tstride) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) ex[FO::out_index(gi, e)] = z[e];
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = FO::out_index(gi, e);
+      if (k < XP) {
+        cpx<T> pk = czero<T>(), qk = czero<T>();
+        if (k <= K) {
+          const cpx<T> a = z[e], b = ex[(N - k) & (N - 1)];
+          pk = cpx<T>{a.x + b.x, a.y - b.y};
+          qk = cpx<T>{a.y + b.y, b.x - a.x};
+        }
+        const long o = (long)(k / kTileW) * tstride + (k % kTileW);
+        P[o] = pk;
+        Q[o] = qk;
+      }
+    }
+    __syncwarp();
+  }
+
+  // FP32: forward transforms of (p + i q) and (r + i s) as one packed line pair;
+  // p, q (and r, s with s) pre-scaled by 1/2 for the split; s == nullptr: r
+  // alone, stored directly into Rr
+  template <int PK>
+  static __device__ __forceinline__ void r2c_quad(const T (&p)[E], const T (&q)[E], const T (&r)[E],
+                                                  const T* s, int K, int XP, int gi,
+                                                  const cpx<T>* tw, cpx<T>* ex,
+                                                  cpx<T>* __restrict__ P, cpx<T>* __restrict__ Q,
+                                                  cpx<T>* __restrict__ Rr, cpx<T>* __restrict__ S,
+                                                  long tstride) {
+    static_assert(sizeof(T) == 4 && PK >= 1 && PK <= 2, "packed transforms are FP32");
+    Pk v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = Pk{make_float2(p[e], r[e]), make_float2(q[e], s ? s[e] : 0.f)};
+    using FO2 = LineFFT2<N, -1, true>;
+    if constexpr (PK == 2) FO2::run(v, gi, tw, reinterpret_cast<float4*>(ex), WarpSync());
+    else FO2::run(v, gi, tw, reinterpret_cast<float2*>(ex), WarpSync());
+    cpx<T> z[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) z[e] = cpx<T>{v[e].re.x, v[e].im.x};
+    split_store(z, K, XP, gi, ex, P, Q, tstride);
+#pragma unroll
+    for (int e = 0; e < E; ++e) z[e] = cpx<T>{v[e].re.y, v[e].im.y};
+    if (s) {
+      split_store(z, K, XP, gi, ex, Rr, S, tstride);
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = FO::out_index(gi, e);
+        if (k < XP) Rr[(long)(k / kTileW) * tstride + (k % kTileW)] = (k <= K) ? z[e] : czero<T>();
+      }
+    }
   }
 
   // forward transform of two real signals p, q (q == nullptr: p alone); writes
@@ -389,12 +478,17 @@ struct RowOps {
 // memory), leaves the block count to the compiler (0).  Passes A and E in
 // FP64 at 256^3 likewise ask for one block per SM: their shared memory allows
 // no more, and the register cap of three would only make them spill.
-template <typename T, int N, int NF, int L, int ST>
+// PK (FP32 only): 0 one scalar transform per complex line; 1 or 2 two lines per
+// packed f32x2 transform (RowOps::c2r_quad / r2c_quad), with the exchange in
+// two halves through the scalar-sized buffer (1) or in one pass through a
+// buffer twice that size (2).
+template <typename T, int N, int NF, int L, int ST, int PK = 0>
 __global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G,
                                   (sizeof(T) == 4 && NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
        const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt,
        unsigned long long* __restrict__ umax) {
+  static_assert(PK == 0 || (sizeof(T) == 4 && NF != 7), "packed x-pass: FP32 forward fields");
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
   constexpr int RPW = 32 / G, WPB = L / RPW;  // rows per warp tile, warps per block
@@ -431,7 +525,7 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   if (lane == 0 && t < nwt) issue(t, 0);
   const long tstride = (long)N * N * kTileW;  // B3: successive xt tiles
   const long fstride = (long)XT * tstride;
-  cpx<T>* ex = s_ex + (warp * RPW + j) * R::SX;
+  cpx<T>* ex = s_ex + (warp * RPW + j) * R::SX * (PK == 2 ? 2 : 1);
   for (int i = 0; t < nwt; ++i, t += wstride) {
     const int b = (ST == 2) ? (i & 1) : 0;
     const uint32_t parity = (ST == 2) ? ((i >> 1) & 1) : (i & 1);
@@ -480,8 +574,58 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
       continue;
     }
     T xi[E], et[E], zt[E], u[E], v[E], w[E];
-    R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
-    R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
+    if constexpr (PK != 0) {
+      // packed: (u + i rho_x, v + i rho_y) -> (w + i rho_z, xi + i eta) -> zeta
+      // alone for the Boussinesq fields (u.grad rho first, so that at most six
+      // physical fields are live); (xi + i eta, zeta + i u) -> (v + i w) else
+      if constexpr (BOUS) {
+        T rx[E], ry[E], n4[E];
+        R::template c2r_quad<PK>(src + 3 * fs, src + 6 * fs, src + 4 * fs, src + 7 * fs, K, gi,
+                                 s_tw, ex, u, rx, v, ry);
+#pragma unroll
+        for (int e = 0; e < E; ++e) n4[e] = u[e] * rx[e] + v[e] * ry[e];
+        R::template c2r_quad<PK>(src + 5 * fs, src + 8 * fs, src, src + fs, K, gi, s_tw, ex, w, rx,
+                                 xi, et);
+#pragma unroll
+        for (int e = 0; e < E; ++e) n4[e] = (n4[e] + w[e] * rx[e]) * hscale;
+        R::c2r_pair(src + 2 * fs, nullptr, K, gi, s_tw, ex, zt, ry);
+        release();
+        if (umax) {
+          double m = 0.0;
+#pragma unroll
+          for (int e = 0; e < E; ++e) m = fmax(m, fabs((double)u[e]));
+          for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+          if (lane == 0) atomicMax(umax, (unsigned long long)__double_as_longlong(m));
+        }
+        if (dump) {
+          const long base = row * N;
+          const long nr = (long)N * N * N;
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const int x = R::FI::out_index(gi, e);
+            dump[base + x] = xi[e];
+            dump[nr + base + x] = et[e];
+            dump[2 * nr + base + x] = zt[e];
+          }
+        }
+        T n1[E], n2[E], n3[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          n1[e] = -(v[e] * zt[e] - w[e] * et[e]) * hscale;
+          n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * hscale;
+          n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * hscale;
+        }
+        R::template r2c_quad<PK>(n1, n2, n3, n4, K, XP, gi, two, ex, dst, dst + fstride,
+                                 dst + 2 * fstride, dst + 3 * fstride, tstride);
+        __syncwarp();
+        continue;
+      }
+      R::template c2r_quad<PK>(src, src + fs, src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, xi, et,
+                               zt, u);
+    } else {
+      R::c2r_pair(src, src + fs, K, gi, s_tw, ex, xi, et);
+      R::c2r_pair(src + 2 * fs, src + 3 * fs, K, gi, s_tw, ex, zt, u);
+    }
     R::c2r_pair(src + 4 * fs, src + 5 * fs, K, gi, s_tw, ex, v, w);
     if (!BOUS) release();
     if (umax) {
@@ -512,7 +656,10 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
       n2[e] = -(w[e] * xi[e] - u[e] * zt[e]) * hscale;
       n3[e] = -(u[e] * et[e] - v[e] * xi[e]) * (BOUS ? hscale : scale);
     }
-    if (!BOUS) {
+    if constexpr (PK != 0 && !BOUS) {
+      R::template r2c_quad<PK>(n1, n2, n3, nullptr, K, XP, gi, two, ex, dst, dst + fstride,
+                               dst + 2 * fstride, nullptr, tstride);
+    } else if (!BOUS) {
       R::r2c_pair(n1, n2, K, XP, gi, two, ex, dst, dst + fstride, tstride);
       R::r2c_pair(n3, nullptr, K, XP, gi, two, ex, dst + 2 * fstride, nullptr, tstride);
     } else {
@@ -1377,8 +1524,8 @@ struct Engine3D final : Engine3DBase {
   Fields4<T> LA{}, LN{}, LS{}, LZ{}, LK1{}, LK2{}, LK3{}, PA{}, PB{}, LD{}, LT{};
   Fields4<T> SA{}, SB{};       // Boussinesq adjoint products: psi (i k rho) | psi u
   int c_variant = 0;           // x-pass variant chosen by the autotuner
-  int c_resident[4] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
-  float c_ms[4] = {0, 0, 0, 0};      // autotuner timings (ms per launch)
+  int c_resident[8] = {1, 1, 1, 1, 0, 0, 0, 0};  // resident blocks of each x-pass variant
+  float c_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // autotuner timings (ms per launch)
   long launches = 0;
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
@@ -1426,10 +1573,12 @@ struct Engine3D final : Engine3DBase {
   size_t smem_b() const {
     return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.Y * kTileW, (size_t)kTileW * col_stride()) + g.n);
   }
-  // x-pass variants (rows per block in units of 128/G, buffers per warp)
-  static constexpr int kCVariants = 4;
+  // x-pass variants (rows per block in units of 128/G, buffers per warp; FP32
+  // also packed f32x2 transforms, two lines each, exchanging in two halves)
+  static constexpr int kCVariants = 8;
   static int c_rows_mult(int v) { return (v & 1) ? 2 : 1; }
   static int c_stages(int v) { return (v & 2) ? 2 : 1; }
+  static bool c_packed(int v) { return (v & 4) != 0; }
   size_t smem_c_v(int v) const {
     const size_t L = (size_t)(128 / fft_g()) * c_rows_mult(v);
     return sizeof(cpx<T>) * ((size_t)c_stages(v) * nfi * L * g.XP + 2 * g.n + L * row_stride());
@@ -1578,6 +1727,16 @@ struct Engine3D final : Engine3DBase {
     PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 1>));
     PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 2>));
     PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 2>));
+    if constexpr (sizeof(T) == 4) {
+      PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 1, 1>));
+      PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 1, 1>));
+      PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 2, 1>));
+      PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 2, 1>));
+      PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 1, 1>));
+      PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 1, 1>));
+      PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 2, 1>));
+      PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 2, 1>));
+    }
     PSG_SMEM((pass_d<T, N>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_HEUN>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_EULER_HEUN>));
@@ -1588,11 +1747,10 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     for (int v = 0; v < kCVariants; ++v) {
       int occ = 0;
-      if (smem_c_v(v) <= (size_t)big) {
-        const void* k = c_kernel<N>(v);
+      const void* k = c_kernel<N>(v);
+      if (k && smem_c_v(v) <= (size_t)big)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, c_threads<N>(v), smem_c_v(v));
-      }
-      c_resident[v] = nsm * occ;  // 0: variant does not fit
+      c_resident[v] = nsm * occ;  // 0: variant does not fit (or FP64 packed)
     }
     return PSG_OK;
   }
@@ -1603,6 +1761,17 @@ struct Engine3D final : Engine3DBase {
   const void* c_kernel(int v) const {
     constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
+    if (c_packed(v)) {
+      if constexpr (sizeof(T) == 4) {
+        switch (v & 3) {
+          case 0: return bous ? (const void*)pass_c<T, N, 9, L1, 1, 1> : (const void*)pass_c<T, N, 6, L1, 1, 1>;
+          case 1: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 1, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 1, 1>;
+          case 2: return bous ? (const void*)pass_c<T, N, 9, L1, 2, 1> : (const void*)pass_c<T, N, 6, L1, 2, 1>;
+          default: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 2, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 2, 1>;
+        }
+      }
+      return nullptr;
+    }
     switch (v) {
       case 0: return bous ? (const void*)pass_c<T, N, 9, L1, 1> : (const void*)pass_c<T, N, 6, L1, 1>;
       case 1: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 1>;
@@ -1623,6 +1792,24 @@ struct Engine3D final : Engine3DBase {
     const size_t sm = smem_c_v(v);
     const int th = c_threads<N>(v);
     if (!nf) nf = (scheme == SCHEME_BOUS_RK4) ? 9 : 6;
+    if constexpr (sizeof(T) == 4) {
+      // packed variants take the forward fields (6, 9); the adjoint's products
+      // (7) run the scalar variant of the same shape
+      if (c_packed(v) && nf != 7) {
+#define PSG_LCP(LL, STG)                                                                          \
+  if (nf == 9) pass_c<T, N, 9, LL, STG, 1><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
+  else pass_c<T, N, 6, LL, STG, 1><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um);
+        switch (v & 3) {
+          case 0: PSG_LCP(L1, 1); break;
+          case 1: PSG_LCP(2 * L1, 1); break;
+          case 2: PSG_LCP(L1, 2); break;
+          default: PSG_LCP(2 * L1, 2); break;
+        }
+#undef PSG_LCP
+        return PSG_OK;
+      }
+    }
+    v &= 3;
 #define PSG_LC(LL, STG)                                                                          \
   if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
   else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
@@ -1642,7 +1829,7 @@ struct Engine3D final : Engine3DBase {
   // fastest.  The transforms' cost does not depend on the data.
   template <int N>
   int autotune_n() {
-    // PSG_XPASS_VARIANT=0..3 pins the choice (reproducible profiling runs)
+    // PSG_XPASS_VARIANT=0..7 pins the choice (reproducible profiling runs)
     if (const char* pin = getenv("PSG_XPASS_VARIANT")) {
       const int v = atoi(pin);
       if (v >= 0 && v < kCVariants && c_resident[v] > 0) {

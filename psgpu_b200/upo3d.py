@@ -123,8 +123,9 @@ class UPO3D:
     # ------------------------------------------------------------------- solve
     def solve(self, Z, T, shifts=None, max_newton=100):
         """Z: array (ncomp, IKTZ, IKTY, IKTX) complex128; shifts: dict of the shift
-        unknowns (and fixed shifts).  Returns a dict with the orbit, the status
-        and a per-step trace."""
+        unknowns (and fixed shifts).  Returns a dict with the orbit, the status,
+        a per-step trace and, per Newton step, the GMRES residual after each
+        Krylov iteration (gmres_residuals)."""
         torch = self.torch
         dev = self.mask.device
         s = {a: 0.0 for a in ("x", "y", "z")}
@@ -140,7 +141,8 @@ class UPO3D:
         normfn = math.sqrt(self._dot(fn, fn))
         normz = math.sqrt(self._dot(znn, znn) + self._dot(znewt, znewt))
         ner = normfn / normz
-        out = {"status": "NEWTON FAILED", "steps": [], "gmres": 0, "hook": 0}
+        out = {"status": "NEWTON FAILED", "steps": [], "gmres": 0, "hook": 0,
+               "gmres_residuals": []}
         if ner <= self.netol:
             out.update(status="CONVERGED", Z=znewt.cpu().numpy(), T=tnewt, shifts=dict(s), ner=ner,
                        newton=0, integrations=self.integrations)
@@ -176,6 +178,8 @@ class UPO3D:
             # -------------------------------------------------------------- GMRES
             igm_done, gmr = 0, float("inf")
             P = S = VH = None
+            gmr_hist = []
+            out["gmres_residuals"].append(gmr_hist)
             for igm in range(1, kmax + 1):
                 v = jv(q[igm - 1], qn[igm - 1])
                 vn = np.array([self._dot(dzdt, q[igm - 1])] +
@@ -196,6 +200,7 @@ class UPO3D:
                 r = Hm @ yh
                 r[0] -= normb
                 gmr = float(np.sqrt(np.sum(r * r)) / normb)
+                gmr_hist.append(gmr)
                 if gmr <= self.gmtol:
                     igm_done = igm
                     break

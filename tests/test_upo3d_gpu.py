@@ -71,7 +71,10 @@ def test_phi_and_tangent():
 @pytest.mark.parametrize("jv", ["exact", "fd"])
 def test_newton_converges_to_laminar_state(jv):
     eng = _engine()
-    u = UPO3D(eng, DT, jv=jv, kmax=40)
+    # the x and z shifts barely move the near-laminar state (its shear mode is
+    # invariant under them): GMRES plateaus before it reaches GMTOL = 1e-7 near
+    # 45 iterations, inside a Krylov space of 80
+    u = UPO3D(eng, DT, jv=jv, kmax=80)
     r = u.solve(_perturbed(), T=1.0, shifts={"x": 0.0, "z": 0.0}, max_newton=15)
     assert r["status"] == "CONVERGED", (r["status"], r["ner"], r["steps"])
     assert r["ner"] <= 1e-10
