@@ -256,9 +256,10 @@ def run_ours(args, rank, world, dist):
             "reference_steady": ref_steady,
             "clocks": clocks, "gpu_launches": int(launches),
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
-                                "variants": ["L=128/G,1 buffer per warp", "L=256/G,1 buffer per warp",
-                                             "L=128/G,2 buffers per warp",
-                                             "L=256/G,2 buffers per warp"]},
+                                "variants": "bit 0: 256/G rows per block (else 128/G), bit 3: "
+                                            "64/G rows, bit 1: two copy buffers per warp, bit 2: "
+                                            "packed f32x2 transforms (FP32); -1: not built or "
+                                            "does not fit"},
         }
         if out_note:
             out["note"] = out_note

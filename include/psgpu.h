@@ -89,12 +89,13 @@ int psg_ns3d_layout(psg_ns3d* h, int* xp, void** comps);
 int psg_ns3d_profile(psg_ns3d* h, int enable);
 int psg_ns3d_profile_read(psg_ns3d* h, double* ms, long* counts);
 /* re-run the set-up autotuner (x-pass rows per block, buffers per warp and, in FP32,
- * packed f32x2 transforms; timed on this device); variant receives the choice (0..7:
- * bit 0 twice the rows, bit 1 two buffers, bit 2 packed), ms[8] the timing of each
- * variant (-1: does not fit, or packed in FP64) */
+ * packed f32x2 transforms; timed on this device); variant receives the choice (0..15:
+ * bit 0 twice the rows, bit 3 half of them, bit 1 two buffers, bit 2 packed), ms[16]
+ * the timing of each variant (-1: does not fit, or not built: bits 0 and 3 together,
+ * packed in FP64) */
 int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
 /* the autotuner's current choice and timings, without re-running it
- * (PSG_XPASS_VARIANT=0..7 in the environment pins the choice at set-up) */
+ * (PSG_XPASS_VARIANT=0..15 in the environment pins the choice at set-up) */
 int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms);
 /* the state from / to device arrays: FP64 complex boxes in the reference
  * layout (IKTX*IKTY*IKTZ double2 per component), ordered on the engine's

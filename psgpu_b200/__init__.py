@@ -280,7 +280,7 @@ class NS3D:
     def autotune(self, rerun: bool = True):
         """x-pass autotuner: (chosen variant, ms per launch of each variant)"""
         v = C.c_int()
-        ms = (C.c_float * 8)()
+        ms = (C.c_float * 16)()
         fn = lib().psg_ns3d_autotune if rerun else lib().psg_ns3d_tuning
         _check(fn(self._h, C.byref(v), ms))
         return v.value, list(ms)

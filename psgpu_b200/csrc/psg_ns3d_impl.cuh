@@ -1339,10 +1339,12 @@ __device__ __forceinline__ void remove_div(const TileMode<T>& m, cpx<T> (&o)[M])
 }
 
 // tangent final stage:
-// D' = Pdiv LL [(1 - eS) D + (1 - eI)(K1/6 + dt n/6 + (K2 + K3)/3)]
+// D' = Pdiv LL [(1 - eS) D + (1 - eI)(K1/6 + dt n/6 + (K2 + K3)/3)]; DX' = the
+// same before the divergence removal (the tangent of the stage input the next
+// step starts from: the forward step hands its final stage on unprojected)
 template <typename T>
 __global__ void tan_final(Geom3<T> g, T dt, T nu, Fields4<T> n, Fields4<T> K1, Fields4<T> K2,
-                          Fields4<T> K3, Fields4<T> D, long len, int nc, T sc) {
+                          Fields4<T> K3, Fields4<T> D, Fields4<T> DX, long len, int nc, T sc) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
        i += (long)gridDim.x * blockDim.x) {
     const TileMode<T> m = tile_mode(g, i);
@@ -1357,6 +1359,7 @@ __global__ void tan_final(Geom3<T> g, T dt, T nu, Fields4<T> n, Fields4<T> K1, F
       const T iy = sixth * (a.y + dt * nn.y) + third * (b.y + k3.y);
       o[c] = cpx<T>{LL * ((d.x - eS * d.x) + (ix - eI * ix)), LL * ((d.y - eS * d.y) + (iy - eI * iy))};
     }
+    for (int c = 0; c < nc; ++c) DX.c[c][i] = o[c];
     remove_div(m, o);
     for (int c = 0; c < nc; ++c) D.c[c][i] = o[c];
   }
@@ -1522,10 +1525,15 @@ struct Engine3D final : Engine3DBase {
   cpx<T>* lin = nullptr;
   Fields4<T> Zb[4]{};          // base stage states z, z1, z2, z3
   Fields4<T> LA{}, LN{}, LS{}, LZ{}, LK1{}, LK2{}, LK3{}, PA{}, PB{}, LD{}, LT{};
+  // LX: the stage input X0 kept across a Boussinesq tangent right-hand side
+  // (which evaluates the engine's own right-hand side through X0); LDX: the
+  // tangent of X0 after a tangent step, valid while lin_dx is set
+  Fields4<T> LX{}, LDX{};
+  bool lin_dx = false;
   Fields4<T> SA{}, SB{};       // Boussinesq adjoint products: psi (i k rho) | psi u
   int c_variant = 0;           // x-pass variant chosen by the autotuner
-  int c_resident[8] = {1, 1, 1, 1, 0, 0, 0, 0};  // resident blocks of each x-pass variant
-  float c_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // autotuner timings (ms per launch)
+  int c_resident[16] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
+  float c_ms[16] = {};                 // autotuner timings (ms per launch)
   long launches = 0;
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
@@ -1573,14 +1581,16 @@ struct Engine3D final : Engine3DBase {
   size_t smem_b() const {
     return sizeof(cpx<T>) * (std::max<size_t>((size_t)g.Y * kTileW, (size_t)kTileW * col_stride()) + g.n);
   }
-  // x-pass variants (rows per block in units of 128/G, buffers per warp; FP32
-  // also packed f32x2 transforms, two lines each, exchanging in two halves)
-  static constexpr int kCVariants = 8;
-  static int c_rows_mult(int v) { return (v & 1) ? 2 : 1; }
+  // x-pass variants: bit 0 twice the rows per block (256/G instead of 128/G),
+  // bit 3 half of them (64/G; not with bit 0), bit 1 two copy buffers per
+  // warp, bit 2 (FP32) packed f32x2 transforms, two lines each
+  static constexpr int kCVariants = 16;
+  static int c_rows_x2(int v) { return (v & 8) ? 1 : (v & 1) ? 4 : 2; }  // rows in units of 64/G
   static int c_stages(int v) { return (v & 2) ? 2 : 1; }
   static bool c_packed(int v) { return (v & 4) != 0; }
+  static bool c_valid(int v) { return !((v & 8) && (v & 1)) && (!c_packed(v) || sizeof(T) == 4); }
   size_t smem_c_v(int v) const {
-    const size_t L = (size_t)(128 / fft_g()) * c_rows_mult(v);
+    const size_t L = (size_t)(64 / fft_g()) * c_rows_x2(v);
     return sizeof(cpx<T>) * ((size_t)c_stages(v) * nfi * L * g.XP + 2 * g.n + L * row_stride());
   }
   size_t smem_d() const {
@@ -1719,23 +1729,12 @@ struct Engine3D final : Engine3DBase {
     PSG_SMEM((pass_a<T, N, 3, 6>));
     PSG_SMEM((pass_a<T, N, 4, 9, 0, 3>));
     PSG_SMEM((pass_b<T, N>));
-    PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 1>));
-    PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 1>));
-    PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 2>));
-    PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 2>));
-    PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 1>));
-    PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 1>));
-    PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 2>));
-    PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 2>));
-    if constexpr (sizeof(T) == 4) {
-      PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 1, 1>));
-      PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 1, 1>));
-      PSG_SMEM((pass_c<T, N, 6, 128 / LineFFT<N, 1, T>::G, 2, 1>));
-      PSG_SMEM((pass_c<T, N, 6, 256 / LineFFT<N, 1, T>::G, 2, 1>));
-      PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 1, 1>));
-      PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 1, 1>));
-      PSG_SMEM((pass_c<T, N, 9, 128 / LineFFT<N, 1, T>::G, 2, 1>));
-      PSG_SMEM((pass_c<T, N, 9, 256 / LineFFT<N, 1, T>::G, 2, 1>));
+    for (int v = 0; v < kCVariants; ++v) {
+      if (!c_valid(v)) continue;
+      for (int nf : {6, 9, 7}) {
+        const void* k = c_kernel_nf<N>(v, nf);
+        if (k) PSG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      }
     }
     PSG_SMEM((pass_d<T, N>));
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_HEUN>));
@@ -1747,80 +1746,67 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     for (int v = 0; v < kCVariants; ++v) {
       int occ = 0;
-      const void* k = c_kernel<N>(v);
+      const void* k = c_valid(v) ? c_kernel<N>(v) : nullptr;
       if (k && smem_c_v(v) <= (size_t)big)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, c_threads<N>(v), smem_c_v(v));
-      c_resident[v] = nsm * occ;  // 0: variant does not fit (or FP64 packed)
+      c_resident[v] = nsm * occ;  // 0: variant does not fit (or is not built)
     }
     return PSG_OK;
   }
 
   template <int N>
-  static int c_threads(int v) { return 128 * c_rows_mult(v); }
+  static int c_threads(int v) { return 64 * c_rows_x2(v); }
+
+  // the kernel of variant v for nf fields (nullptr: not built; the packed
+  // form takes the forward fields only, the adjoint's products (7) run the
+  // scalar kernel of the same shape)
+  template <int N, int L, int ST>
+  static const void* c_fn(int nf, bool pk) {
+    if constexpr (sizeof(T) == 4) {
+      if (pk && nf != 7)
+        return nf == 9 ? (const void*)pass_c<T, N, 9, L, ST, 1> : (const void*)pass_c<T, N, 6, L, ST, 1>;
+    }
+    if (pk && sizeof(T) != 4) return nullptr;
+    return nf == 9 ? (const void*)pass_c<T, N, 9, L, ST> :
+           nf == 7 ? (const void*)pass_c<T, N, 7, L, ST> : (const void*)pass_c<T, N, 6, L, ST>;
+  }
+  template <int N>
+  static const void* c_kernel_nf(int v, int nf) {
+    constexpr int L0 = 64 / LineFFT<N, 1, T>::G;
+    const bool pk = c_packed(v);
+    const int rows = c_rows_x2(v), st = c_stages(v);
+    if (rows == 1) return st == 1 ? c_fn<N, L0, 1>(nf, pk) : c_fn<N, L0, 2>(nf, pk);
+    if (rows == 2) return st == 1 ? c_fn<N, 2 * L0, 1>(nf, pk) : c_fn<N, 2 * L0, 2>(nf, pk);
+    return st == 1 ? c_fn<N, 4 * L0, 1>(nf, pk) : c_fn<N, 4 * L0, 2>(nf, pk);
+  }
   template <int N>
   const void* c_kernel(int v) const {
-    constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
-    const bool bous = (scheme == SCHEME_BOUS_RK4);
-    if (c_packed(v)) {
-      if constexpr (sizeof(T) == 4) {
-        switch (v & 3) {
-          case 0: return bous ? (const void*)pass_c<T, N, 9, L1, 1, 1> : (const void*)pass_c<T, N, 6, L1, 1, 1>;
-          case 1: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 1, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 1, 1>;
-          case 2: return bous ? (const void*)pass_c<T, N, 9, L1, 2, 1> : (const void*)pass_c<T, N, 6, L1, 2, 1>;
-          default: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 2, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 2, 1>;
-        }
-      }
-      return nullptr;
-    }
-    switch (v) {
-      case 0: return bous ? (const void*)pass_c<T, N, 9, L1, 1> : (const void*)pass_c<T, N, 6, L1, 1>;
-      case 1: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 1> : (const void*)pass_c<T, N, 6, 2 * L1, 1>;
-      case 2: return bous ? (const void*)pass_c<T, N, 9, L1, 2> : (const void*)pass_c<T, N, 6, L1, 2>;
-      default: return bous ? (const void*)pass_c<T, N, 9, 2 * L1, 2> : (const void*)pass_c<T, N, 6, 2 * L1, 2>;
-    }
+    return c_kernel_nf<N>(v, scheme == SCHEME_BOUS_RK4 ? 9 : 6);
   }
   template <int N>
   // nf: fields the x-pass reads (6: -(u x w); 9: + u.grad rho; 7: the
   // Boussinesq adjoint's scalar products); 0: the engine's own
   int launch_c(int v, T scale, T* dp, int nf = 0, unsigned long long* um = nullptr) {
-    constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
+    constexpr int L0 = 64 / LineFFT<N, 1, T>::G;
     constexpr int RPW = 32 / LineFFT<N, 1, T>::G;  // rows per warp tile
-    const int wpb = L1 * c_rows_mult(v) / RPW;     // warps per block
+    const int wpb = L0 * c_rows_x2(v) / RPW;       // warps per block
     const int nwt = (N * N) / RPW;
     const int nblk = (nwt + wpb - 1) / wpb;
     const int grid = nblk < c_resident[v] ? nblk : c_resident[v];
     const size_t sm = smem_c_v(v);
     const int th = c_threads<N>(v);
     if (!nf) nf = (scheme == SCHEME_BOUS_RK4) ? 9 : 6;
-    if constexpr (sizeof(T) == 4) {
-      // packed variants take the forward fields (6, 9); the adjoint's products
-      // (7) run the scalar variant of the same shape
-      if (c_packed(v) && nf != 7) {
-#define PSG_LCP(LL, STG)                                                                          \
-  if (nf == 9) pass_c<T, N, 9, LL, STG, 1><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
-  else pass_c<T, N, 6, LL, STG, 1><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um);
-        switch (v & 3) {
-          case 0: PSG_LCP(L1, 1); break;
-          case 1: PSG_LCP(2 * L1, 1); break;
-          case 2: PSG_LCP(L1, 2); break;
-          default: PSG_LCP(2 * L1, 2); break;
-        }
-#undef PSG_LCP
-        return PSG_OK;
-      }
-    }
-    v &= 3;
-#define PSG_LC(LL, STG)                                                                          \
-  if (nf == 9) pass_c<T, N, 9, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
-  else if (nf == 7) pass_c<T, N, 7, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um); \
-  else pass_c<T, N, 6, LL, STG><<<grid, th, sm, stream>>>(g, B2, B1, tw, scale, dp, d_status, nwt, um);
-    switch (v) {
-      case 0: PSG_LC(L1, 1); break;
-      case 1: PSG_LC(2 * L1, 1); break;
-      case 2: PSG_LC(L1, 2); break;
-      default: PSG_LC(2 * L1, 2); break;
-    }
-#undef PSG_LC
+    const void* k = c_kernel_nf<N>(v, nf);
+    if (!k) { psg_set_error("x-pass variant %d is not built", v); return PSG_ERR_ARG; }
+    Geom3<T> gg = g;
+    const cpx<T>* in = B2;
+    cpx<T>* out = B1;
+    const cpx<T>* twp = tw;
+    int* st = d_status;
+    int nw = nwt;
+    unsigned long long* u = um;
+    void* args[] = {&gg, &in, &out, &twp, &scale, &dp, &st, &nw, &u};
+    PSG_CUDA_TRY(cudaLaunchKernel(k, dim3(grid), dim3(th), args, sm, stream));
     return PSG_OK;
   }
 
@@ -1829,7 +1815,7 @@ struct Engine3D final : Engine3DBase {
   // fastest.  The transforms' cost does not depend on the data.
   template <int N>
   int autotune_n() {
-    // PSG_XPASS_VARIANT=0..7 pins the choice (reproducible profiling runs)
+    // PSG_XPASS_VARIANT=0..15 pins the choice (reproducible profiling runs)
     if (const char* pin = getenv("PSG_XPASS_VARIANT")) {
       const int v = atoi(pin);
       if (v >= 0 && v < kCVariants && c_resident[v] > 0) {
@@ -1971,6 +1957,7 @@ struct Engine3D final : Engine3DBase {
   // predictor (Heun schemes)
   int step(T dt, bool want_dump = false) {
     prm.dt = dt;
+    lin_dx = false;
     int rc;
     if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) {
       if ((rc = rhs(STAGE_HEUN_PRED))) return rc;
@@ -1997,6 +1984,7 @@ struct Engine3D final : Engine3DBase {
       ++launches;
     }
     first_rhs = 1;
+    lin_dx = false;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -2015,6 +2003,7 @@ struct Engine3D final : Engine3DBase {
       ++launches;
     }
     first_rhs = 1;
+    lin_dx = false;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -2068,11 +2057,8 @@ struct Engine3D final : Engine3DBase {
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, big));
       PSG_CUDA_TRY(cudaFuncSetAttribute(pass_e<T, N, 6, SCHEME_RAW>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-      constexpr int L1 = 128 / LineFFT<N, 1, T>::G;
-      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, L1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, 2 * L1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, L1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-      PSG_CUDA_TRY(cudaFuncSetAttribute(pass_c<T, N, 7, 2 * L1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+      // the x-pass kernels of the adjoint's products (7 fields) got their
+      // shared-memory limit with the engine's own (set_smem_limits_n)
     }
     return PSG_OK;
   }
@@ -2093,9 +2079,9 @@ struct Engine3D final : Engine3DBase {
     }
     if (rc) return rc;
     // state-shaped registers (nc components) and product outputs (3, or 4 + 2)
-    constexpr int kState = 13;
+    constexpr int kState = 15;
     Fields4<T>* st[kState] = {&Zb[0], &Zb[1], &Zb[2], &Zb[3], &LA, &LN, &LS,
-                              &LZ, &LK1, &LK2, &LK3, &LD, &LT};
+                              &LZ, &LK1, &LK2, &LK3, &LD, &LT, &LX, &LDX};
     const long words = ((long)kState * nc + 3 + 3 + (nc > 3 ? 6 : 0)) * box;
     PSG_CUDA_TRY(cudaMalloc(&lin, sizeof(cpx<T>) * words));
     PSG_CUDA_TRY(cudaMemsetAsync(lin, 0, sizeof(cpx<T>) * words, stream));
@@ -2221,6 +2207,7 @@ struct Engine3D final : Engine3DBase {
       const T sc = (T)(nz > 0.0 ? sqrt(nz / nx) : 1.0);
       const int saved_first = first_rhs;
       first_rhs = 0;
+      copy_fields<T><<<592, 256, 0, stream>>>(R.X0, LX, nc, box);
       lin_shift<T><<<592, 256, 0, stream>>>(R.X0, z, sc, x, box, nc);
       ++launches;
       if ((rc = rhs(STAGE_DERIV))) return rc;
@@ -2231,7 +2218,8 @@ struct Engine3D final : Engine3DBase {
       first_rhs = saved_first;
       copy_fields<T><<<592, 256, 0, stream>>>(LT, out, nc, box);
       lin_axpby<T><<<592, 256, 0, stream>>>(out, (T)(0.5) / sc, (T)(-0.5) / sc, R.K1, box, nc);
-      launches += 2;
+      copy_fields<T><<<592, 256, 0, stream>>>(LX, R.X0, nc, box);
+      launches += 4;
       PSG_CUDA_TRY(cudaGetLastError());
       return PSG_OK;
     }
@@ -2246,11 +2234,14 @@ struct Engine3D final : Engine3DBase {
   }
 
   // one forward step from S with X0 = S, keeping the four stage states
+  // the base step as step() takes it: from the stage input X0 (the state after
+  // an upload, the previous step's final stage before its divergence removal
+  // otherwise), stage inputs kept in Zb; afterwards S and X0 are what step()
+  // leaves
   int base_stages(T dt) {
     prm.dt = dt;
-    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
-    copy_fields<T><<<592, 256, 0, stream>>>(R.S, Zb[0], nc, box);
-    launches += 2;
+    copy_fields<T><<<592, 256, 0, stream>>>(R.X0, Zb[0], nc, box);
+    launches += 1;
     const int stg[3] = {STAGE_RK1, STAGE_RK2, STAGE_RK3};
     for (int s = 0; s < 3; ++s) {
       if (int rc = rhs(stg[s])) return rc;
@@ -2260,21 +2251,17 @@ struct Engine3D final : Engine3DBase {
     return rhs(STAGE_RK4);
   }
 
-  // after a linearised step: the stage state of the advanced state is the
-  // state itself, as after an upload (the Boussinesq tangent reuses X0, K1)
-  void reset_stage_state() {
-    copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
-    ++launches;
-  }
-
-  // D <- dPhi(S) D, S <- Phi(S)
-  int tangent_step_t(T dt, Fields4<T> D) {
+  // (D, DX) <- the tangent of one step at (S, X0) applied to the tangent D of
+  // the state and DX of the stage input; S, X0 <- the step.  DXout receives the
+  // tangent of the new stage input (may alias DX, read only by the first
+  // stage).
+  int tangent_step_t(T dt, Fields4<T> D, Fields4<T> DX, Fields4<T> DXout) {
     int rc;
     if ((rc = base_stages(dt))) return rc;
     const T nu = prm.nu;
     const T qs[3] = {(T)0.25, (T)0.25, (T)0.5}, frs[3] = {(T)0.5, (T)0.5, (T)1};
     Fields4<T> Ks[3] = {LK1, LK2, LK3};
-    Fields4<T> in = D;
+    Fields4<T> in = DX;
     const T sc = prm.sc;
     for (int s = 0; s < 3; ++s) {
       if ((rc = lin_rhs(0, Zb[s], in, LN))) return rc;
@@ -2283,9 +2270,8 @@ struct Engine3D final : Engine3DBase {
       in = LA;
     }
     if ((rc = lin_rhs(0, Zb[3], LA, LN))) return rc;
-    tan_final<T><<<592, 256, 0, stream>>>(g, dt, nu, LN, LK1, LK2, LK3, D, box, nc, sc);
+    tan_final<T><<<592, 256, 0, stream>>>(g, dt, nu, LN, LK1, LK2, LK3, D, DXout, box, nc, sc);
     ++launches;
-    reset_stage_state();
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -2309,7 +2295,6 @@ struct Engine3D final : Engine3DBase {
     lin_axpby<T><<<592, 256, 0, stream>>>(LZ, (T)1, (T)1, LS, box, nc);
     copy_fields<T><<<592, 256, 0, stream>>>(LZ, L, nc, box);
     launches += 2;
-    reset_stage_state();
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
@@ -2325,8 +2310,14 @@ struct Engine3D final : Engine3DBase {
     launches += nc;
     Fields4<T> res = LD;
     switch (mode) {
-      case 0: rc = tangent_step_t((T)dt, LD); break;
-      case 1: rc = adjoint_step_t((T)dt, LD); break;
+      case 0:
+        // a tangent step that follows another on the same trajectory starts
+        // from the previous one's stage-input tangent; after an upload or a
+        // plain step, from the state's
+        rc = tangent_step_t((T)dt, LD, lin_dx ? LDX : LD, LDX);
+        lin_dx = true;
+        break;
+      case 1: rc = adjoint_step_t((T)dt, LD); lin_dx = false; break;
       case 2: rc = lin_rhs(0, R.S, LD, LS); res = LS; break;
       case 3: rc = lin_rhs(1, R.S, LD, LS); res = LS; break;
       default: psg_set_error("linear mode %d unknown", mode); return PSG_ERR_ARG;

@@ -6,6 +6,8 @@
 // parallel); other files see only the explicit-instantiation declarations
 // below.
 #pragma once
+#include <stdlib.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -159,6 +161,9 @@ struct IntPlan {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[0], 256, smem);
+    // PSG_UPO_BLOCKS_PER_SM caps the blocks the dealing counts on per SM (the
+    // FP32 integrator fits two)
+    if (const char* e = getenv("PSG_UPO_BLOCKS_PER_SM")) occ = std::min(occ, std::max(1, atoi(e)));
     grid_cap = nsm * std::max(occ, 1);
     return PSG_OK;
   }

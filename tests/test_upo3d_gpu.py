@@ -5,10 +5,17 @@
   T - t > dt, then the remainder; the drop-in is checked against the
   reference in test_parity_gpu.py); the exact tangent of that integration
   equals the central difference of Phi_T to 1e-7.
+  The tangent carries the stage input the engine's step hands on to the next
+  step (its final stage before the divergence removal), so the check holds
+  over many steps for inputs with a divergence too (a random q).
 * Newton from a perturbed laminar state of forced Boussinesq flow at 16^3
   (Re = 2, Ri = 1: the laminar shear is stable) reaches the reference's
   NETOL = 1e-10 with the exact tangent and with the forward difference, and
-  lands on the laminar state.
+  lands on the laminar state.  The shear is invariant under the x and z
+  shifts and steady in time, so those unknowns are nearly degenerate and
+  GMRES stalls on its way to the driver's GMTOL = 1e-7 (80 iterations were
+  not always enough); the test asks for 1e-4, which Newton turns into the
+  same final residual in a few more steps.
 """
 import numpy as np
 import pytest
@@ -72,10 +79,9 @@ def test_phi_and_tangent():
 def test_newton_converges_to_laminar_state(jv):
     eng = _engine()
     # the x and z shifts barely move the near-laminar state (its shear mode is
-    # invariant under them): GMRES plateaus before it reaches GMTOL = 1e-7 near
-    # 45 iterations, inside a Krylov space of 80
-    u = UPO3D(eng, DT, jv=jv, kmax=80)
-    r = u.solve(_perturbed(), T=1.0, shifts={"x": 0.0, "z": 0.0}, max_newton=15)
+    # invariant under them) and it is nearly steady: GMRES tolerance 1e-4
+    u = UPO3D(eng, DT, jv=jv, kmax=80, gmtol=1e-4)
+    r = u.solve(_perturbed(), T=1.0, shifts={"x": 0.0, "z": 0.0}, max_newton=25)
     assert r["status"] == "CONVERGED", (r["status"], r["ner"], r["steps"])
     assert r["ner"] <= 1e-10
     lam = _laminar()

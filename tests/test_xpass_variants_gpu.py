@@ -3,8 +3,9 @@ a variant that does not fit the device at that size is skipped) gives the
 same step as variant 1, for the RK4/CN and the Heun/CN (with the physical
 vorticity it keeps) schemes and the Boussinesq RK4/CN scheme (nine fields
 through the x-pass): 1e-12 in FP64, 2e-6 in FP32 (max-norm relative).  The
-FP32 variants 4-7 transform two lines per packed f32x2 instruction (their
-products round in another order: 2e-6 holds them too)."""
+FP32 variants 4-7 and 12, 14 transform two lines per packed f32x2
+instruction (their products round in another order: 2e-6 holds them too);
+variants 8-14 (even) run blocks of half the rows."""
 import numpy as np
 import pytest
 
@@ -43,7 +44,7 @@ def _rel(a, b):
 def test_xpass_variants_agree(monkeypatch, prec, scheme, n):
     ref, ref_ph = _run(monkeypatch, 1, n, scheme, prec)
     assert ref is not None
-    for v in (0, 2, 3, 4, 5, 6, 7):
+    for v in (0, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14):
         st, ph = _run(monkeypatch, v, n, scheme, prec)
         if st is None:
             continue
