@@ -530,7 +530,9 @@ def run_upo(args):
     form (exact tangent Jv integrated in FP32), with the FP64 forward
     difference of the same solver beside it, and the reference's plain form
     (one guess at a time, one reference timestep_cuda_ call per integration)
-    run on the shortest-period guess."""
+    run on the shortest-period guess; then the --upo-converge shortest-period
+    guesses solved in both forms for up to --upo-converge-newton iterations,
+    with the orbits converged to 1e-10 and the seconds per converged orbit."""
     guesses, out = upo_guesses()
     out["workload"] = ("2D Kolmogorov Re=40 128^2, 64 guesses from turbulent states after a "
                        "500 time-unit spin-up, periods in [5,20] from the recurrence search, "
@@ -549,6 +551,16 @@ def run_upo(args):
                                           plain["newton_iters_per_s"], 1)
     out["exact_vs_fd"] = round(out["exact_jv"]["newton_iters_per_s"] /
                                out["fd_jv"]["newton_iters_per_s"], 3)
+    if args.upo_converge:
+        # to convergence within the default run's time: the shortest-period
+        # guesses, up to `upo_converge_newton` Newton iterations each
+        short = sorted(guesses, key=lambda g: g[1])[:args.upo_converge]
+        conv = {"guesses": len(short), "newton_per_guess_max": args.upo_converge_newton,
+                "periods": [round(float(g[1]), 3) for g in short]}
+        for form in ("exact32", "fd"):
+            conv[{"exact32": "exact_jv", "fd": "fd_jv"}[form]] = \
+                solve_upo(short, form, args.upo_converge_newton)
+        out["to_convergence"] = conv
     return out
 
 
@@ -1119,6 +1131,10 @@ def main():
     ap.add_argument("--no-upo", action="store_true", help="skip the UPO Newton leg")
     ap.add_argument("--upo-newton", type=int, default=3,
                     help="largest number of Newton iterations per guess in the UPO leg")
+    ap.add_argument("--upo-converge", type=int, default=8, metavar="G",
+                    help="also solve the G shortest-period guesses to convergence (0: skip)")
+    ap.add_argument("--upo-converge-newton", type=int, default=12,
+                    help="Newton iterations per guess of the to-convergence sub-leg")
     ap.add_argument("--upo-all-forms", action="store_true",
                     help="also solve with the FP64 exact tangent")
     ap.add_argument("--no-upo-plain", action="store_true",
