@@ -630,6 +630,7 @@ def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
         b.upload(i, ics[i])
     b.set_params(nu, 0.005, steps)
     tune = b.autotune()
+    sched = b.schedule()
     stream = torch.cuda.current_stream()
     b.set_stream(stream.cuda_stream)
     b.launch()  # warm-up: captures the graph
@@ -667,7 +668,9 @@ def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
            "e2e_instance_steps_per_s": round(M * steps / e2e_s, 1), "e2e_seconds": round(e2e_s, 3),
            "scaling": "strong", "ranks": world, "gpu_launches": launches, "finite": bool(finite),
            "block_autotune": {"variant": tune[0], "ms_per_2_steps": [round(x, 4) for x in tune[1]],
-                              "threads": [128, 256, 512]}}
+                              "threads": [128, 256, 512]},
+           "transform_schedule": {str(n): {"packed": pk, "ms_scalar_packed": [round(x, 4) for x in ms]}
+                                  for n, (pk, ms) in sched.items() if ms[0] >= 0}}
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
     if os.path.exists(path) and world == 1:
         out["plain_reference"] = ensemble_plain(sizes_all, nu_all, path)

@@ -79,6 +79,19 @@ int psg_ns3d_step(psg_ns3d* h, double dt, int nsteps, int dump_last);
 int psg_ns3d_timederiv(psg_ns3d* h, double* const* out);
 /* physical fields kept by dump_last: out[0..2], n^3 doubles each, x fastest */
 int psg_ns3d_download_phys(psg_ns3d* h, double* const* out);
+/* Heun schemes: what dump_last keeps.  mode bit 0 clear (default): the
+ * physical vorticity the last step's corrector starts from (the predicted
+ * state, what the DNS returns in xir/etr/ztr, 3D_NavierStokes/src/finalise.h:
+ * 9-11); set: the physical fields of the state the last step started from (what
+ * the DNS's raw volumes and mean squares take, cuda.cu:68-93).  Bit 1: the
+ * velocity u, v, w as well (psg_ns3d_download_phys_velocity). */
+int psg_ns3d_dump_mode(psg_ns3d* h, int mode);
+int psg_ns3d_download_phys_velocity(psg_ns3d* h, double* const* out);
+/* running mean squares of the kept velocity on the device (FP64):
+ * rms = (rms count + u^2) / (count + 1), the DNS's avgVelocity
+ * (3D_NavierStokes/src/kernels.h:70-81); psg_ns3d_rms_download: out[0..2] */
+int psg_ns3d_rms_accumulate(psg_ns3d* h, double count);
+int psg_ns3d_rms_download(psg_ns3d* h, double* const* out);
 int psg_ns3d_sync(psg_ns3d* h);
 long psg_ns3d_launches(psg_ns3d* h);
 /* device state pointers and padded row length (complex words) */
@@ -164,9 +177,18 @@ int psg_batch2d_set_params(psg_batch2d* h, const double* nu, const double* dt, c
 int psg_batch2d_launch(psg_batch2d* h);
 /* time the persistent kernel at 128, 256 and 512 threads per block on the
  * current parameters (2-step runs, states restored afterwards) and keep the
- * fastest; variant 0/1/2, ms[3] per run (-1: does not fit) */
+ * fastest, then (FP32) pick each grid size's transform schedule, scalar or
+ * packed, the same way; variant 0/1/2, ms[3] per run (-1: does not fit) */
 int psg_batch2d_autotune(psg_batch2d* h, int* variant, float* ms);
 int psg_batch2d_tuning(psg_batch2d* h, int* variant, float* ms);
+/* the transform schedule psg_batch2d_autotune chose per grid size (n = 16, 32,
+ * 64, 128, 256): packed[5] = 1 where the size runs its transforms two lines per
+ * packed f32x2 instruction (FP32 batches), ms[10] the timing of the batch with
+ * that size scalar / packed (-1: size absent, or FP64) */
+int psg_batch2d_schedule(psg_batch2d* h, int* packed, float* ms);
+/* pin the schedule (packed[5] as above); PSG_ERR_UNSUPPORTED for packed sizes in
+ * an FP64 batch */
+int psg_batch2d_set_schedule(psg_batch2d* h, const int* packed);
 int psg_batch2d_sync(psg_batch2d* h);
 long psg_batch2d_launches(psg_batch2d* h);
 /* device pointer of instance i's state (complex of the batch precision, [2K+1][K+1]).

@@ -95,6 +95,23 @@ psg_stats3d* psg_stats3d_create(int n, double v2, double ampfor, int kf);
 void psg_stats3d_destroy(psg_stats3d* s);
 int psg_stats3d_add(psg_stats3d* s, double t, const double* xii, const double* eta,
                     const double* zet, FILE* stats, FILE* engy);
+/* the same, keeping the energy, dissipation and input at history index
+ * nt/nout - 1 (nt: the step index of the reference's loop, functions.h:197-200) */
+int psg_stats3d_add_at(psg_stats3d* s, int nt, int nout, double t, const double* xii,
+                       const double* eta, const double* zet, FILE* stats, FILE* engy);
+/* the number of statistics added so far (the reference's tavgCount) */
+double psg_stats3d_count(const psg_stats3d* s);
+/* the running time average of the state (XIItavg, ETAtavg, ZETtavg), reference layout */
+int psg_stats3d_mean(const psg_stats3d* s, double* xii, double* eta, double* zet);
+/* the DNS's end-of-run statistics (3D_NavierStokes/src/finalise.h:19-166): avgs
+ * (five records: time, n^3 doubles of U, V, W of the time average, mean v^2, mean
+ * u^2 - U^2), means (y, z and x averages of U, V, u variance and mean v^2 per
+ * (z, y)) and pdfs (100 bins of energy, dissipation and input); uvw: the
+ * physical velocity of psg_stats3d_mean's state, ms: the running mean squares
+ * of the physical velocity (psg_ns3d_rms_download); any FILE may be NULL */
+int psg_stats3d_finish(psg_stats3d* s, int nstop, int nout, double time,
+                       const double* const* uvw, const double* const* ms, FILE* avgs,
+                       FILE* means, FILE* pdfs);
 
 #ifdef __cplusplus
 }

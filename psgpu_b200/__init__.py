@@ -64,6 +64,10 @@ def lib():
     L.psg_ns3d_step.argtypes = [vp, d, i, i]
     L.psg_ns3d_timederiv.argtypes = [vp, pp]
     L.psg_ns3d_download_phys.argtypes = [vp, pp]
+    L.psg_ns3d_dump_mode.argtypes = [vp, i]
+    L.psg_ns3d_download_phys_velocity.argtypes = [vp, pp]
+    L.psg_ns3d_rms_accumulate.argtypes = [vp, C.c_double]
+    L.psg_ns3d_rms_download.argtypes = [vp, pp]
     L.psg_ns3d_sync.argtypes = [vp]
     L.psg_ns3d_launches.argtypes = [vp]
     L.psg_ns3d_launches.restype = C.c_long
@@ -96,6 +100,8 @@ def _declare_2d(L):
     L.psg_batch2d_launch.argtypes = [vp]
     L.psg_batch2d_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
     L.psg_batch2d_tuning.argtypes = [vp, ip, C.POINTER(C.c_float)]
+    L.psg_batch2d_schedule.argtypes = [vp, ip, C.POINTER(C.c_float)]
+    L.psg_batch2d_set_schedule.argtypes = [vp, ip]
     L.psg_batch2d_sync.argtypes = [vp]
     L.psg_batch2d_launches.argtypes = [vp]
     L.psg_batch2d_launches.restype = C.c_long
@@ -216,6 +222,28 @@ class NS3D:
         n = self.n
         out = [np.zeros(n * n * n) for _ in range(3)]
         _check(lib().psg_ns3d_download_phys(self._h, _ptrs(out)))
+        return np.stack([o.reshape(n, n, n) for o in out])
+
+    def dump_mode(self, start_of_step: bool = False, velocity: bool = False):
+        """Heun schemes: what step(..., dump_last=True) keeps: the physical
+        vorticity of the predicted state (default) or of the state the step
+        starts from, and optionally the velocity too (physical_velocity)."""
+        _check(lib().psg_ns3d_dump_mode(self._h, int(start_of_step) | (2 * int(velocity))))
+
+    def physical_velocity(self):
+        n = self.n
+        out = [np.zeros(n * n * n) for _ in range(3)]
+        _check(lib().psg_ns3d_download_phys_velocity(self._h, _ptrs(out)))
+        return np.stack([o.reshape(n, n, n) for o in out])
+
+    def rms_accumulate(self, count: float):
+        """mean squares of the kept velocity: ms = (ms count + u^2) / (count + 1)"""
+        _check(lib().psg_ns3d_rms_accumulate(self._h, float(count)))
+
+    def rms(self):
+        n = self.n
+        out = [np.zeros(n * n * n) for _ in range(3)]
+        _check(lib().psg_ns3d_rms_download(self._h, _ptrs(out)))
         return np.stack([o.reshape(n, n, n) for o in out])
 
     def sync(self):
@@ -370,6 +398,21 @@ class Batch2D:
         ms = (C.c_float * 3)()
         _check(lib().psg_batch2d_autotune(self._h, C.byref(v), ms))
         return v.value, list(ms)
+
+    def schedule(self):
+        """transform schedule per grid size {16, 32, 64, 128, 256}: (packed or
+        not, (ms scalar, ms packed) of the batch); set by autotune()"""
+        pk = (C.c_int * 5)()
+        ms = (C.c_float * 10)()
+        _check(lib().psg_batch2d_schedule(self._h, pk, ms))
+        return {16 << q: (bool(pk[q]), (ms[2 * q], ms[2 * q + 1])) for q in range(5)}
+
+    def set_schedule(self, packed):
+        """pin the transform schedule: packed = a set of grid sizes (or a dict
+        size -> bool) that run packed f32x2 transforms"""
+        sel = {k for k, v in packed.items() if v} if isinstance(packed, dict) else set(packed)
+        pk = (C.c_int * 5)(*[int((16 << q) in sel) for q in range(5)])
+        _check(lib().psg_batch2d_set_schedule(self._h, pk))
 
     def sync(self):
         _check(lib().psg_batch2d_sync(self._h))

@@ -18,12 +18,28 @@ namespace psg {
 template <typename T>
 struct Twiddles2D {
   const cpx<T>* t[5];  // n = 16, 32, 64, 128, 256
+  int pk = 0;          // bit q: size class q runs the packed transforms (FP32)
 };
+
+template <typename T, int NN, bool HASPK>
+__device__ __forceinline__ void rhs2d_run(const Inst2D<T>& I, const cpx<T>* tw, cpx<T>* smem,
+                                          bool pk) {
+  if constexpr (sizeof(T) == 4 && HASPK) {
+    if (pk) {
+      Rhs2D<T, NN, 1>::run(I, tw, smem);
+      return;
+    }
+  }
+  Rhs2D<T, NN>::run(I, tw, smem);
+}
 
 // block sizes of the persistent kernel the autotuner chooses from
 constexpr int kBlock2D[3] = {128, 256, 512};
 
-template <typename T, int NT>
+// HASPK: the packed transform schedules are compiled in (a schedule with no
+// packed size class launches the build without them, whose registers are
+// those of the scalar transforms alone)
+template <typename T, int NT, bool HASPK = false>
 __global__ void __launch_bounds__(NT)
 ns2d_persistent(const Inst2D<T>* __restrict__ insts, int ninst, int* __restrict__ next,
                 Twiddles2D<T> tws) {
@@ -38,11 +54,11 @@ ns2d_persistent(const Inst2D<T>* __restrict__ insts, int ninst, int* __restrict_
     if (i >= ninst) break;
     const Inst2D<T> I = insts[i];
     switch (I.n) {
-      case 16: Rhs2D<T, 16>::run(I, tws.t[0], smem); break;
-      case 32: Rhs2D<T, 32>::run(I, tws.t[1], smem); break;
-      case 64: Rhs2D<T, 64>::run(I, tws.t[2], smem); break;
-      case 128: Rhs2D<T, 128>::run(I, tws.t[3], smem); break;
-      default: Rhs2D<T, 256>::run(I, tws.t[4], smem); break;
+      case 16: rhs2d_run<T, 16, HASPK>(I, tws.t[0], smem, tws.pk & 1); break;
+      case 32: rhs2d_run<T, 32, HASPK>(I, tws.t[1], smem, tws.pk & 2); break;
+      case 64: rhs2d_run<T, 64, HASPK>(I, tws.t[2], smem, tws.pk & 4); break;
+      case 128: rhs2d_run<T, 128, HASPK>(I, tws.t[3], smem, tws.pk & 8); break;
+      default: rhs2d_run<T, 256, HASPK>(I, tws.t[4], smem, tws.pk & 16); break;
     }
   }
 }
@@ -80,6 +96,8 @@ struct Batch2DBase {
   virtual int launch() = 0;
   virtual int autotune(int* variant, float* ms) = 0;
   virtual int tuning(int* variant, float* ms) const = 0;
+  virtual int schedule(int* pk, float* ms) const = 0;
+  virtual int set_schedule(const int* pk) = 0;
   virtual int sync() = 0;
   virtual long launch_count() const = 0;
   virtual void set_stream(cudaStream_t s) = 0;
@@ -103,8 +121,15 @@ struct Batch2D final : Batch2DBase {
   std::vector<int> order;     // instances sorted by cost, largest first
   size_t smem_v[3] = {0, 0, 0};  // dynamic shared memory per block-size variant
   int grid_v[3] = {0, 0, 0};     // resident blocks per variant (0: does not fit)
+  int grid_pk[3] = {0, 0, 0};    // the same for the build with packed schedules
   int variant = 1;               // 256 threads unless the autotuner picks another
   float tune_ms[3] = {-1.f, -1.f, -1.f};
+  // transform schedule per size class (n = 16 .. 256): bit q packed f32x2
+  // transforms (FP32), chosen by the autotuner; sched_ms[q][0 / 1] the timing of
+  // the batch with class q scalar / packed (-1: class absent or not timed)
+  int pk_mask = 0;
+  float sched_ms[5][2] = {{-1.f, -1.f}, {-1.f, -1.f}, {-1.f, -1.f}, {-1.f, -1.f}, {-1.f, -1.f}};
+  int gexec_pk = -1;
   long state_words = 0;          // states (+ carried errors) of all instances
   bool params_set = false;
   // the persistent launch as a CUDA graph: reset the work counter, launch
@@ -192,6 +217,14 @@ struct Batch2D final : Batch2DBase {
       int per_sm = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kBlock2D[v], smem_v[v]);
       grid_v[v] = std::max(0, std::min(ninst, nsm * per_sm));
+      grid_pk[v] = 0;
+      if constexpr (sizeof(T) == 4) {
+        const void* kp = kernel_pk(v);
+        PSG_CUDA_TRY(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_v[v]));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, kBlock2D[v], smem_v[v]);
+        grid_pk[v] = std::max(0, std::min(ninst, nsm * per_sm));
+      }
     }
     if (!grid_v[variant]) {
       variant = -1;
@@ -213,16 +246,34 @@ struct Batch2D final : Batch2DBase {
       default: return (const void*)ns2d_persistent<T, 512>;
     }
   }
+  static const void* kernel_pk(int v) {
+    switch (v) {
+      case 0: return (const void*)ns2d_persistent<T, 128, true>;
+      case 1: return (const void*)ns2d_persistent<T, 256, true>;
+      default: return (const void*)ns2d_persistent<T, 512, true>;
+    }
+  }
 
   Twiddles2D<T> twiddles() const {
     Twiddles2D<T> tws;
     long o = 0;
     for (int q = 0, n = 16; q < 5; ++q, n *= 2) { tws.t[q] = twp + o; o += 2 * n; }
+    tws.pk = pk_mask;
     return tws;
   }
 
   void launch_kernel(int v, cudaStream_t st) {
     const Twiddles2D<T> tws = twiddles();
+    if constexpr (sizeof(T) == 4) {
+      if (tws.pk) {
+      switch (v) {
+        case 0: ns2d_persistent<T, 128, true><<<grid_pk[0], 128, smem_v[0], st>>>(d_insts, ninst, d_next, tws); break;
+        case 1: ns2d_persistent<T, 256, true><<<grid_pk[1], 256, smem_v[1], st>>>(d_insts, ninst, d_next, tws); break;
+        default: ns2d_persistent<T, 512, true><<<grid_pk[2], 512, smem_v[2], st>>>(d_insts, ninst, d_next, tws); break;
+      }
+      return;
+      }
+    }
     switch (v) {
       case 0: ns2d_persistent<T, 128><<<grid_v[0], 128, smem_v[0], st>>>(d_insts, ninst, d_next, tws); break;
       case 1: ns2d_persistent<T, 256><<<grid_v[1], 256, smem_v[1], st>>>(d_insts, ninst, d_next, tws); break;
@@ -232,7 +283,7 @@ struct Batch2D final : Batch2DBase {
 
   // (re)build the graph of one persistent launch for the current variant
   int build_graph() {
-    if (gexec && gexec_variant == variant) return PSG_OK;
+    if (gexec && gexec_variant == variant && gexec_pk == pk_mask) return PSG_OK;
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
     cudaGraph_t graph = nullptr;
     PSG_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
@@ -244,6 +295,7 @@ struct Batch2D final : Batch2DBase {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) { psg_set_error("graph instantiate: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
     gexec_variant = variant;
+    gexec_pk = pk_mask;
     return PSG_OK;
   }
 
@@ -288,7 +340,9 @@ struct Batch2D final : Batch2DBase {
 
   // time every block size on the current parameters (3 timed launches of a
   // 2-step copy of the run after one warm-up), restoring the states after
-  // each, and keep the fastest
+  // each, and keep the fastest; then, at that block size and in FP32, the
+  // transform schedule of each size class present (scalar or packed f32x2
+  // transforms), one class at a time, keeping the faster
   int autotune(int* v_out, float* ms) override {
     if (!params_set) { psg_set_error("2D batch: parameters not set"); return PSG_ERR_STATE; }
     std::vector<Inst2D<T>> h(hparams), shortp(hparams);
@@ -301,11 +355,8 @@ struct Batch2D final : Batch2DBase {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    float best = 1e30f;
-    int pick = variant;
-    for (int v = 0; v < 3; ++v) {
-      tune_ms[v] = -1.f;
-      if (!grid_v[v]) continue;
+    // ms per launch of the short run with block-size variant v and the current schedule
+    auto time_v = [&](int v, float* out) -> int {
       cudaMemsetAsync(d_next, 0, sizeof(int), stream);
       launch_kernel(v, stream);
       cudaEventRecord(a, stream);
@@ -314,16 +365,42 @@ struct Batch2D final : Batch2DBase {
         launch_kernel(v, stream);
       }
       cudaEventRecord(b, stream);
+      launches += 4;
       cudaError_t e = cudaEventSynchronize(b);
-      if (e != cudaSuccess) { cudaFree(save); psg_set_error("autotune: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
+      if (e != cudaSuccess) { psg_set_error("autotune: %s", cudaGetErrorString(e)); return PSG_ERR_CUDA; }
       float t = 0.f;
       cudaEventElapsedTime(&t, a, b);
-      tune_ms[v] = t / 3.f;
-      if (tune_ms[v] < best) { best = tune_ms[v]; pick = v; }
+      *out = t / 3.f;
+      return PSG_OK;
+    };
+    int rc = PSG_OK;
+    float best = 1e30f;
+    int pick = variant;
+    for (int v = 0; v < 3 && !rc; ++v) {
+      tune_ms[v] = -1.f;
+      if (!grid_v[v]) continue;
+      rc = time_v(v, &tune_ms[v]);
+      if (!rc && tune_ms[v] < best) { best = tune_ms[v]; pick = v; }
     }
-    launches += 4 * 3;
+    for (int q = 0; q < 5; ++q) sched_ms[q][0] = sched_ms[q][1] = -1.f;
+    if (sizeof(T) == 4) {
+      int present = 0;
+      for (int n : sizes)
+        for (int q = 0; q < 5; ++q)
+          if (n == (16 << q)) present |= 1 << q;
+      for (int q = 0; q < 5 && !rc && grid_pk[pick] > 0; ++q) {
+        if (!(present & (1 << q))) continue;
+        for (int p = 0; p < 2 && !rc; ++p) {
+          pk_mask = p ? (pk_mask | (1 << q)) : (pk_mask & ~(1 << q));
+          rc = time_v(pick, &sched_ms[q][p]);
+        }
+        if (!rc && sched_ms[q][1] >= 0.f && sched_ms[q][1] < sched_ms[q][0]) pk_mask |= 1 << q;
+        else pk_mask &= ~(1 << q);
+      }
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (rc) { cudaFree(save); return rc; }
     PSG_CUDA_TRY(cudaMemcpyAsync(pool, save, sizeof(cpx<T>) * state_words, cudaMemcpyDeviceToDevice, stream));
     PSG_CUDA_TRY(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst2D<T>) * ninst,
                                  cudaMemcpyHostToDevice, stream));
@@ -332,6 +409,26 @@ struct Batch2D final : Batch2DBase {
     variant = pick;
     if (v_out) *v_out = variant;
     if (ms) for (int v = 0; v < 3; ++v) ms[v] = tune_ms[v];
+    return PSG_OK;
+  }
+
+  int set_schedule(const int* pk) override {
+    int m = 0;
+    for (int q = 0; q < 5; ++q)
+      if (pk[q]) m |= 1 << q;
+    if (m && (sizeof(T) != 4 || !grid_pk[variant])) {
+      psg_set_error("packed transforms need an FP32 batch whose packed build fits");
+      return PSG_ERR_UNSUPPORTED;
+    }
+    pk_mask = m;
+    return PSG_OK;
+  }
+
+  int schedule(int* pk, float* ms) const override {
+    for (int q = 0; q < 5; ++q) {
+      if (pk) pk[q] = (pk_mask >> q) & 1;
+      if (ms) { ms[2 * q] = sched_ms[q][0]; ms[2 * q + 1] = sched_ms[q][1]; }
+    }
     return PSG_OK;
   }
 
@@ -442,6 +539,20 @@ extern "C" int psg_batch2d_tuning(psg_batch2d* h, int* variant, float* ms) {
   PSG_B2(h);
   return h->b->tuning(variant, ms);
 }
+
+// the transform schedule the autotuner chose per size class
+extern "C" int psg_batch2d_schedule(psg_batch2d* h, int* packed, float* ms) {
+  PSG_B2(h);
+  return h->b->schedule(packed, ms);
+}
+
+// pin the transform schedule per grid size (packed[5], as psg_batch2d_schedule)
+extern "C" int psg_batch2d_set_schedule(psg_batch2d* h, const int* packed) {
+  PSG_B2(h);
+  if (!packed) { psg_set_error("bad arguments"); return PSG_ERR_ARG; }
+  return h->b->set_schedule(packed);
+}
+
 extern "C" int psg_batch2d_sync(psg_batch2d* h) {
   PSG_B2(h);
   return h->b->sync();

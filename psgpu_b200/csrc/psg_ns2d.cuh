@@ -18,6 +18,7 @@
 
 #include "psg_common.cuh"
 #include "psg_fft.cuh"
+#include "psg_fft2.cuh"
 
 namespace psg {
 
@@ -77,16 +78,54 @@ __device__ __forceinline__ cpx<T> field2(const cpx<T>* __restrict__ Z0, int f, i
   return r;
 }
 
-template <typename T, int N>
+// PK (FP32 only): the transforms of two lines at once as packed f32x2 ones
+// (psg_fft2.cuh): phase 1 two columns per lane group, phase 2 the inverse rows
+// of (w + i u) and v together, phase 3 the two product columns together.  The
+// batch's autotuner picks PK per grid size (Batch2D::autotune).
+template <typename T, int N, int PK = 0>
 struct Rhs2D {
+  static_assert(PK == 0 || sizeof(T) == 4, "packed transforms are FP32");
   using FI = LineFFT<N, +1, T>;
   using FO = LineFFT<N, -1, T>;
   using FX = LineFFT<N, -1, T, true>;  // forward transform of phase 2: consumes FI's output
   static constexpr int G = FI::G, E = FI::E;
   static constexpr int K = N / 3, X = K + 1, Y = 2 * K + 1;
 
+  // phase 1, packed: columns 2p and 2p + 1 of the 3X (three fields) together
+  static __device__ void phase1_pk(const Inst2D<T>& I, const cpx<T>* tw, cpx<T>* ex) {
+    const int gid = threadIdx.x / G, gi = threadIdx.x % G, ng = blockDim.x / G;
+    constexpr int NP = (3 * X + 1) / 2;
+    for (int base = 0; base < NP; base += ng) {
+      const int p = base + gid;
+      const int c0 = 2 * p, c1 = 2 * p + 1;
+      const bool l0 = c0 < 3 * X, l1 = c1 < 3 * X;
+      const int f0 = l0 ? c0 / X : 0, x0 = l0 ? c0 % X : 0;
+      const int f1 = l1 ? c1 / X : 0, x1 = l1 ? c1 % X : 0;
+      Pk v[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int iky = row_to_box2(FI::in_index(gi, e), K, N);
+        const cpx<T> a = (l0 && iky >= 0) ? field2(I.Z0, f0, x0, iky, K, X) : czero<T>();
+        const cpx<T> b = (l1 && iky >= 0) ? field2(I.Z0, f1, x1, iky, K, X) : czero<T>();
+        v[e] = Pk{make_float2(a.x, b.x), make_float2(a.y, b.y)};
+      }
+      LineFFT2<N, +1>::run(v, gi, tw, reinterpret_cast<float2*>(ex), WarpSync());
+      if (l0) {
+        cpx<T>* dst = I.work + (long)f0 * N * X + x0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) dst[FI::out_index(gi, e) * X] = cpx<T>{v[e].re.x, v[e].im.x};
+      }
+      if (l1) {
+        cpx<T>* dst = I.work + (long)f1 * N * X + x1;
+#pragma unroll
+        for (int e = 0; e < E; ++e) dst[FI::out_index(gi, e) * X] = cpx<T>{v[e].re.y, v[e].im.y};
+      }
+    }
+  }
+
   // phase 1: y-inverse of the three fields, written to work[f][y][kx]
   static __device__ void phase1(const Inst2D<T>& I, const cpx<T>* tw, cpx<T>* ex) {
+    if constexpr (PK != 0) { phase1_pk(I, tw, ex); return; }
     const int gid = threadIdx.x / G, gi = threadIdx.x % G, ng = blockDim.x / G;
     for (int base = 0; base < 3 * X; base += ng) {
       const int col = base + gid;
@@ -118,34 +157,65 @@ struct Rhs2D {
       const cpx<T>* ru = rw + (long)N * X;
       const cpx<T>* rv = rw + 2L * N * X;
       cpx<T> v[E];
-      // (w, u) packed: w + i u
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const int r = FI::in_index(gi, e);
-        cpx<T> z = czero<T>();
-        if (live) {
-          if (r == 0) z = cpx<T>{rw[0].x, ru[0].x};
-          else if (r <= K) { const cpx<T> a = rw[r], b = ru[r]; z = cpx<T>{a.x - b.y, a.y + b.x}; }
-          else if (r >= N - K) { const cpx<T> a = rw[N - r], b = ru[N - r]; z = cpx<T>{a.x + b.y, -a.y + b.x}; }
-        }
-        v[e] = z;
-      }
-      FI::run(v, gi, tw, ex, WarpSync());
       T w[E], u[E];
+      if constexpr (PK != 0) {
+        // (w + i u) and v (its Hermitian line) through one packed transform
+        Pk pv[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) { w[e] = v[e].x; u[e] = v[e].y; }
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const int r = FI::in_index(gi, e);
-        cpx<T> z = czero<T>();
-        if (live) {
-          if (r == 0) z = cpx<T>{rv[0].x, (T)0};
-          else if (r <= K) z = rv[r];
-          else if (r >= N - K) { const cpx<T> a = rv[N - r]; z = cpx<T>{a.x, -a.y}; }
+        for (int e = 0; e < E; ++e) {
+          const int r = FI::in_index(gi, e);
+          cpx<T> za = czero<T>(), zb = czero<T>();
+          if (live) {
+            if (r == 0) {
+              za = cpx<T>{rw[0].x, ru[0].x};
+              zb = cpx<T>{rv[0].x, (T)0};
+            } else if (r <= K) {
+              const cpx<T> a = rw[r], b = ru[r];
+              za = cpx<T>{a.x - b.y, a.y + b.x};
+              zb = rv[r];
+            } else if (r >= N - K) {
+              const cpx<T> a = rw[N - r], b = ru[N - r], c = rv[N - r];
+              za = cpx<T>{a.x + b.y, -a.y + b.x};
+              zb = cpx<T>{c.x, -c.y};
+            }
+          }
+          pv[e] = Pk{make_float2(za.x, zb.x), make_float2(za.y, zb.y)};
         }
-        v[e] = z;
+        LineFFT2<N, +1>::run(pv, gi, tw, reinterpret_cast<float2*>(ex), WarpSync());
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          w[e] = pv[e].re.x; u[e] = pv[e].im.x;
+          v[e] = cpx<T>{pv[e].re.y, pv[e].im.y};
+        }
+      } else {
+        // (w, u) packed: w + i u
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int r = FI::in_index(gi, e);
+          cpx<T> z = czero<T>();
+          if (live) {
+            if (r == 0) z = cpx<T>{rw[0].x, ru[0].x};
+            else if (r <= K) { const cpx<T> a = rw[r], b = ru[r]; z = cpx<T>{a.x - b.y, a.y + b.x}; }
+            else if (r >= N - K) { const cpx<T> a = rw[N - r], b = ru[N - r]; z = cpx<T>{a.x + b.y, -a.y + b.x}; }
+          }
+          v[e] = z;
+        }
+        FI::run(v, gi, tw, ex, WarpSync());
+#pragma unroll
+        for (int e = 0; e < E; ++e) { w[e] = v[e].x; u[e] = v[e].y; }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int r = FI::in_index(gi, e);
+          cpx<T> z = czero<T>();
+          if (live) {
+            if (r == 0) z = cpx<T>{rv[0].x, (T)0};
+            else if (r <= K) z = rv[r];
+            else if (r >= N - K) { const cpx<T> a = rv[N - r]; z = cpx<T>{a.x, -a.y}; }
+          }
+          v[e] = z;
+        }
+        FI::run(v, gi, tw, ex, WarpSync());
       }
-      FI::run(v, gi, tw, ex, WarpSync());
       // products (multReal, 2D_NavierStokes/src_RK4/kernels.h:187-201): p = v w, q = u w
 #pragma unroll
       for (int e = 0; e < E; ++e) v[e] = cpx<T>{v[e].x * w[e] * scale, u[e] * w[e] * scale};
@@ -178,13 +248,30 @@ struct Rhs2D {
       const bool live = ikx < X;
       cpx<T> a[E], b[E];
       const cpx<T>* src = I.work + (live ? ikx : 0);
+      if constexpr (PK != 0) {
+        // both product columns through one packed transform
+        Pk pv[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) a[e] = live ? src[FO::in_index(gi, e) * X] : czero<T>();
-      FO::run(a, gi, tw, ex, WarpSync());
+        for (int e = 0; e < E; ++e) {
+          const cpx<T> x = live ? src[FO::in_index(gi, e) * X] : czero<T>();
+          const cpx<T> y = live ? src[(long)N * X + FO::in_index(gi, e) * X] : czero<T>();
+          pv[e] = Pk{make_float2(x.x, y.x), make_float2(x.y, y.y)};
+        }
+        LineFFT2<N, -1>::run(pv, gi, tw, reinterpret_cast<float2*>(ex), WarpSync());
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        b[e] = live ? src[(long)N * X + FO::in_index(gi, e) * X] : czero<T>();
-      FO::run(b, gi, tw, ex, WarpSync());
+        for (int e = 0; e < E; ++e) {
+          a[e] = cpx<T>{pv[e].re.x, pv[e].im.x};
+          b[e] = cpx<T>{pv[e].re.y, pv[e].im.y};
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) a[e] = live ? src[FO::in_index(gi, e) * X] : czero<T>();
+        FO::run(a, gi, tw, ex, WarpSync());
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          b[e] = live ? src[(long)N * X + FO::in_index(gi, e) * X] : czero<T>();
+        FO::run(b, gi, tw, ex, WarpSync());
+      }
       if (!live) continue;
       const T dt = I.dt;
 #pragma unroll

@@ -83,6 +83,10 @@ struct Engine3DBase {
   virtual int steps(double dt, int nsteps, int dump_last) = 0;
   virtual int timederiv(double* const* out) = 0;
   virtual int phys(double* const* out) = 0;
+  virtual int set_dump_mode(int mode) = 0;
+  virtual int phys_velocity(double* const* out) = 0;
+  virtual int rms_accumulate(double count) = 0;
+  virtual int rms_download(double* const* out) = 0;
   virtual int layout(int* xp, void** comps) = 0;
   virtual long launch_count() const = 0;
   virtual int sync() = 0;  // wait for the stream and check the device error flag

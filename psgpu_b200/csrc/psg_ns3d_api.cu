@@ -87,6 +87,29 @@ extern "C" int psg_ns3d_download_phys(psg_ns3d* h, double* const* out) {
   return h->e->phys(out);
 }
 
+extern "C" int psg_ns3d_dump_mode(psg_ns3d* h, int mode) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->set_dump_mode(mode);
+}
+
+extern "C" int psg_ns3d_download_phys_velocity(psg_ns3d* h, double* const* out) {
+  PSG_CHECK_HANDLE(h);
+  if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  return h->e->phys_velocity(out);
+}
+
+extern "C" int psg_ns3d_rms_accumulate(psg_ns3d* h, double count) {
+  PSG_CHECK_HANDLE(h);
+  if (count < 0) { psg_set_error("count must be >= 0"); return PSG_ERR_ARG; }
+  return h->e->rms_accumulate(count);
+}
+
+extern "C" int psg_ns3d_rms_download(psg_ns3d* h, double* const* out) {
+  PSG_CHECK_HANDLE(h);
+  if (!out) { psg_set_error("null output"); return PSG_ERR_ARG; }
+  return h->e->rms_download(out);
+}
+
 extern "C" int psg_ns3d_sync(psg_ns3d* h) {
   PSG_CHECK_HANDLE(h);
   return h->e->sync();

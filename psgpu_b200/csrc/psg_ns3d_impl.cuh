@@ -487,7 +487,7 @@ __global__ void __launch_bounds__(L * LineFFT<N, 1, T>::G,
                                   (sizeof(T) == 4 && NF == 9 && L * LineFFT<N, 1, T>::G <= 128) ? 3 : 0)
 pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
        const cpx<T>* __restrict__ tw, T scale, T* __restrict__ dump, int* status, int nwt,
-       unsigned long long* __restrict__ umax) {
+       unsigned long long* __restrict__ umax, int dnf) {
   static_assert(PK == 0 || (sizeof(T) == 4 && NF != 7), "packed x-pass: FP32 forward fields");
   using R = RowOps<T, N>;
   constexpr int G = R::G, E = R::E;
@@ -606,6 +606,11 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
             dump[base + x] = xi[e];
             dump[nr + base + x] = et[e];
             dump[2 * nr + base + x] = zt[e];
+            if (dnf == 6) {
+              dump[3 * nr + base + x] = u[e];
+              dump[4 * nr + base + x] = v[e];
+              dump[5 * nr + base + x] = w[e];
+            }
           }
         }
         T n1[E], n2[E], n3[E];
@@ -646,6 +651,11 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
         dump[base + x] = xi[e];
         dump[nr + base + x] = et[e];
         dump[2 * nr + base + x] = zt[e];
+        if (dnf == 6) {  // the velocity too (the DNS's mean-square statistics)
+          dump[3 * nr + base + x] = u[e];
+          dump[4 * nr + base + x] = v[e];
+          dump[5 * nr + base + x] = w[e];
+        }
       }
     }
     T n1[E], n2[E], n3[E];
@@ -1215,6 +1225,15 @@ __global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* 
   }
 }
 
+// running mean squares (the DNS's avgVelocity, 3D_NavierStokes/src/kernels.h:70-81)
+template <typename T>
+__global__ void rms_acc(const T* __restrict__ u, double* __restrict__ rms, long n, double count) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double v = (double)u[i];
+    rms[i] = (rms[i] * count + v * v) / (count + 1.0);
+  }
+}
+
 template <typename T>
 __global__ void real_to_double(const T* __restrict__ src, double* __restrict__ dst, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
@@ -1512,7 +1531,12 @@ struct Engine3D final : Engine3DBase {
   int first_rhs = 1;     // mask velocity on the first evaluation after an upload
   cpx<T>* pool = nullptr;
   cpx<T>* tw = nullptr;
-  T* dump = nullptr;     // physical vorticity of the last predictor (Heun schemes)
+  T* dump = nullptr;     // physical fields of the last step (Heun schemes)
+  // dump_mode bit 0: the fields the step starts from (the predictor's input)
+  // instead of the predicted state's (the corrector's input); bit 1: the
+  // velocity beside the vorticity (six fields)
+  int dump_mode = 0;
+  double* d_rms = nullptr;  // running mean squares of u, v, w (FP64, 3 n^3)
   Regs<T> R{};
   cpx<T>* B1 = nullptr;
   cpx<T>* B2 = nullptr;
@@ -1706,6 +1730,8 @@ struct Engine3D final : Engine3DBase {
     if (d_energ) cudaFree(d_energ);
     if (d_umax) cudaFree(d_umax);
     if (d_flux) cudaFree(d_flux);
+    if (d_rms) cudaFree(d_rms);
+    d_rms = nullptr;
     if (lin) cudaFree(lin);
     lin = nullptr;
     d_energ = nullptr; d_umax = nullptr; d_flux = nullptr;
@@ -1805,7 +1831,8 @@ struct Engine3D final : Engine3DBase {
     int* st = d_status;
     int nw = nwt;
     unsigned long long* u = um;
-    void* args[] = {&gg, &in, &out, &twp, &scale, &dp, &st, &nw, &u};
+    int dnf = (dp && (dump_mode & 2)) ? 6 : 3;
+    void* args[] = {&gg, &in, &out, &twp, &scale, &dp, &st, &nw, &u, &dnf};
     PSG_CUDA_TRY(cudaLaunchKernel(k, dim3(grid), dim3(th), args, sm, stream));
     return PSG_OK;
   }
@@ -1960,8 +1987,8 @@ struct Engine3D final : Engine3DBase {
     lin_dx = false;
     int rc;
     if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) {
-      if ((rc = rhs(STAGE_HEUN_PRED))) return rc;
-      return rhs(STAGE_HEUN_CORR, want_dump);
+      if ((rc = rhs(STAGE_HEUN_PRED, want_dump && (dump_mode & 1)))) return rc;
+      return rhs(STAGE_HEUN_CORR, want_dump && !(dump_mode & 1));
     }
     if ((rc = rhs(STAGE_RK1))) return rc;
     if ((rc = rhs(STAGE_RK2))) return rc;
@@ -2429,6 +2456,54 @@ struct Engine3D final : Engine3DBase {
   int phys(double* const* out) override {
     if (!dump) { psg_set_error("scheme keeps no physical fields"); return PSG_ERR_STATE; }
     return download_phys(out);
+  }
+  int set_dump_mode(int mode) override {
+    if (!dump) { psg_set_error("scheme keeps no physical fields"); return PSG_ERR_STATE; }
+    if (mode < 0 || mode > 3) { psg_set_error("dump mode %d unknown", mode); return PSG_ERR_ARG; }
+    if ((mode & 2) && !(dump_mode & 2)) {
+      cudaFree(dump);
+      dump = nullptr;
+      PSG_CUDA_TRY(cudaMalloc(&dump, sizeof(T) * 6L * g.n * g.n * g.n));
+    }
+    dump_mode = mode;
+    return PSG_OK;
+  }
+  int phys_velocity(double* const* out) override {
+    if (!dump || !(dump_mode & 2)) {
+      psg_set_error("the velocity is kept in dump mode 2 or 3");
+      return PSG_ERR_STATE;
+    }
+    const long nr = (long)g.n * g.n * g.n;
+    T* keep = dump;
+    dump = keep + 3 * nr;
+    const int rc = download_phys(out);
+    dump = keep;
+    return rc;
+  }
+  // running mean squares of the kept velocity: rms = (rms count + u^2)/(count + 1)
+  int rms_accumulate(double count) override {
+    if (!dump || !(dump_mode & 2)) {
+      psg_set_error("the velocity is kept in dump mode 2 or 3");
+      return PSG_ERR_STATE;
+    }
+    const long nr = (long)g.n * g.n * g.n;
+    if (!d_rms) {
+      PSG_CUDA_TRY(cudaMalloc(&d_rms, sizeof(double) * 3 * nr));
+      PSG_CUDA_TRY(cudaMemsetAsync(d_rms, 0, sizeof(double) * 3 * nr, stream));
+    }
+    rms_acc<T><<<592, 256, 0, stream>>>(dump + 3 * nr, d_rms, 3 * nr, count);
+    ++launches;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+  int rms_download(double* const* out) override {
+    if (!d_rms) { psg_set_error("no mean squares accumulated"); return PSG_ERR_STATE; }
+    const long nr = (long)g.n * g.n * g.n;
+    for (int q = 0; q < 3; ++q)
+      PSG_CUDA_TRY(cudaMemcpyAsync(out[q], d_rms + q * nr, sizeof(double) * nr,
+                                   cudaMemcpyDeviceToHost, stream));
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return check_status();
   }
   int download_from(double* const* comps, const Fields4<T>* src) {
     if (int rc = check_status()) return rc;

@@ -14,8 +14,11 @@
  * FP64 volumes JOBDIR/xii%03d.raw, eta%03d.raw, zet%03d.raw, x fastest
  * (3D_NavierStokes/src/cuda.cu:72-93), and JOBDIR/Zk.out: main.F90's header
  * record (1, IKTX, IKTY, IKTZ) followed by the final state as a type "D"
- * restart record.  The grid is compile-time in the reference
- * (global_params.F90, 128^3); here it is -n (default 128). */
+ * restart record.  With STATSFLAG = 1 it also keeps the running mean squares
+ * of the physical velocity (every NOUT steps, kernels.h:70-81) and at the end
+ * writes avgs.dat, means.dat and pdfs.dat (finalise.h:19-166).  The grid is
+ * compile-time in the reference (global_params.F90, 128^3); here it is -n
+ * (default 128). */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -82,7 +85,7 @@ int main(int argc, char** argv) {
   double* out[3] = {st[0], st[1], st[2]};
   if (psg_ns3d_upload(h, in)) FAIL("%s", psg_last_error());
 
-  FILE *fs = NULL, *fe = NULL, *fu = NULL, *fi = NULL;
+  FILE *fs = NULL, *fe = NULL, *fu = NULL, *fi = NULL, *fa = NULL, *fm = NULL, *fp = NULL;
   psg_stats3d* S = NULL;
   psg_rec3d* rec = NULL;
   if (P.rcflag == 1) {
@@ -100,36 +103,47 @@ int main(int argc, char** argv) {
     fprintf(fi, "Guess No : Start time : guess Period : guess Shift x: guess Shift y: guess Residual \n");
   }
   if (P.statsflag) {
-    snprintf(path, sizeof path, "%s/stats.dat", dir);
-    fs = fopen(path, "w");
-    snprintf(path, sizeof path, "%s/engy.dat", dir);
-    fe = fopen(path, "w");
+    /* the statistics files of init.h:114-133 */
+    static const char* names[5] = {"stats.dat", "engy.dat", "avgs.dat", "means.dat", "pdfs.dat"};
+    FILE** fl[5] = {&fs, &fe, &fa, &fm, &fp};
+    for (int k = 0; k < 5; ++k) {
+      snprintf(path, sizeof path, "%s/%s", dir, names[k]);
+      *fl[k] = fopen(path, k == 2 ? "wb" : "w");
+      if (!*fl[k]) FAIL("cannot open %s", path);
+    }
     S = psg_stats3d_create(n, P.v2, P.ampfor, P.kf);
-    if (!fs || !fe || !S) FAIL("cannot open the statistics files in %s", dir);
+    if (!S) FAIL("out of host memory");
   }
+  const long nr = (long)n * n * n;
+  /* the fields a step starts from are kept (the raw volumes and the mean
+   * squares hold those of the state before step NT, cuda.cu:68-93); the
+   * velocity too when statistics are on */
+  if (psg_ns3d_dump_mode(h, 1 | (S ? 2 : 0))) FAIL("%s", psg_last_error());
   const double t0 = now();
   int done = 0;
-  /* raw physical vorticity volumes before steps NT = 0, NOUTV, 2 NOUTV, ...:
-   * step through NT with the last predictor's physical fields kept */
-  const long nr = (long)n * n * n;
   double* vol[3] = {NULL, NULL, NULL};
   int nvol = 0;
   const int want_vol = P.noutv > 0 && P.nstop > 1;
   if (want_vol)
     for (int q = 0; q < 3; ++q)
       if (!(vol[q] = (double*)malloc(sizeof(double) * nr))) FAIL("out of host memory");
-  int next_vol = want_vol ? 0 : P.nstop;
-  /* statistics after step NT for NT = NOUT, 2 NOUT, ... (NT counted from 0) */
   int izkout = 0;
-  int nt = (S || rec) ? P.nout : P.nstop;
+  /* events at the step index NT of the reference's loop (NT = 0 .. NSTOP-1): a raw
+   * volume of the state before step NT (NT a multiple of NOUTV), the mean squares
+   * of its velocity (statistics on, NT a multiple of NOUT), then after the step
+   * the recurrence check and the statistics of the new state (NT a multiple of
+   * NOUT, NT > 0) */
+  int next_vol = want_vol ? 0 : P.nstop;
+  int next_out = (S || rec) ? 0 : P.nstop;
   for (;;) {
-    /* the next event: a volume before step next_vol, or the statistics after step nt */
-    const int upto = next_vol < nt + 1 ? next_vol + 1 : nt + 1;
-    if (upto > P.nstop) break;
-    if (upto > done && psg_ns3d_step(h, P.delt, upto - done, upto == next_vol + 1))
+    const int NT = next_vol < next_out ? next_vol : next_out;
+    if (NT >= P.nstop) break;
+    const int is_vol = NT == next_vol, is_out = NT == next_out;
+    const int want_dump = is_vol || (is_out && S);
+    if (NT + 1 > done && psg_ns3d_step(h, P.delt, NT + 1 - done, want_dump))
       FAIL("%s", psg_last_error());
-    done = upto;
-    if (done == next_vol + 1) {
+    done = NT + 1;
+    if (is_vol) {
       static const char* names[3] = {"xii", "eta", "zet"};
       if (psg_ns3d_download_phys(h, vol)) FAIL("%s", psg_last_error());
       ++nvol;
@@ -140,13 +154,15 @@ int main(int argc, char** argv) {
         fclose(fv);
       }
       next_vol += P.noutv;
-      continue;
     }
-    if (!(S || rec) || nt >= P.nstop) break;
+    if (!is_out) continue;
+    next_out += P.nout;
+    if (S && psg_ns3d_rms_accumulate(h, psg_stats3d_count(S))) FAIL("%s", psg_last_error());
+    if (NT == 0) continue;
     const double tme = done * P.delt;
     if (rec) {
       int emitted = 0;
-      if (psg_rec3d_add_engine(rec, nt, h, &emitted)) FAIL("%s", psg_last_error());
+      if (psg_rec3d_add_engine(rec, NT, h, &emitted)) FAIL("%s", psg_last_error());
       if (emitted) {
         double meta[7];
         if (psg_rec3d_guess(rec, meta, st[0], st[1], st[2])) FAIL("%s", psg_last_error());
@@ -161,9 +177,9 @@ int main(int argc, char** argv) {
     }
     if (S && !(P.statsflag == 2 && tme <= 500.0)) {
       if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
-      psg_stats3d_add(S, tme, st[0], st[1], st[2], fs, fe);
+      if (psg_stats3d_add_at(S, NT, P.nout, tme, st[0], st[1], st[2], fs, fe))
+        FAIL("%s", psg_last_error());
     }
-    nt += P.nout;
   }
   if (done < P.nstop && psg_ns3d_step(h, P.delt, P.nstop - done, 0)) FAIL("%s", psg_last_error());
   if (psg_ns3d_download(h, out)) FAIL("%s", psg_last_error());
@@ -176,6 +192,27 @@ int main(int argc, char** argv) {
   if (psg_write_state3d_header(fz, 1, n) || psg_write_state3d_record(fz, n, fin, st[0], st[1], st[2]))
     FAIL("writing %s failed", path);
   fclose(fz);
+  if (S && P.statsflag == 1 && P.nstop > 1) {
+    /* finalise.h:19-166: the statistics of the final state, then the mean
+     * profiles of the time average and the pdfs */
+    const double tend = P.nstop * P.delt;
+    if (psg_stats3d_add_at(S, P.nstop + 1, P.nout, tend, st[0], st[1], st[2], fs, fe))
+      FAIL("%s", psg_last_error());
+    double* fld[6];
+    for (int q = 0; q < 6; ++q)
+      if (!(fld[q] = (double*)malloc(sizeof(double) * nr))) FAIL("out of host memory");
+    if (psg_stats3d_mean(S, st[0], st[1], st[2]) || psg_ns3d_upload(h, in) ||
+        psg_ns3d_step(h, P.delt, 1, 1) || psg_ns3d_download_phys_velocity(h, fld) ||
+        psg_ns3d_rms_download(h, fld + 3))
+      FAIL("%s", psg_last_error());
+    if (psg_stats3d_finish(S, P.nstop, P.nout, tend, (const double* const*)fld,
+                           (const double* const*)(fld + 3), fa, fm, fp))
+      FAIL("%s", psg_last_error());
+    for (int q = 0; q < 6; ++q) free(fld[q]);
+  }
+  if (fa) fclose(fa);
+  if (fm) fclose(fm);
+  if (fp) fclose(fp);
   if (fs) fclose(fs);
   if (fe) fclose(fe);
   if (fu) fclose(fu);

@@ -14,6 +14,11 @@
 
 void psg_set_error(const char* fmt, ...);
 
+static int set_err(const char* msg) {
+  psg_set_error("%s", msg);
+  return -1;
+}
+
 /* ------------------------------------------------------------ parameters */
 
 static int next_line(FILE* f, char* buf, size_t cap) {
@@ -357,6 +362,12 @@ struct psg_stats3d {
   long nkt;
   double v2, ampfor, count;
   double* avg[3];  /* running time averages of the state (XIItavg, ...) */
+  /* histories by statistics index NT/NOUT - 1 (energy, dissipation, input),
+   * their extrema (from 0: the reference's globals start at zero, kernels.h:24)
+   * and running averages */
+  double* hist[3];
+  long nhist, index;
+  double lo[3], hi[3], mean[3];
 };
 
 psg_stats3d* psg_stats3d_create(int n, double v2, double ampfor, int kf) {
@@ -365,6 +376,7 @@ psg_stats3d* psg_stats3d_create(int n, double v2, double ampfor, int kf) {
   s->n = n; s->K = n / 3; s->X = s->K + 1; s->Y = 2 * s->K + 1; s->kf = kf;
   s->nkt = (long)s->X * s->Y * s->Y;
   s->v2 = v2; s->ampfor = ampfor;
+  s->index = -1;
   for (int q = 0; q < 3; ++q) {
     s->avg[q] = (double*)calloc(2 * s->nkt, sizeof(double));
     if (!s->avg[q]) { psg_stats3d_destroy(s); return NULL; }
@@ -374,8 +386,19 @@ psg_stats3d* psg_stats3d_create(int n, double v2, double ampfor, int kf) {
 
 void psg_stats3d_destroy(psg_stats3d* s) {
   if (!s) return;
-  for (int q = 0; q < 3; ++q) free(s->avg[q]);
+  for (int q = 0; q < 3; ++q) { free(s->avg[q]); free(s->hist[q]); }
   free(s);
+}
+
+double psg_stats3d_count(const psg_stats3d* s) { return s ? s->count : 0.0; }
+
+int psg_stats3d_mean(const psg_stats3d* s, double* xii, double* eta, double* zet) {
+  double* out[3] = {xii, eta, zet};
+  for (int q = 0; q < 3; ++q) {
+    if (!out[q]) return set_err("null output");
+    memcpy(out[q], s->avg[q], sizeof(double) * 2 * s->nkt);
+  }
+  return 0;
 }
 
 static double sq(double x) { return x * x; }
@@ -418,8 +441,114 @@ int psg_stats3d_add(psg_stats3d* s, double t, const double* xii, const double* e
   input *= s->v2 * kfy * kfy;
   diss *= s->v2 * s->v2 * 8.0 * kfy * kfy;
   dturb *= s->v2 * 16.0 * kfy * kfy;
+  const double val[3] = {energy, diss, input};
+  for (int q = 0; q < 3; ++q) {
+    s->lo[q] = val[q] < s->lo[q] ? val[q] : s->lo[q];
+    s->hi[q] = val[q] > s->hi[q] ? val[q] : s->hi[q];
+    s->mean[q] = (s->mean[q] * c + val[q]) / (c + 1.0);
+  }
+  if (s->index >= 0) {
+    if (s->index >= s->nhist) {
+      const long m = s->index + 64;
+      for (int q = 0; q < 3; ++q) {
+        double* h = (double*)realloc(s->hist[q], sizeof(double) * m);
+        if (!h) return set_err("out of host memory");
+        for (long i = s->nhist; i < m; ++i) h[i] = 0.0;
+        s->hist[q] = h;
+      }
+      s->nhist = m;
+    }
+    for (int q = 0; q < 3; ++q) s->hist[q][s->index] = val[q];
+  }
   s->count += 1.0;
   if (stats) { fprintf(stats, "%e %e %e %e %e %e \n", t, energy, eturb, diss, dturb, input); fflush(stats); }
   if (engy) { fprintf(engy, "%e %e %e %e %e %e %e \n", t, Ua, Va, Wa, XIa, ETa, ZTa); fflush(engy); }
   return 0;
+}
+
+/* the same, storing the history at index nt/nout - 1 as computeStats does
+ * (functions.h:197-200); nt: the step index NT of the reference's loop */
+int psg_stats3d_add_at(psg_stats3d* s, int nt, int nout, double t, const double* xii,
+                       const double* eta, const double* zet, FILE* stats, FILE* engy) {
+  if (nout < 1) return set_err("NOUT must be >= 1");
+  s->index = nt / nout - 1;
+  const int rc = psg_stats3d_add(s, t, xii, eta, zet, stats, engy);
+  s->index = -1;
+  return rc;
+}
+
+/* The end-of-run statistics of the DNS (3D_NavierStokes/src/finalise.h:19-166,
+ * statsFLAG = 1, NSTOP > 1), after the last psg_stats3d_add_at of the final state:
+ * uvw = the physical velocity of the time-averaged state (psg_stats3d_mean),
+ * ms = the running mean squares of the physical velocity (u^2, v^2, w^2).
+ * avgs: five records (time, n^3 doubles): U, V, W, mean v^2, mean u^2 - U^2.
+ * means: per (z, y) (z outer), y, z and the x averages of U, V, mean u^2 - U^2
+ * and mean v^2.  pdfs (when the dissipation spans more than 1e-3): 100 bins of
+ * energy, dissipation and input over the first NSTOP/NOUT histories, bin j
+ * holding the values with int((x - min)/dx) + 1 = j (a value in bin 100, the
+ * top one, falls outside the array in the reference and is not counted here).
+ * Prints the averages and extrema as the reference does. */
+int psg_stats3d_finish(psg_stats3d* s, int nstop, int nout, double time,
+                       const double* const* uvw, const double* const* ms, FILE* avgs,
+                       FILE* means, FILE* pdfs) {
+  const int n = s->n;
+  const long nr = (long)n * n * n, ny = n, nz = n, nx = n;
+  const double twopi = 8.0 * atan(1.0);
+  double* prof[4];
+  for (int q = 0; q < 4; ++q) {
+    prof[q] = (double*)calloc(ny * nz, sizeof(double));
+    if (!prof[q]) { for (int p = 0; p < q; ++p) free(prof[p]); return set_err("out of host memory"); }
+  }
+  double* uvar = (double*)malloc(sizeof(double) * nr);
+  if (!uvar) { for (int q = 0; q < 4; ++q) free(prof[q]); return set_err("out of host memory"); }
+  for (long i = 0; i < nr; ++i) uvar[i] = ms[0][i] - uvw[0][i] * uvw[0][i];
+  const double* rec[5] = {uvw[0], uvw[1], uvw[2], ms[1], uvar};
+  int rc = 0;
+  for (int r = 0; r < 5 && !rc; ++r)
+    if (avgs && (fwrite(&time, sizeof(double), 1, avgs) != 1 ||
+                 fwrite(rec[r], sizeof(double), nr, avgs) != (size_t)nr))
+      rc = set_err("writing avgs failed");
+  /* x averages: U, V, u variance, v mean square */
+  const double* src[4] = {uvw[0], uvw[1], uvar, ms[1]};
+  for (long iz = 0; iz < nz && !rc; ++iz)
+    for (long iy = 0; iy < ny; ++iy) {
+      const long ik = iz * ny + iy;
+      for (int q = 0; q < 4; ++q) {
+        double a = 0.0;
+        for (long ix = 0; ix < nx; ++ix) a += src[q][(ny * iz + iy) * nx + ix];
+        prof[q][ik] = a / (double)nx;
+      }
+      if (means)
+        fprintf(means, "%.15e %.15e %.15e %.15e %.15e %.15e \n", iy * twopi / (double)ny,
+                iz * twopi / (double)nz, prof[0][ik], prof[1][ik], prof[2][ik], prof[3][ik]);
+    }
+  printf("AVERAGE STATS *****\n");
+  printf("energy = %e,  eturb = %e \n", s->mean[0], 0.0);
+  printf("dissipation = %e,  dturb = %e \n", s->mean[1], 0.0);
+  printf("input E = %e \n", s->mean[2]);
+  printf("max/min dissipation %e, %e \n ", s->hi[1], s->lo[1]);
+  printf("max/min energy %e, %e \n", s->hi[0], s->lo[0]);
+  printf("max/min input %e, %e \n", s->hi[2], s->lo[2]);
+  const long nstats = nstop / nout + 1;
+  if (!rc && s->hi[1] - s->lo[1] > 0.001) {
+    enum { NBIN = 100 };
+    const double correct = 1.0000001;
+    long cnt[3][NBIN + 1] = {{0}};
+    double dx[3];
+    for (int q = 0; q < 3; ++q) dx[q] = (s->hi[q] * correct - s->lo[q]) / (double)NBIN;
+    for (long t = 0; t < nstats - 1; ++t)
+      for (int q = 0; q < 3; ++q) {
+        const double x = t < s->nhist ? s->hist[q][t] : 0.0;
+        const long j = (long)((x - s->lo[q]) / dx[q]) + 1;
+        if (j >= 0 && j <= NBIN) ++cnt[q][j];
+      }
+    const double norm = (double)(nstats - 1);
+    for (int ib = 0; ib < NBIN && pdfs; ++ib)
+      fprintf(pdfs, "%.15e %.15e %.15e %.15e %.15e %.15e \n", s->lo[0] + (ib - 0.5) * dx[0],
+              cnt[0][ib] / (norm * dx[0]), s->lo[1] + (ib - 0.5) * dx[1], cnt[1][ib] / (norm * dx[1]),
+              s->lo[2] + (ib - 0.5) * dx[2], cnt[2][ib] / (norm * dx[2]));
+  }
+  for (int q = 0; q < 4; ++q) free(prof[q]);
+  free(uvar);
+  return rc;
 }
