@@ -72,6 +72,13 @@ int psg_ns3d_upload(psg_ns3d* h, const double* const* comps);
 int psg_ns3d_download(psg_ns3d* h, double* const* comps);
 /* RK4 schemes: the stage state x0 (vorticity before the divergence clean-up) */
 int psg_ns3d_download_stage(psg_ns3d* h, double* const* comps);
+/* The state to / from page-locked host arrays in the reference layout, kept
+ * modes only: the conversion kernels read / write the host memory directly and
+ * leave its other entries alone (the upload sets the engine's other modes to
+ * zero).  PSG_ERR_UNSUPPORTED for pageable memory.  The drop-ins use them for
+ * in-place calls on page-locked arrays whose non-kept entries are zero. */
+int psg_ns3d_upload_kept(psg_ns3d* h, const double* const* comps);
+int psg_ns3d_download_kept(psg_ns3d* h, double* const* comps);
 /* nsteps steps of length dt, enqueued on the handle's stream.  dump_last:
  * keep the physical vorticity of the last predictor (Heun schemes) */
 int psg_ns3d_step(psg_ns3d* h, double dt, int nsteps, int dump_last);

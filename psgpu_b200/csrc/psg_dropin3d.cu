@@ -86,6 +86,77 @@ bool check_sizes(const char* who, int IKTX, int IKTY, int IKTZ, int KTZ, int NKT
   return true;
 }
 
+#if defined(PSG_FLAVOUR_BOUS3D)
+// Runs [begin, end) of the reference box (in doubles, ikx fastest) that hold
+// modes outside the kept set: |k| > N/3 - 1/2, and the kx = 0 half-plane's
+// duplicates (ky < 0, or ky = 0 and kz <= 0) (3D_NavierStokes/src/init.F90:
+// 38-57).  Built once per grid size.
+const std::vector<long>& nonkept_runs(int n) {
+  static int cached_n = 0;
+  static std::vector<long> runs;
+  if (cached_n == n) return runs;
+  runs.clear();
+  const int K = n / 3, X = K + 1, Y = 2 * K + 1;
+  const double lim = (K - 0.5) * (K - 0.5);
+  long i = 0, start = -1;
+  for (int ikz = 0; ikz < Y; ++ikz)
+    for (int iky = 0; iky < Y; ++iky)
+      for (int ikx = 0; ikx < X; ++ikx, ++i) {
+        const int ky = iky - K, kz = ikz - K;
+        const bool keep = !(ikx == 0 && ky < 0) && !(ikx == 0 && ky == 0 && kz <= 0) &&
+                          !((double)ikx * ikx + (double)ky * ky + (double)kz * kz > lim);
+        if (!keep && start < 0) start = i;
+        if (keep && start >= 0) {
+          runs.push_back(2 * start);
+          runs.push_back(2 * i);
+          start = -1;
+        }
+      }
+  if (start >= 0) {
+    runs.push_back(2 * start);
+    runs.push_back(2 * i);
+  }
+  cached_n = n;
+  return runs;
+}
+
+bool nonkept_zero(const double* a, int n) {
+  const std::vector<long>& r = nonkept_runs(n);
+  for (size_t k = 0; k < r.size(); k += 2)
+    for (long i = r[k]; i < r[k + 1]; ++i)
+      if (a[i] != 0.0) return false;
+  return true;
+}
+
+// Upload, steps() and download of an in-place call.  When the state arrays are
+// page-locked and every entry outside the kept modes is zero, only the kept
+// modes cross the host link (the conversion kernels read and write the host
+// arrays directly; the zero check runs on the host while the device steps).
+// Otherwise, or with PSG_DROPIN_FULL_COPY=1, the whole boxes are copied; both
+// paths return the same state.
+template <typename Steps>
+int advance(psg_ns3d* h, double2* const* state, int nc, int n, Steps steps) {
+  const double* in[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* out[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int q = 0; q < nc; ++q) {
+    in[q] = (const double*)state[q];
+    out[q] = (double*)state[q];
+  }
+  const char* full = getenv("PSG_DROPIN_FULL_COPY");
+  if (!(full && atoi(full) == 1) && psg_ns3d_upload_kept(h, in) == PSG_OK) {
+    if (int rc = steps()) return rc;
+    bool zero = true;
+    for (int q = 0; q < nc && zero; ++q) zero = nonkept_zero(in[q], n);
+    if (zero) return psg_ns3d_download_kept(h, out);
+    // a non-kept entry was set: once more from the whole box
+    if (int rc = psg_ns3d_sync(h)) return rc;
+  }
+  if (int rc = psg_ns3d_upload(h, in)) return rc;
+  if (int rc = steps()) return rc;
+  return psg_ns3d_download(h, out);
+}
+#endif
+
 #if defined(PSG_FLAVOUR_BOUS3D_DNS)
 // one guess of the recurrence search in the reference's records
 // (3D_Boussinesq/src/functions.h:592-609): UPO_ZK.out gets start time, v2,
@@ -218,8 +289,6 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
     return;
   }
   psg_ns3d* h = engine(*NX, PSG_SCHEME_BOUS_RK4);
-  const double* in[4] = {(const double*)xii, (const double*)eta, (const double*)zet, (const double*)rho};
-  double* out[4] = {(double*)xii, (double*)eta, (double*)zet, (double*)rho};
   const double delt = *DELT;
   double tme = *TSTART;
   int nfull = 0;
@@ -227,9 +296,12 @@ extern "C" void timestep_cuda_(double2* xii, double2* eta, double2* zet, double2
     ++nfull;
     tme += delt;
   }
+  auto steps = [&]() -> int {
+    if (int rc = psg_ns3d_step(h, delt, nfull, 0)) return rc;
+    return tme != *Tstep ? psg_ns3d_step(h, *Tstep - tme, 1, 0) : PSG_OK;
+  };
   if (!h || psg_ns3d_set_params(h, *V2, *AMPFOR, *KFY, *Ri, *Sc, *Theta) ||
-      psg_ns3d_upload(h, in) || psg_ns3d_step(h, delt, nfull, 0) ||
-      (tme != *Tstep && psg_ns3d_step(h, *Tstep - tme, 1, 0)) || psg_ns3d_download(h, out)) {
+      advance(h, state, 4, *NX, steps)) {
     report("timestep_cuda_");
     fill_nan(state, 4, *NKT);
     return;

@@ -75,6 +75,8 @@ struct Engine3DBase {
   virtual int download_stage(double* const* comps) = 0;
   virtual int upload_device(const void* const* comps) = 0;
   virtual int download_device(void* const* comps) = 0;
+  virtual int upload_kept(const double* const* comps) = 0;
+  virtual int download_kept(double* const* comps) = 0;
   virtual int energetics(double* out) = 0;
   virtual int max_velocity(double* out) = 0;
   virtual int buoyancy_flux(double* out) = 0;

@@ -148,6 +148,18 @@ extern "C" int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms) {
   return h->e->tuning(variant, ms);
 }
 
+extern "C" int psg_ns3d_upload_kept(psg_ns3d* h, const double* const* comps) {
+  PSG_CHECK_HANDLE(h);
+  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
+  return h->e->upload_kept(comps);
+}
+
+extern "C" int psg_ns3d_download_kept(psg_ns3d* h, double* const* comps) {
+  PSG_CHECK_HANDLE(h);
+  if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }
+  return h->e->download_kept(comps);
+}
+
 extern "C" int psg_ns3d_upload_device(psg_ns3d* h, void* const* comps) {
   PSG_CHECK_HANDLE(h);
   return h->e->upload_device((const void* const*)comps);

@@ -1225,6 +1225,57 @@ __global__ void box_to_ref(Geom3<T> g, const cpx<T>* __restrict__ src, double2* 
   }
 }
 
+// The same two conversions on the kept modes only, for host boxes in
+// page-locked memory that the kernels address directly: the upload reads the
+// kept modes (and stores zero for every other mode of the state), the download
+// writes the kept modes and leaves the other entries of the host box alone.
+template <typename T>
+__global__ void box_from_ref_kept(Geom3<T> g, const double2* __restrict__ src,
+                                  cpx<T>* __restrict__ dst, cpx<T>* __restrict__ low) {
+  const int W = kTileW;
+  const long total = (long)g.XP * g.Y * g.Y;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % W);
+    long r = i / W;
+    const int ikz = (int)(r % g.Y); r /= g.Y;
+    const int iky = (int)(r % g.Y);
+    const int xt = (int)(r / g.Y);
+    const int ikx = xt * W + w;
+    cpx<T> v = czero<T>(), lo = czero<T>();
+    if (ikx < g.X && keep_mode<T>(ikx, iky - g.K, ikz - g.K, g.K, g.alpha)) {
+      const double2 s = src[((long)ikz * g.Y + iky) * g.X + ikx];
+      v = cpx<T>{(T)s.x, (T)s.y};
+      lo = cpx<T>{(T)(s.x - (double)v.x), (T)(s.y - (double)v.y)};
+    }
+    dst[i] = v;
+    if (low) low[i] = lo;
+  }
+}
+
+template <typename T>
+__global__ void box_to_ref_kept(Geom3<T> g, const cpx<T>* __restrict__ src, double2* __restrict__ dst,
+                                const cpx<T>* __restrict__ low) {
+  const int W = kTileW;
+  const long total = (long)g.Y * g.Y * g.X;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ikx = (int)(i % g.X);
+    const long r = i / g.X;
+    const int iky = (int)(r % g.Y), ikz = (int)(r / g.Y);
+    if (!keep_mode<T>(ikx, iky - g.K, ikz - g.K, g.K, g.alpha)) continue;
+    const long j = (((long)(ikx / W) * g.Y + iky) * g.Y + ikz) * W + (ikx % W);
+    const cpx<T> s = src[j];
+    double2 v = make_double2((double)s.x, (double)s.y);
+    if (low) {
+      const cpx<T> c = low[j];
+      v.x += (double)c.x;
+      v.y += (double)c.y;
+    }
+    dst[i] = v;
+  }
+}
+
 // running mean squares (the DNS's avgVelocity, 3D_NavierStokes/src/kernels.h:70-81)
 template <typename T>
 __global__ void rms_acc(const T* __restrict__ u, double* __restrict__ rms, long n, double count) {
@@ -2017,6 +2068,54 @@ struct Engine3D final : Engine3DBase {
   }
 
   int download(double* const* comps) override { return download_from(comps, nullptr); }
+
+  // the kept modes only, read from / written to page-locked host memory by the
+  // conversion kernels themselves (no staging copy; the other entries of the
+  // host boxes are neither read nor written)
+  static const void* host_mapped(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+  }
+  int upload_kept(const double* const* comps) override {
+    const void* dp[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < nc; ++q)
+      if (!(dp[q] = host_mapped(comps[q]))) {
+        psg_set_error("kept-mode upload needs page-locked host memory");
+        return PSG_ERR_UNSUPPORTED;
+      }
+    for (int q = 0; q < nc; ++q) {
+      box_from_ref_kept<T><<<592, 256, 0, stream>>>(g, (const double2*)dp[q], R.S.c[q], R.SC.c[q]);
+      ++launches;
+    }
+    if (R.X0.c[0]) {
+      copy_fields<T><<<592, 256, 0, stream>>>(R.S, R.X0, nc, box);
+      ++launches;
+    }
+    first_rhs = 1;
+    lin_dx = false;
+    PSG_CUDA_TRY(cudaGetLastError());
+    return PSG_OK;
+  }
+  int download_kept(double* const* comps) override {
+    void* dp[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < nc; ++q)
+      if (!(dp[q] = (void*)host_mapped(comps[q]))) {
+        psg_set_error("kept-mode download needs page-locked host memory");
+        return PSG_ERR_UNSUPPORTED;
+      }
+    if (int rc = check_status()) return rc;
+    for (int q = 0; q < nc; ++q) {
+      box_to_ref_kept<T><<<592, 256, 0, stream>>>(g, R.S.c[q], (double2*)dp[q], R.SC.c[q]);
+      ++launches;
+    }
+    PSG_CUDA_TRY(cudaGetLastError());
+    PSG_CUDA_TRY(cudaStreamSynchronize(stream));
+    return PSG_OK;
+  }
 
   // device FP64 boxes (reference layout) <-> state, ordered on the engine's
   // stream, no host synchronisation
