@@ -117,6 +117,11 @@ int psg_ns3d_autotune(psg_ns3d* h, int* variant, float* ms);
 /* the autotuner's current choice and timings, without re-running it
  * (PSG_XPASS_VARIANT=0..15 in the environment pins the choice at set-up) */
 int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms);
+/* the autotuner's pass-A choice (FP32 engines): *packed = 1 when the z-inverse
+ * transforms two fields per packed f32x2 instruction, 0 for the scalar kernel;
+ * ms[2] its timings (scalar, packed; -1: not timed: FP64, or the packed
+ * kernel's shared memory does not fit).  PSG_PASSA_PACKED=0/1 pins it. */
+int psg_ns3d_tuning_a(psg_ns3d* h, int* packed, float* ms);
 /* the state from / to device arrays: FP64 complex boxes in the reference
  * layout (IKTX*IKTY*IKTZ double2 per component), ordered on the engine's
  * stream without a host synchronisation */

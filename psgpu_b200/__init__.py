@@ -313,6 +313,14 @@ class NS3D:
         _check(fn(self._h, C.byref(v), ms))
         return v.value, list(ms)
 
+    def pass_a_tuning(self):
+        """pass-A choice of the autotuner: (packed f32x2 transforms or not,
+        (ms scalar, ms packed) per launch; -1 where not timed)"""
+        pk = C.c_int()
+        ms = (C.c_float * 2)()
+        _check(lib().psg_ns3d_tuning_a(self._h, C.byref(pk), ms))
+        return bool(pk.value), (ms[0], ms[1])
+
     def device_state(self):
         xp = C.c_int()
         ptrs = (C.c_void_p * 4)()

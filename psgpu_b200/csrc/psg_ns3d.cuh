@@ -95,6 +95,7 @@ struct Engine3DBase {
   // x-pass autotuner: run at set-up; report the chosen variant and timings
   virtual int autotune() = 0;
   virtual int tuning(int* variant, float* ms) = 0;
+  virtual int tuning_a(int* packed, float* ms) = 0;
   // per-pass timing (A, B, C, D, E) with CUDA events between the launches
   virtual int profile(int enable) = 0;
   virtual int profile_read(double* ms, long* counts) = 0;

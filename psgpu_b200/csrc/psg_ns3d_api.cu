@@ -148,6 +148,11 @@ extern "C" int psg_ns3d_tuning(psg_ns3d* h, int* variant, float* ms) {
   return h->e->tuning(variant, ms);
 }
 
+extern "C" int psg_ns3d_tuning_a(psg_ns3d* h, int* packed, float* ms) {
+  PSG_CHECK_HANDLE(h);
+  return h->e->tuning_a(packed, ms);
+}
+
 extern "C" int psg_ns3d_upload_kept(psg_ns3d* h, const double* const* comps) {
   PSG_CHECK_HANDLE(h);
   if (!comps) { psg_set_error("null state"); return PSG_ERR_ARG; }

@@ -79,6 +79,19 @@ struct RowStride {
   static constexpr int value = S + ((off - (S % 16)) + 16) % 16;
 };
 
+// Programmatic dependent launch.  pdl_trigger: the next kernel of the stream
+// may be launched once every block of this one has executed it (its blocks
+// then take the SM slots this grid's last blocks free, and run their set-up).
+// pdl_wait: block until the kernels this launch depends on have completed and
+// their writes are visible.  Every pass calls pdl_wait before its first global
+// access other than the constant twiddle table, reads and writes alike (the
+// next pass writes buffers the previous one reads).  Both are no-ops for a
+// launch without the programmatic-serialisation attribute.
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Load `n` contiguous chunks into shared memory with one mbarrier; returns
 // false (uniformly) if the copy did not complete within the wait bound.
 __device__ __forceinline__ bool tile_load(uint64_t* bar, int* s_ok, void* const* dst,
@@ -124,6 +137,56 @@ __device__ __forceinline__ cpx<T> spec_op(int op, int comp, const cpx<T>* x, T k
   return r;
 }
 
+// pass A's staging of one (xt, ky) tile: twiddles and the signed 1/k^2 table
+// (negated where the 2/3 rule drops the mode), then the NC state tiles by bulk
+// copy, and the kx = 0 column of tile 0 for ky <= 0 patched with the conjugate
+// of the stored mode at (-ky, -kz) (Hermitian completion).  False (uniformly)
+// if the copy did not complete within the wait bound.
+template <typename T, int N, int NC, typename Src>
+__device__ __forceinline__ bool a_stage(const Geom3<T>& g, Src src_comp, const cpx<T>* __restrict__ tw,
+                                        cpx<T>* s_in, cpx<T>* s_tw, T* s_wk, uint64_t* s_bar,
+                                        int* s_ok, int* status) {
+  constexpr int W = kTileW;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int xt = blockIdx.x, iky = blockIdx.y;
+  const long tile = ((long)xt * Y + iky) * Y * W;
+  pdl_trigger();
+  if (tid == 0) mbar_init(s_bar, 1);
+  __syncthreads();
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
+  const bool mirror = (xt == 0) && (iky <= K);
+  for (int idx = tid; idx < Y * W; idx += nth) {
+    const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
+    bool ll;
+    if (ikx >= Box<N>::X) ll = false;
+    else if (ikx == 0 && mirror && !(iky == K && ikz > K))  // value taken from the mirror mode
+      ll = (iky == K && ikz == K) ? false : keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
+    else ll = keep_mode<T>(ikx, iky - K, ikz - K, K, g.alpha);
+    const T kx = (T)ikx * g.alpha, ky = (T)(iky - K), kz = (T)(ikz - K);
+    const T wki = wkinv(kx * kx + ky * ky + kz * kz);
+    s_wk[idx] = ll ? wki : -wki;
+  }
+  pdl_wait();
+  if (tid == 0) {
+    mbar_expect_tx(s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
+    for (int q = 0; q < NC; ++q)
+      bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), s_bar);
+  }
+  if (!tile_wait(s_bar, s_ok, status)) return false;
+  if (mirror) {
+    const long mt = (long)(2 * K - iky) * Y * W;
+    for (int i = tid; i < NC * Y; i += nth) {
+      const int q = i / Y, ikz = i % Y;
+      cpx<T>* d = s_in + q * Y * W + ikz * W;
+      if (iky == K && ikz == K) *d = czero<T>();
+      else if (!(iky == K && ikz > K)) *d = cconj(src_comp(q)[mt + (long)(2 * K - ikz) * W]);
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
 template <typename T, int N, int NC, int NF, int MODE = 0, int NG = 2>
 __global__ void __launch_bounds__(NG * kTileW * LineFFT<N, 1, T>::G,
                                   sizeof(T) > 4 ? (N >= 256 ? 1 : 2) : (NG == 2 ? 3 : 2))
@@ -143,49 +206,16 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   T* s_wk = reinterpret_cast<T*>(s_ex + NG * W * SX);     // [Y][W]
 
   // NG groups of W x G threads transform NG output fields at a time
-  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tid = threadIdx.x;
   const int grp = tid / (W * F::G), ht = tid % (W * F::G);
   const int c = ht % W, gi = ht / W;
   const int xt = blockIdx.x, iky = blockIdx.y;
-  const long tile = ((long)xt * Y + iky) * Y * W;
-  if (tid == 0) mbar_init(&s_bar, 1);
-  __syncthreads();
   auto src_comp = [&](int q) -> const cpx<T>* {
     if (MODE == 1 && q >= 3) return in2.c[q - 3];
     if (MODE == 2 && q == 4) return in2.c[0];
     return in.c[q];
   };
-  if (tid == 0) {
-    mbar_expect_tx(&s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
-    for (int q = 0; q < NC; ++q)
-      bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), &s_bar);
-  }
-  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
-  const bool mirror = (xt == 0) && (iky <= K);
-  for (int idx = tid; idx < Y * W; idx += nth) {
-    const int ikz = idx / W, cc = idx % W, ikx = xt * W + cc;
-    bool ll;
-    if (ikx >= Box<N>::X) ll = false;
-    else if (ikx == 0 && mirror && !(iky == K && ikz > K))  // value taken from the mirror mode
-      ll = (iky == K && ikz == K) ? false : keep_mode<T>(0, K - iky, K - ikz, K, g.alpha);
-    else ll = keep_mode<T>(ikx, iky - K, ikz - K, K, g.alpha);
-    const T kx = (T)ikx * g.alpha, ky = (T)(iky - K), kz = (T)(ikz - K);
-    const T wki = wkinv(kx * kx + ky * ky + kz * kz);
-    s_wk[idx] = ll ? wki : -wki;
-  }
-  if (!tile_wait(&s_bar, &s_ok, status)) return;
-  // the kx = 0 column of tile 0 for ky <= 0 is the conjugate of the stored
-  // mode at (-ky, -kz) (Hermitian completion): patched into the staged tile
-  if (mirror) {
-    const long mt = (long)(2 * K - iky) * Y * W;
-    for (int i = tid; i < NC * Y; i += nth) {
-      const int q = i / Y, ikz = i % Y;
-      cpx<T>* d = s_in + q * Y * W + ikz * W;
-      if (iky == K && ikz == K) *d = czero<T>();
-      else if (!(iky == K && ikz > K)) *d = cconj(src_comp(q)[mt + (long)(2 * K - ikz) * W]);
-    }
-    __syncthreads();
-  }
+  if (!a_stage<T, N, NC>(g, src_comp, tw, s_in, s_tw, s_wk, &s_bar, &s_ok, status)) return;
 
   const int ikx = xt * W + c;
   const T kx = (T)ikx * g.alpha;
@@ -252,6 +282,84 @@ pass_a(Geom3<T> g, Fields4<T> in, cpx<T>* __restrict__ out, const cpx<T>* __rest
   }
 }
 
+// pass A with two fields per thread on packed f32x2 arithmetic (FP32 engine,
+// the step's own right-hand side, MODE 0 of pass_a): one group of W x G
+// threads takes the output fields in pairs (f, f+1) through one LineFFT2
+// transform, so every butterfly and twiddle instruction serves two fields.
+// Staging, field values and output layout are pass_a's; the exchange holds
+// the pair's values side by side (16-byte words, row stride odd mod 8 so that
+// the eight columns of a quarter warp fall on distinct bank groups).
+template <int N, int NC, int NF>
+__global__ void __launch_bounds__(kTileW * LineFFT<N, 1, float>::G, 3)
+pass_a_pk(Geom3<float> g, Fields4<float> in, cpx<float>* __restrict__ out,
+          const cpx<float>* __restrict__ tw, int mask_vel, int* status) {
+  using T = float;
+  using F = LineFFT<N, +1, T>;
+  using F2 = LineFFT2<N, +1>;
+  constexpr int W = kTileW;
+  constexpr int SX = F::SMEM + ((1 - F::SMEM % 8) + 8) % 8;
+  constexpr int Y = Box<N>::Y, K = Box<N>::K, XT = Box<N>::XT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_ok;
+  cpx<T>* s_in = reinterpret_cast<cpx<T>*>(smem_raw);  // [NC][Y][W]
+  cpx<T>* s_tw = s_in + NC * Y * W;                      // [N]
+  float4* s_ex = reinterpret_cast<float4*>(s_tw + N);    // [W][SX]
+  T* s_wk = reinterpret_cast<T*>(s_ex + W * SX);         // [Y][W]
+  const int tid = threadIdx.x, c = tid % W, gi = tid / W;
+  const int xt = blockIdx.x, iky = blockIdx.y;
+  auto src_comp = [&](int q) -> const cpx<T>* { return in.c[q]; };
+  if (!a_stage<T, N, NC>(g, src_comp, tw, s_in, s_tw, s_wk, &s_bar, &s_ok, status)) return;
+  const int ikx = xt * W + c;
+  const T kx = (T)ikx * g.alpha, ky = (T)(iky - K);
+  const bool live = ikx < Box<N>::X;
+  // field f at staged mode o (pass_a, MODE 0)
+  auto value = [&](int f, int o, T kz, T tk) -> cpx<T> {
+    if (f < 3) return s_in[f * Y * W + o];
+    if (f < 6) {
+      const T wki = (mask_vel && tk < (T)0) ? (T)0 : fabsf(tk);
+      const cpx<T> xi = s_in[o], et = s_in[Y * W + o], zt = s_in[2 * Y * W + o];
+      if (f == 3) return cpx<T>{-(ky * zt.y - kz * et.y) * wki, -(kz * et.x - ky * zt.x) * wki};
+      if (f == 4) return cpx<T>{-(kz * xi.y - kx * zt.y) * wki, -(kx * zt.x - kz * xi.x) * wki};
+      return cpx<T>{-(kx * et.y - ky * xi.y) * wki, -(ky * xi.x - kx * et.x) * wki};
+    }
+    if (NC > 3 && f < 9) {
+      const cpx<T> rho = s_in[3 * Y * W + o];
+      const T kk = (f == 6) ? kx : (f == 7) ? ky : kz;
+      return cpx<T>{-kk * rho.y, kk * rho.x};
+    }
+    return czero<T>();
+  };
+#pragma unroll 1
+  for (int f0 = 0; f0 < NF; f0 += 2) {
+    const bool two = f0 + 1 < NF;
+    Pk v[F::E];
+#pragma unroll
+    for (int e = 0; e < F::E; ++e) {
+      const int ikz = row_to_box(F::in_index(gi, e), K, N);
+      const int o = ikz * W + c;
+      cpx<T> a = czero<T>(), b = czero<T>();
+      if (ikz >= 0 && live) {
+        const T kz = (T)(ikz - K), tk = s_wk[o];
+        a = value(f0, o, kz, tk);
+        if (two) b = value(f0 + 1, o, kz, tk);
+      }
+      v[e] = Pk{make_float2(a.x, b.x), make_float2(a.y, b.y)};
+    }
+    F2::run(v, gi, s_tw, s_ex + c * SX, BlockSync());
+    if (live) {
+      cpx<T>* o0 = out + ((((long)f0 * XT + xt) * N) * Y + iky) * W + c;
+      cpx<T>* o1 = o0 + (long)XT * N * Y * W;
+#pragma unroll
+      for (int e = 0; e < F::E; ++e) {
+        const long off = (long)F::out_index(gi, e) * Y * W;
+        o0[off] = cpx<T>{v[e].re.x, v[e].im.x};
+        if (two) o1[off] = cpx<T>{v[e].re.y, v[e].im.y};
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // pass B: y-inverse.  grid (XT, N, NF): tile B1[f][xt][z] = [ky][W] -> B2 rows
 // ---------------------------------------------------------------------------
@@ -272,14 +380,16 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   cpx<T>* s_tw = s_in + AREA;
   const int tid = threadIdx.x, c = tid % W, gi = tid / W;
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
+  pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
+  pdl_wait();
   if (tid == 0) {
     mbar_expect_tx(&s_bar, (uint32_t)(Y * W * sizeof(cpx<T>)));
     bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * Y * W, (uint32_t)(Y * W * sizeof(cpx<T>)),
              &s_bar);
   }
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   cpx<T> v[F::E];
 #pragma unroll
@@ -507,9 +617,11 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   uint64_t* bar = s_bar[warp];
   const long plane = (long)N * N * XP;
   const uint32_t bytes = (uint32_t)(RPW * XP * sizeof(cpx<T>));
+  pdl_trigger();
   if (lane == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); }
   for (int i = tid; i < 2 * N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
+  pdl_wait();
   // warp tile t = rows [t*RPW, t*RPW + RPW) of every field, one bulk copy per
   // field; the buffer's earlier contents were read by this warp's lanes before
   // the __syncwarp that precedes every call
@@ -708,14 +820,16 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   cpx<T>* s_tw = s_in + AREA;
   const int tid = threadIdx.x, c = tid % W, gi = tid / W;
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
+  pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
+  pdl_wait();
   if (tid == 0) {
     mbar_expect_tx(&s_bar, (uint32_t)(N * W * sizeof(cpx<T>)));
     bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * N * W, (uint32_t)(N * W * sizeof(cpx<T>)),
              &s_bar);
   }
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   cpx<T> v[F::E];
 #pragma unroll
@@ -993,9 +1107,12 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   cpx<T>* s_ex = s_tw + N;  // without ALIAS: the first group's; then the second's
   const int tid = threadIdx.x, nth = blockDim.x, c = tid % W;
   const int xt = blockIdx.x, iky = blockIdx.y;
+  pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   __syncthreads();
   const long tile = ((long)xt * Y + iky) * Y * W;
+  pdl_wait();
   if (tid == 0) {
     const uint32_t bytes = (uint32_t)(N * W * sizeof(cpx<T>));
     mbar_expect_tx(&s_bar, NO * bytes);
@@ -1018,7 +1135,6 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
       }
     }
   }
-  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   // three fields: both halves transform (fields 2 and 1, then 0), the second
   // half in an exchange area of its own; more fields: the first half alone
@@ -1607,11 +1723,19 @@ struct Engine3D final : Engine3DBase {
   bool lin_dx = false;
   Fields4<T> SA{}, SB{};       // Boussinesq adjoint products: psi (i k rho) | psi u
   int c_variant = 0;           // x-pass variant chosen by the autotuner
+  // pass A on packed f32x2 transforms (FP32 engine; chosen by the autotuner
+  // when its shared memory fits) and the autotuner's timings (scalar, packed)
+  bool a_pk = false, a_pk_ok = false;
+  float a_ms[2] = {-1.f, -1.f};
   int c_resident[16] = {1, 1, 1, 1};  // resident blocks of each x-pass variant
   float c_ms[16] = {};                 // autotuner timings (ms per launch)
   long launches = 0;
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
+  // programmatic dependent launch of the passes of a right-hand side (each
+  // pass's blocks launch and set up while the previous pass drains); off with
+  // PSG_PDL=0 and while the per-pass events are recorded
+  bool pdl = true;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<int> ev_tag;
   size_t ev_used = 0;
@@ -1718,6 +1842,7 @@ struct Engine3D final : Engine3DBase {
     g.XP = (g.X + kTileW - 1) / kTileW * kTileW;
     g.alpha = (T)alpha;
     scheme = scheme_;
+    if (const char* e = getenv("PSG_PDL")) pdl = atoi(e) != 0;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
     nc = bous ? 4 : 3;
     nfi = bous ? 9 : 6;
@@ -1805,6 +1930,13 @@ struct Engine3D final : Engine3DBase {
 #define PSG_SMEM(kern) PSG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, big))
     PSG_SMEM((pass_a<T, N, 3, 6>));
     PSG_SMEM((pass_a<T, N, 4, 9, 0, 3>));
+    if constexpr (sizeof(T) == 4) {
+      a_pk_ok = smem_a_pk_n<N>(nc) <= (size_t)big;
+      if (a_pk_ok) {
+        PSG_SMEM((pass_a_pk<N, 3, 6>));
+        PSG_SMEM((pass_a_pk<N, 4, 9>));
+      }
+    }
     PSG_SMEM((pass_b<T, N>));
     for (int v = 0; v < kCVariants; ++v) {
       if (!c_valid(v)) continue;
@@ -1860,10 +1992,32 @@ struct Engine3D final : Engine3DBase {
   const void* c_kernel(int v) const {
     return c_kernel_nf<N>(v, scheme == SCHEME_BOUS_RK4 ? 9 : 6);
   }
-  template <int N>
+  // launch on the engine's stream; dep: with the programmatic-serialisation
+  // attribute, for a pass whose predecessor on the stream is another pass
+  // kernel (both wait and trigger through pdl_wait / pdl_trigger)
+  template <typename... P, typename... A>
+  int launch_k(bool dep, void (*k)(P...), dim3 grid, dim3 blk, size_t smem, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = blk;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    if (dep && pdl && !profiling) {
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+    }
+    PSG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...));
+    return PSG_OK;
+  }
+
   // nf: fields the x-pass reads (6: -(u x w); 9: + u.grad rho; 7: the
   // Boussinesq adjoint's scalar products); 0: the engine's own
-  int launch_c(int v, T scale, T* dp, int nf = 0, unsigned long long* um = nullptr) {
+  template <int N>
+  int launch_c(int v, T scale, T* dp, int nf = 0, unsigned long long* um = nullptr,
+               bool dep = false) {
     constexpr int L0 = 64 / LineFFT<N, 1, T>::G;
     constexpr int RPW = 32 / LineFFT<N, 1, T>::G;  // rows per warp tile
     const int wpb = L0 * c_rows_x2(v) / RPW;       // warps per block
@@ -1884,7 +2038,19 @@ struct Engine3D final : Engine3DBase {
     unsigned long long* u = um;
     int dnf = (dp && (dump_mode & 2)) ? 6 : 3;
     void* args[] = {&gg, &in, &out, &twp, &scale, &dp, &st, &nw, &u, &dnf};
-    PSG_CUDA_TRY(cudaLaunchKernel(k, dim3(grid), dim3(th), args, sm, stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(th);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    if (dep && pdl && !profiling) {
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+    }
+    PSG_CUDA_TRY(cudaLaunchKernelExC(&cfg, k, args));
     return PSG_OK;
   }
 
@@ -1928,14 +2094,56 @@ struct Engine3D final : Engine3DBase {
     PSG_CUDA_TRY(cudaGetLastError());
     return check_status();
   }
-  int autotune() override {
-    switch (g.n) {
-      case 16: return autotune_n<16>();
-      case 32: return autotune_n<32>();
-      case 64: return autotune_n<64>();
-      case 128: return autotune_n<128>();
-      default: return autotune_n<256>();
+  // pass A, FP32: scalar or packed transforms, timed the same way
+  // (PSG_PASSA_PACKED=0/1 pins the choice)
+  template <int N>
+  int autotune_a_n() {
+    a_ms[0] = a_ms[1] = -1.f;
+    a_pk = false;
+    if (sizeof(T) != 4 || !a_pk_ok) return PSG_OK;
+    if (const char* pin = getenv("PSG_PASSA_PACKED")) {
+      a_pk = atoi(pin) != 0;
+      return PSG_OK;
     }
+    cudaEvent_t a, b;
+    PSG_CUDA_TRY(cudaEventCreate(&a));
+    PSG_CUDA_TRY(cudaEventCreate(&b));
+    for (int pk = 0; pk < 2; ++pk) {
+      int rc = launch_a<N>(false, pk != 0, stage_input(), 0);
+      cudaEventRecord(a, stream);
+      for (int r = 0; r < 3 && !rc; ++r) rc = launch_a<N>(false, pk != 0, stage_input(), 0);
+      cudaEventRecord(b, stream);
+      cudaError_t e = cudaEventSynchronize(b);
+      if (rc || e != cudaSuccess) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (rc) return rc;
+        PSG_CUDA_TRY(e);
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      a_ms[pk] = ms / 3.f;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    a_pk = a_ms[1] < a_ms[0];
+    PSG_CUDA_TRY(cudaGetLastError());
+    return check_status();
+  }
+  int autotune() override {
+    int rc;
+    switch (g.n) {
+      case 16: rc = autotune_n<16>(); return rc ? rc : autotune_a_n<16>();
+      case 32: rc = autotune_n<32>(); return rc ? rc : autotune_a_n<32>();
+      case 64: rc = autotune_n<64>(); return rc ? rc : autotune_a_n<64>();
+      case 128: rc = autotune_n<128>(); return rc ? rc : autotune_a_n<128>();
+      default: rc = autotune_n<256>(); return rc ? rc : autotune_a_n<256>();
+    }
+  }
+  int tuning_a(int* packed, float* ms) override {
+    if (packed) *packed = a_pk ? 1 : 0;
+    if (ms) { ms[0] = a_ms[0]; ms[1] = a_ms[1]; }
+    return PSG_OK;
   }
   int tuning(int* variant, float* ms) override {
     if (variant) *variant = c_variant;
@@ -1974,77 +2182,108 @@ struct Engine3D final : Engine3DBase {
   }
 
   // one right-hand-side evaluation followed by the stage update
+  // pass A of the step's right-hand side, scalar or on packed transforms
   template <int N>
-  int rhs_n(int stage, bool want_dump, bool want_umax = false) {
+  int launch_a(bool chain, bool packed, Fields4<T> in, int mv) {
+    constexpr int G = LineFFT<N, 1, T>::G;
+    const int XT = g.XP / kTileW;
+    const bool bous = (scheme == SCHEME_BOUS_RK4);
+    if constexpr (sizeof(T) == 4) {
+      if (packed && a_pk_ok) {
+        if (bous)
+          return launch_k(chain, pass_a_pk<N, 4, 9>, dim3(XT, g.Y), dim3(kTileW * G), smem_a_pk_n<N>(4),
+                          g, in, B1, tw, mv, d_status);
+        return launch_k(chain, pass_a_pk<N, 3, 6>, dim3(XT, g.Y), dim3(kTileW * G), smem_a_pk_n<N>(3), g,
+                        in, B1, tw, mv, d_status);
+      }
+    }
+    const Fields4<T> none{};
+    if (bous)
+      return launch_k(chain, pass_a<T, N, 4, 9, 0, 3>, dim3(XT, g.Y), dim3(3 * kTileW * G), smem_a(), g,
+                      in, B1, tw, mv, d_status, none, 0);
+    return launch_k(chain, pass_a<T, N, 3, 6>, dim3(XT, g.Y), dim3(2 * kTileW * G), smem_a(), g, in, B1,
+                    tw, mv, d_status, none, 0);
+  }
+
+  // chain: the stream's last operation is the pass E of the previous
+  // right-hand side (so that pass A may launch programmatically after it)
+  template <int N>
+  int rhs_n(int stage, bool want_dump, bool want_umax = false, bool chain = false) {
     using FG = LineFFT<N, 1, T>;
     const int G = FG::G;
     const dim3 blk(kTileW * G);
     const int XT = g.XP / kTileW;
-    const bool bous = (scheme == SCHEME_BOUS_RK4);
     Fields4<T> in = stage_input();
     const int mv = first_rhs;
     first_rhs = 0;
     mark(-1);
     const dim3 blk2(2 * kTileW * G);
-    if (bous)
-      pass_a<T, N, 4, 9, 0, 3><<<dim3(XT, g.Y), dim3(3 * kTileW * G), smem_a(), stream>>>(g, in, B1, tw,
-                                                                                       mv, d_status);
-    else
-      pass_a<T, N, 3, 6><<<dim3(XT, g.Y), blk2, smem_a(), stream>>>(g, in, B1, tw, mv, d_status);
+    int rc = launch_a<N>(chain, a_pk, in, mv);
+    if (rc) return rc;
     mark(0);
-    pass_b<T, N><<<dim3(XT, N, nfi), blk, smem_b(), stream>>>(g, B1, B2, tw, d_status);
+    if ((rc = launch_k(true, pass_b<T, N>, dim3(XT, N, nfi), blk, smem_b(), g, B1, B2, tw, d_status)))
+      return rc;
     mark(1);
     const T scale = (T)1 / ((T)N * (T)N * (T)N);
     T* dp = want_dump ? dump : nullptr;
     if (want_umax) PSG_CUDA_TRY(cudaMemsetAsync(d_umax, 0, sizeof(unsigned long long), stream));
-    launch_c<N>(c_variant, scale, dp, 0, want_umax ? d_umax : nullptr);
+    // after the memset the x-pass is an ordinary launch
+    if ((rc = launch_c<N>(c_variant, scale, dp, 0, want_umax ? d_umax : nullptr, !want_umax)))
+      return rc;
     mark(2);
-    pass_d<T, N><<<dim3(XT, N, nfo), blk, smem_d(), stream>>>(g, B1, B2, tw, d_status);
+    if ((rc = launch_k(true, pass_d<T, N>, dim3(XT, N, nfo), blk, smem_d(), g, B1, B2, tw, d_status)))
+      return rc;
     mark(3);
     const dim3 ge(XT, g.Y);
     switch (scheme) {
       case SCHEME_NS_HEUN:
-        pass_e<T, N, 3, SCHEME_NS_HEUN><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        rc = launch_k(true, pass_e<T, N, 3, SCHEME_NS_HEUN>, ge, blk2, smem_e(), g, B2, tw, R, prm,
+                      stage, d_status);
         break;
       case SCHEME_EULER_HEUN:
-        pass_e<T, N, 3, SCHEME_EULER_HEUN><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        rc = launch_k(true, pass_e<T, N, 3, SCHEME_EULER_HEUN>, ge, blk2, smem_e(), g, B2, tw, R, prm,
+                      stage, d_status);
         break;
       case SCHEME_NS_RK4:
-        pass_e<T, N, 3, SCHEME_NS_RK4><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        rc = launch_k(true, pass_e<T, N, 3, SCHEME_NS_RK4>, ge, blk2, smem_e(), g, B2, tw, R, prm,
+                      stage, d_status);
         break;
       default:
-        pass_e<T, N, 4, SCHEME_BOUS_RK4><<<ge, blk2, smem_e(), stream>>>(g, B2, tw, R, prm, stage, d_status);
+        rc = launch_k(true, pass_e<T, N, 4, SCHEME_BOUS_RK4>, ge, blk2, smem_e(), g, B2, tw, R, prm,
+                      stage, d_status);
     }
+    if (rc) return rc;
     mark(4);
     launches += 5;
     PSG_CUDA_TRY(cudaGetLastError());
     return PSG_OK;
   }
 
-  int rhs(int stage, bool want_dump = false, bool want_umax = false) {
+  int rhs(int stage, bool want_dump = false, bool want_umax = false, bool chain = false) {
     switch (g.n) {
-      case 16: return rhs_n<16>(stage, want_dump, want_umax);
-      case 32: return rhs_n<32>(stage, want_dump, want_umax);
-      case 64: return rhs_n<64>(stage, want_dump, want_umax);
-      case 128: return rhs_n<128>(stage, want_dump, want_umax);
-      default: return rhs_n<256>(stage, want_dump, want_umax);
+      case 16: return rhs_n<16>(stage, want_dump, want_umax, chain);
+      case 32: return rhs_n<32>(stage, want_dump, want_umax, chain);
+      case 64: return rhs_n<64>(stage, want_dump, want_umax, chain);
+      case 128: return rhs_n<128>(stage, want_dump, want_umax, chain);
+      default: return rhs_n<256>(stage, want_dump, want_umax, chain);
     }
   }
 
   // one full time step of length dt; dump: keep the physical vorticity of the
-  // predictor (Heun schemes)
-  int step(T dt, bool want_dump = false) {
+  // predictor (Heun schemes).  chain: the previous step's last pass is the
+  // stream's last operation (steps() back to back)
+  int step(T dt, bool want_dump = false, bool chain = false) {
     prm.dt = dt;
     lin_dx = false;
     int rc;
     if (scheme == SCHEME_NS_HEUN || scheme == SCHEME_EULER_HEUN) {
-      if ((rc = rhs(STAGE_HEUN_PRED, want_dump && (dump_mode & 1)))) return rc;
-      return rhs(STAGE_HEUN_CORR, want_dump && !(dump_mode & 1));
+      if ((rc = rhs(STAGE_HEUN_PRED, want_dump && (dump_mode & 1), false, chain))) return rc;
+      return rhs(STAGE_HEUN_CORR, want_dump && !(dump_mode & 1), false, true);
     }
-    if ((rc = rhs(STAGE_RK1))) return rc;
-    if ((rc = rhs(STAGE_RK2))) return rc;
-    if ((rc = rhs(STAGE_RK3))) return rc;
-    return rhs(STAGE_RK4);
+    if ((rc = rhs(STAGE_RK1, false, false, chain))) return rc;
+    if ((rc = rhs(STAGE_RK2, false, false, true))) return rc;
+    if ((rc = rhs(STAGE_RK3, false, false, true))) return rc;
+    return rhs(STAGE_RK4, false, false, true);
   }
 
   // host FP64 boxes (reference layout) -> device state; RK4 schemes also set
@@ -2144,6 +2383,15 @@ struct Engine3D final : Engine3DBase {
 
   // ---------------------------------------------------------------- linearised step
   // pass A: staged tile [ncin][Y][W], twiddles, ng exchange groups, 1/k^2 table
+  // packed pass A: staged tile, twiddles, one exchange of 16-byte words with
+  // pass_a_pk's row stride, 1/k^2 table
+  template <int N>
+  size_t smem_a_pk_n(int ncin) const {
+    constexpr int S = LineFFT<N, 1, float>::SMEM;
+    constexpr int SX = S + ((1 - S % 8) + 8) % 8;
+    return sizeof(cpx<float>) * ((size_t)ncin * g.Y * kTileW + g.n) + 16 * (size_t)kTileW * SX +
+           sizeof(float) * g.Y * kTileW;
+  }
   size_t smem_a_nc(int ncin, int ng = 2) const {
     return sizeof(cpx<T>) * ((size_t)ncin * g.Y * kTileW + g.n + (size_t)ng * kTileW * col_stride()) +
            sizeof(T) * g.Y * kTileW;
@@ -2541,7 +2789,7 @@ struct Engine3D final : Engine3DBase {
   long launch_count() const override { return launches; }
   int steps(double dt, int nsteps, int dump_last) override {
     for (int s = 0; s < nsteps; ++s) {
-      int rc = step((T)dt, dump_last && s == nsteps - 1);
+      int rc = step((T)dt, dump_last && s == nsteps - 1, s > 0);
       if (rc) return rc;
     }
     return PSG_OK;
