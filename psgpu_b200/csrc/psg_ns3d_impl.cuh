@@ -617,7 +617,6 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   uint64_t* bar = s_bar[warp];
   const long plane = (long)N * N * XP;
   const uint32_t bytes = (uint32_t)(RPW * XP * sizeof(cpx<T>));
-  pdl_trigger();
   if (lane == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); }
   for (int i = tid; i < 2 * N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
@@ -798,6 +797,10 @@ pass_c(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     }
     __syncwarp();
   }
+  // The x-pass runs as one wave of resident blocks: a trigger at entry would
+  // let the next pass's blocks take the room left on these SMs and wait there
+  // for the whole pass.  Each block triggers when its rows are done.
+  pdl_trigger();
 }
 
 // ---------------------------------------------------------------------------
