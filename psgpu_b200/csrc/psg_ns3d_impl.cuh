@@ -1736,9 +1736,12 @@ struct Engine3D final : Engine3DBase {
   // optional per-pass timing with CUDA events recorded between the passes
   bool profiling = false;
   // programmatic dependent launch of the passes of a right-hand side (each
-  // pass's blocks launch and set up while the previous pass drains); off with
-  // PSG_PDL=0 and while the per-pass events are recorded
-  bool pdl = true;
+  // pass's blocks launch and set up while the previous pass drains), PSG_PDL:
+  // 0 off, 1 every pass, 2 every pass but the x-pass (a single wave of
+  // resident blocks), 3 every pass, with the passes' shared-memory carveout at
+  // its maximum so that blocks of consecutive passes share one SM
+  // configuration.  Off while the per-pass events are recorded.
+  int pdl = 1;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<int> ev_tag;
   size_t ev_used = 0;
@@ -1845,7 +1848,8 @@ struct Engine3D final : Engine3DBase {
     g.XP = (g.X + kTileW - 1) / kTileW * kTileW;
     g.alpha = (T)alpha;
     scheme = scheme_;
-    if (const char* e = getenv("PSG_PDL")) pdl = atoi(e) != 0;
+    if (const char* e = getenv("PSG_PDL")) pdl = atoi(e);
+    if (pdl < 0 || pdl > 3) pdl = 1;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
     nc = bous ? 4 : 3;
     nfi = bous ? 9 : 6;
@@ -1954,6 +1958,29 @@ struct Engine3D final : Engine3DBase {
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_RK4>));
     PSG_SMEM((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
 #undef PSG_SMEM
+    if (pdl == 3) {
+#define PSG_CARVE(kern) \
+  PSG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, \
+                                    (int)cudaSharedmemCarveoutMaxShared))
+      PSG_CARVE((pass_a<T, N, 3, 6>));
+      PSG_CARVE((pass_a<T, N, 4, 9, 0, 3>));
+      PSG_CARVE((pass_b<T, N>));
+      PSG_CARVE((pass_d<T, N>));
+      PSG_CARVE((pass_e<T, N, 3, SCHEME_NS_HEUN>));
+      PSG_CARVE((pass_e<T, N, 3, SCHEME_EULER_HEUN>));
+      PSG_CARVE((pass_e<T, N, 3, SCHEME_NS_RK4>));
+      PSG_CARVE((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
+#undef PSG_CARVE
+      for (int v = 0; v < kCVariants; ++v) {
+        if (!c_valid(v)) continue;
+        for (int nf : {6, 9, 7}) {
+          const void* k = c_kernel_nf<N>(v, nf);
+          if (k)
+            PSG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              (int)cudaSharedmemCarveoutMaxShared));
+        }
+      }
+    }
     int nsm = 0;
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     for (int v = 0; v < kCVariants; ++v) {
@@ -2231,7 +2258,8 @@ struct Engine3D final : Engine3DBase {
     T* dp = want_dump ? dump : nullptr;
     if (want_umax) PSG_CUDA_TRY(cudaMemsetAsync(d_umax, 0, sizeof(unsigned long long), stream));
     // after the memset the x-pass is an ordinary launch
-    if ((rc = launch_c<N>(c_variant, scale, dp, 0, want_umax ? d_umax : nullptr, !want_umax)))
+    if ((rc = launch_c<N>(c_variant, scale, dp, 0, want_umax ? d_umax : nullptr,
+                          !want_umax && pdl != 2)))
       return rc;
     mark(2);
     if ((rc = launch_k(true, pass_d<T, N>, dim3(XT, N, nfo), blk, smem_d(), g, B1, B2, tw, d_status)))

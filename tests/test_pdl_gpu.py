@@ -4,9 +4,10 @@ Each pass of a right-hand side launches with the programmatic-serialisation
 attribute after the pass before it (and pass A after the previous right-hand
 side's pass E), and waits on the previous grid before its first global access.
 The arithmetic is the same with and without it, so every scheme must give
-bit-identical states with PSG_PDL=1 (the default) and PSG_PDL=0, over one call of
-several steps (the steps chained) and over single-step calls, and the energetics
-reduction between calls must see the finished state.
+bit-identical states in every PSG_PDL mode (1: every pass, 2: every pass but the
+x-pass, 3: every pass with the maximum shared-memory carveout) and with it off
+(0), over one call of several steps (the steps chained) and over single-step
+calls, and the energetics reduction between calls must see the finished state.
 """
 import os
 
@@ -20,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _run(pdl, n, scheme, prec, calls):
-    os.environ["PSG_PDL"] = "1" if pdl else "0"
+    os.environ["PSG_PDL"] = str(pdl)
     try:
         e = P.NS3D(n, scheme, precision=prec, nu=1.0 / 400.0)
     finally:
@@ -45,9 +46,10 @@ def _run(pdl, n, scheme, prec, calls):
     (P.SCHEME_BOUS_RK4, 64, 32), (P.SCHEME_NS_HEUN, 32, 32), (P.SCHEME_EULER_HEUN, 64, 32)])
 def test_pdl_steps_bit_identical(scheme, prec, n):
     calls = [3, 1, 1, 2]  # chained steps in one call, and steps in calls of their own
-    a, ea = _run(True, n, scheme, prec, calls)
-    b, eb = _run(False, n, scheme, prec, calls)
-    for x, y in zip(a, b):
-        assert np.array_equal(x, y)
-    assert ea == eb
-    assert all(np.isfinite(v).all() for v in a)
+    b, eb = _run(0, n, scheme, prec, calls)
+    assert all(np.isfinite(v).all() for v in b)
+    for mode in (1, 2, 3):
+        a, ea = _run(mode, n, scheme, prec, calls)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), mode
+        assert ea == eb, mode
