@@ -265,8 +265,9 @@ def run_ours(args, rank, world, dist):
             "clocks": clocks, "gpu_launches": int(launches),
             "pass_a_autotune": {"packed": tune_a[0], "ms_per_launch": [round(x, 4) for x in tune_a[1]],
                                 "choices": "scalar, packed f32x2 (two fields per instruction)"},
-            "launch": "passes chained by programmatic dependent launch (each pass's blocks "
-                      "start and stage their tables while the previous pass drains)",
+            "launch": "passes chained by programmatic dependent launch, the x-pass excepted "
+                      "(each pass's blocks start and stage their tables while the previous pass "
+                      "drains; PSG_PDL=" + os.environ.get("PSG_PDL", "2") + ")",
             "x_pass_autotune": {"variant": tune[0], "ms_per_launch": [round(x, 4) for x in tune[1]],
                                 "variants": "bit 0: 256/G rows per block (else 128/G), bit 3: "
                                             "64/G rows, bit 1: two copy buffers per warp, bit 2: "

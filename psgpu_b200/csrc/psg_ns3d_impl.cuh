@@ -1737,11 +1737,12 @@ struct Engine3D final : Engine3DBase {
   bool profiling = false;
   // programmatic dependent launch of the passes of a right-hand side (each
   // pass's blocks launch and set up while the previous pass drains), PSG_PDL:
-  // 0 off, 1 every pass, 2 every pass but the x-pass (a single wave of
-  // resident blocks), 3 every pass, with the passes' shared-memory carveout at
-  // its maximum so that blocks of consecutive passes share one SM
-  // configuration.  Off while the per-pass events are recorded.
-  int pdl = 1;
+  // 0 off, 1 every pass, 2 (default) every pass but the x-pass.  The x-pass is
+  // a single wave of resident blocks sized to fill the SMs; launched early, its
+  // blocks land beside the y-inverse's last ones, and with the smaller block
+  // variants the step loses more than the overlap gains.  Off while the
+  // per-pass events are recorded.
+  int pdl = 2;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<int> ev_tag;
   size_t ev_used = 0;
@@ -1849,7 +1850,7 @@ struct Engine3D final : Engine3DBase {
     g.alpha = (T)alpha;
     scheme = scheme_;
     if (const char* e = getenv("PSG_PDL")) pdl = atoi(e);
-    if (pdl < 0 || pdl > 3) pdl = 1;
+    if (pdl < 0 || pdl > 2) pdl = 2;
     const bool bous = (scheme == SCHEME_BOUS_RK4);
     nc = bous ? 4 : 3;
     nfi = bous ? 9 : 6;
@@ -1958,29 +1959,6 @@ struct Engine3D final : Engine3DBase {
     PSG_SMEM((pass_e<T, N, 3, SCHEME_NS_RK4>));
     PSG_SMEM((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
 #undef PSG_SMEM
-    if (pdl == 3) {
-#define PSG_CARVE(kern) \
-  PSG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, \
-                                    (int)cudaSharedmemCarveoutMaxShared))
-      PSG_CARVE((pass_a<T, N, 3, 6>));
-      PSG_CARVE((pass_a<T, N, 4, 9, 0, 3>));
-      PSG_CARVE((pass_b<T, N>));
-      PSG_CARVE((pass_d<T, N>));
-      PSG_CARVE((pass_e<T, N, 3, SCHEME_NS_HEUN>));
-      PSG_CARVE((pass_e<T, N, 3, SCHEME_EULER_HEUN>));
-      PSG_CARVE((pass_e<T, N, 3, SCHEME_NS_RK4>));
-      PSG_CARVE((pass_e<T, N, 4, SCHEME_BOUS_RK4>));
-#undef PSG_CARVE
-      for (int v = 0; v < kCVariants; ++v) {
-        if (!c_valid(v)) continue;
-        for (int nf : {6, 9, 7}) {
-          const void* k = c_kernel_nf<N>(v, nf);
-          if (k)
-            PSG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                              (int)cudaSharedmemCarveoutMaxShared));
-        }
-      }
-    }
     int nsm = 0;
     PSG_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     for (int v = 0; v < kCVariants; ++v) {
