@@ -85,8 +85,10 @@ struct RowStride {
 // pdl_wait: block until the kernels this launch depends on have completed and
 // their writes are visible.  Every pass calls pdl_wait before its first global
 // access other than the constant twiddle table, reads and writes alike (the
-// next pass writes buffers the previous one reads).  Both are no-ops for a
-// launch without the programmatic-serialisation attribute.
+// next pass writes buffers the previous one reads), and issues its tile copy
+// right after it, so that the table set-up runs while the copy is in flight in
+// every wave of blocks.  Both are no-ops for a launch without the
+// programmatic-serialisation attribute.
 __device__ __forceinline__ void pdl_trigger() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
@@ -154,6 +156,13 @@ __device__ __forceinline__ bool a_stage(const Geom3<T>& g, Src src_comp, const c
   pdl_trigger();
   if (tid == 0) mbar_init(s_bar, 1);
   __syncthreads();
+  pdl_wait();
+  if (tid == 0) {
+    mbar_expect_tx(s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
+    for (int q = 0; q < NC; ++q)
+      bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), s_bar);
+  }
+  // the tables while the copy is in flight
   for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   const bool mirror = (xt == 0) && (iky <= K);
   for (int idx = tid; idx < Y * W; idx += nth) {
@@ -166,12 +175,6 @@ __device__ __forceinline__ bool a_stage(const Geom3<T>& g, Src src_comp, const c
     const T kx = (T)ikx * g.alpha, ky = (T)(iky - K), kz = (T)(ikz - K);
     const T wki = wkinv(kx * kx + ky * ky + kz * kz);
     s_wk[idx] = ll ? wki : -wki;
-  }
-  pdl_wait();
-  if (tid == 0) {
-    mbar_expect_tx(s_bar, (uint32_t)(NC * Y * W * sizeof(cpx<T>)));
-    for (int q = 0; q < NC; ++q)
-      bulk_g2s(s_in + q * Y * W, src_comp(q) + tile, (uint32_t)(Y * W * sizeof(cpx<T>)), s_bar);
   }
   if (!tile_wait(s_bar, s_ok, status)) return false;
   if (mirror) {
@@ -382,7 +385,6 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
   pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
   pdl_wait();
   if (tid == 0) {
@@ -390,6 +392,7 @@ pass_b(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * Y * W, (uint32_t)(Y * W * sizeof(cpx<T>)),
              &s_bar);
   }
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   cpx<T> v[F::E];
 #pragma unroll
@@ -825,7 +828,6 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
   const int xt = blockIdx.x, z = blockIdx.y, f = blockIdx.z;
   pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
-  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
   pdl_wait();
   if (tid == 0) {
@@ -833,6 +835,7 @@ pass_d(Geom3<T> g, const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
     bulk_g2s(s_in, in + (((long)f * XT + xt) * N + z) * N * W, (uint32_t)(N * W * sizeof(cpx<T>)),
              &s_bar);
   }
+  for (int i = tid; i < N; i += blockDim.x) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   cpx<T> v[F::E];
 #pragma unroll
@@ -1112,7 +1115,6 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
   const int xt = blockIdx.x, iky = blockIdx.y;
   pdl_trigger();
   if (tid == 0) mbar_init(&s_bar, 1);
-  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   __syncthreads();
   const long tile = ((long)xt * Y + iky) * Y * W;
   pdl_wait();
@@ -1138,6 +1140,7 @@ pass_e(Geom3<T> g, const cpx<T>* __restrict__ in, const cpx<T>* __restrict__ tw,
       }
     }
   }
+  for (int i = tid; i < N; i += nth) s_tw[i] = tw[i];
   if (!tile_wait(&s_bar, &s_ok, status)) return;
   // three fields: both halves transform (fields 2 and 1, then 0), the second
   // half in an exchange area of its own; more fields: the first half alone
