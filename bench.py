@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -684,10 +685,42 @@ def run_ensemble2d(args, rank=0, world=1, dist=None, dev=None):
                               "threads": [128, 256, 512]},
            "transform_schedule": {str(n): {"packed": pk, "ms_scalar_packed": [round(x, 4) for x in ms]}
                                   for n, (pk, ms) in sched.items() if ms[0] >= 0}}
+    flops = ensemble_flops([int(n) for n in sizes_all], steps)
+    peak = fp32_simt_peak(dev if dev is not None else torch.cuda.current_device())
+    out["flop_rate"] = {"achieved_tflops": round(flops / dev_s / 1e12, 3),
+                        "peak_tflops": round(peak / 1e12, 2), "frac": round(flops / dev_s / peak, 4),
+                        "peak_kind": "nominal FP32 SIMT (SMs x 128 lanes x 2 x max SM clock)",
+                        "flops": "nominal FFT flops: a real N x N transform 2.5 N^2 log2 N^2, five "
+                                 "per right-hand side, four per RK4 step (the truncated modes the "
+                                 "kernel skips are counted)"}
     path = os.path.join(ROOT, "oracle", "_ref", "libref_ns2d.so")
     if os.path.exists(path) and world == 1:
         out["plain_reference"] = ensemble_plain(sizes_all, nu_all, path)
     return out
+
+
+def ensemble_flops(sizes, steps):
+    """Nominal FFT flops of `steps` RK4/CN steps of 2D instances of the given
+    grid sizes: a real N x N transform counted as 2.5 N^2 log2(N^2) (the
+    5 n log2 n convention for a complex length-n transform), five per
+    right-hand side (w, u, v inverse; the two products forward), four
+    right-hand sides per step."""
+    per_step = sum(4 * 5 * 2.5 * n * n * math.log2(n * n) for n in sizes)
+    return per_step * steps
+
+
+def fp32_simt_peak(dev):
+    """Nominal FP32 SIMT rate of the device in FLOP/s: SMs x 128 FP32 lanes x
+    2 (fused multiply-add) x the maximum SM clock recorded in the peaks file
+    (1965 MHz without one)."""
+    import torch
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = 1965.0
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", mhz))
+    return nsm * 128 * 2 * mhz * 1e6
 
 
 def ensemble_plain(sizes_all, nu_all, path, per_size=4, steps=200):
